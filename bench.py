@@ -1,0 +1,395 @@
+"""Benchmark of the per-step hot path: particle-steps/s of the Evrard collapse
+at N = 1,000,000 on one B200, mixed precision (FP32 walk and SPH sums with
+Kahan compensation, FP64 positions / integration / h convergence) beside the
+plain FP64 step on the same GPU, with the acceleration error of each against
+an FP64 direct-summation oracle on a seeded 10k-particle subset.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  Multi-GPU (torchrun): every rank advances its
+own replica of the workload (the single sphere does not shard without a halo
+exchange), timing is the max over ranks, value is the whole-job
+throughput.  --impl reference times the reference's CPU implementation of the
+step (the oracle's C restatement of MPI_sph/sph_code/libsx.py + shear.py, the
+reference's all-pairs loops with its row-range decomposition) on the host
+cores, on a bounded row sample per step, extrapolated to the full N.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at N=1M Evrard (mixed vs FP64 plain, same B200) at <=1e-4 accel err"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--theta", type=float, default=0.4)
+    ap.add_argument("--leaf", type=int, default=16)
+    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--err-subset", type=int, default=10_000)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.index), "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU sample ----
+def cpu_reference_sample(n, rows_per_thread=64, seed=42):
+    """One step of the reference's CPU path (oracle restatement of
+    h_smooth_fast_mpi, getDensity_mpi, getAcc_g_smth_mimj_mpi, div_curlVel_mpi,
+    getAcc_sph_shear_mpi, get_dU_shear_mpi -- sph_mpi4_v4.py:278-416) on a
+    contiguous row slice of size rows_per_thread * threads against all n
+    sources, extrapolated by n/rows.  Returns (seconds per full step, info)."""
+    from oracle import oracle as O
+    from sph_2_b200 import ic
+    d = ic.evrard(n, seed=seed)
+    pos = np.ascontiguousarray(d["pos"])
+    m, u, h = d["m"], d["u"], d["h"]
+    r = np.linalg.norm(pos, axis=1)
+    rho = 1.0 / (2.0 * np.pi * np.maximum(r, 1e-3))          # analytic profile for j-data
+    P = (5 / 3 - 1) * rho * u
+    c = np.sqrt(5 / 3 * (5 / 3 - 1) * u)
+    v = np.zeros_like(pos)
+    zero = np.zeros(n)
+    eps = np.full(n, 1e-2)
+    thr = O.num_threads()
+    rows = min(n, rows_per_thread * thr)
+    nb = n // 2 - rows // 2
+    ne = nb + rows
+    # steady state of the reference's h iteration: h of the previous step is
+    # already converged, so converge the sample rows once (untimed)
+    hs = h.copy()
+    hs[nb:ne] = O.ref_h_smooth_fast(nb, ne, pos, h)
+    t = {}
+    t0 = time.perf_counter(); O.ref_h_smooth_fast(nb, ne, pos, hs); t["h_smooth_fast"] = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.ref_getDensity(nb, ne, pos, m, hs); t["density"] = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.ref_getAcc_g_smth_mimj(nb, ne, pos, m, 1.0, eps); t["gravity"] = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.ref_div_curlVel(nb, ne, pos, v, rho, m, hs); t["divcurl"] = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.ref_getAcc_sph(nb, ne, pos, v, rho, P, c, hs, m, zero, zero, 1.0); t["acc_sph"] = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.ref_get_dU(nb, ne, pos, v, rho, P, c, hs, m, zero, zero, 1.0); t["dudt"] = time.perf_counter() - t0
+    scale = n / rows
+    step_s = sum(t.values()) * scale
+    return step_s, dict(rows=rows, threads=thr, phase_s={k: round(v * scale, 3) for k, v in t.items()},
+                        sample_s=round(sum(t.values()), 3))
+
+
+def reference_arm(a, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    thr = O.num_threads()
+    rpt = 32
+    for _ in range(a.warmup):
+        cpu_reference_sample(a.n, rpt)
+    steps = []
+    info = None
+    for _ in range(a.steps):
+        s, info = cpu_reference_sample(a.n, rpt)
+        steps.append(s)
+    step_s = float(np.mean(steps))
+    value = a.n / step_s
+    sample = (f"{info['rows']} rows x {a.n} sources per phase per step (contiguous slice at N/2), "
+              f"6 phases, extrapolated x{a.n / info['rows']:.0f}; oracle C restatement of the "
+              "reference numba step, OpenMP over rows")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Evrard sphere)",
+        "config": {"workload": f"evrard_n{a.n}_reference_cpu_step", "n": a.n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "phase_s_extrapolated": info["phase_s"],
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ ours ----
+def rms_rel(a, b):
+    num = np.sum((a - b) ** 2, axis=1)
+    den = np.sum(b * b, axis=1) + 1e-300
+    return float(np.sqrt(np.mean(num / den)))
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        reference_arm(a, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from sph_2_b200 import Config, Context, ic
+    from sph_2_b200 import _lib as L
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = a.n
+    d = ic.evrard(n, seed=42 + rank)
+    stream = torch.cuda.Stream()
+
+    def make(precision, flags=0):
+        cfg = Config(n_max=n, precision=precision, theta=a.theta, leaf_size=a.leaf,
+                     ngb_lanes=a.lanes, flags=flags)
+        c = Context(cfg)
+        c.set_stream(stream.cuda_stream)
+        c.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+        c.prologue()
+        return c
+
+    def timed_steps(ctx, steps, warmup):
+        ctx.step(warmup)
+        ctx.sync()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+            ctx.step(steps)
+            e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    # ---- mixed precision arm (the headline) ----
+    ctx = make("mixed", L.FLAG_TIMING)
+    sampler = ClockSampler(local)
+    ctx.step(a.warmup)
+    ctx.sync()
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+        ctx.step(a.steps)
+        e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * n * a.steps / (ms * 1e-3)
+    phases = ctx.phase_times()
+    kernels_per_step = ctx.graph_kernel_count()
+    status = ctx.status()
+
+    # ---- roofline of the dominant kernel (the gravity walk) ----
+    reps = 5
+    ctx.gravity()
+    ctx.sync()
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        w0.record()
+        for _ in range(reps):
+            ctx.gravity()
+        w1.record()
+    torch.cuda.synchronize()
+    walk_ms = w0.elapsed_time(w1) / reps
+    cnt = ctx.counters()
+    flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"]
+    fp32_peak = ctx.fp32_peak_tflops()
+    achieved = flops / (walk_ms * 1e-3) / 1e12
+    roofline = {"kernel": "k_walk<float> (gravity walk)", "bound": "fp32",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json "
+                               "has no FP32 figure)",
+                "algorithmic": "60 flop per quadrupole cell + 20 per particle interaction",
+                "interactions_per_particle": {"cells": cnt["cells"] / n,
+                                              "particles": cnt["particles"] / n},
+                "walk_ms": walk_ms}
+    try:
+        with open(os.path.join(ROOT, "profiles", "walk_traffic.json")) as f:
+            tr = json.load(f)
+        roofline["traffic"] = tr["dram_bytes_per_interaction"] * (cnt["cells"] + cnt["particles"])
+        roofline["traffic_source"] = tr["source"]
+    except (OSError, KeyError, ValueError):
+        pass
+
+    # ---- accuracy at the common initial state (mixed vs FP64 oracle) ----
+    err = {}
+    ctx64 = None
+    if not a.no_fp64:
+        ctx64 = make("fp64", L.FLAG_TIMING)
+        sub = np.random.default_rng(7).choice(n, min(a.err_subset, n), replace=False)
+        # both prologues ran on the same seeded state; compare in original order
+        ctx_m = make("mixed")
+        ids64 = ctx64.ids()
+        inv = np.empty(n, np.int64)
+        inv[ids64] = np.arange(n)
+        tg = inv[sub].astype(np.int32)                       # storage indices in ctx64
+        ad, _ = ctx64.gravity_direct(tg)                     # FP64 direct sum
+        ag_m = ctx_m.get_acc("grav")[sub]
+        ag_64 = ctx64.get_acc("grav")[sub]
+        as_m = ctx_m.get_acc("sph")[sub]
+        as_64 = ctx64.get_acc("sph")[sub]
+        err = {"grav_mixed_vs_direct_fp64": rms_rel(ag_m, ad),
+               "grav_fp64tree_vs_direct_fp64": rms_rel(ag_64, ad),
+               "sph_mixed_vs_fp64": rms_rel(as_m, as_64),
+               "total_mixed_vs_fp64_oracle": rms_rel(ag_m + as_m, ad + as_64),
+               "rho_mixed_vs_fp64": float(np.max(np.abs(ctx_m.get("rho")[sub] / ctx64.get("rho")[sub] - 1))),
+               "dudt_mixed_vs_fp64": float(np.sqrt(np.mean((ctx_m.get("dudt")[sub] - ctx64.get("dudt")[sub]) ** 2)) /
+                                           np.sqrt(np.mean(ctx64.get("dudt")[sub] ** 2))),
+               "subset": len(sub), "definition": "RMS over the subset of |a-a_ref|/|a_ref|"}
+        ctx_m.close()
+        ms64 = timed_steps(ctx64, max(2, a.steps // 2), a.warmup)
+        k64 = max(2, a.steps // 2)
+        fp64 = {"value": world * n * k64 / (ms64 * 1e-3), "ms_per_step": ms64 / k64, "steps": k64,
+                "phases_ms": ctx64.phase_times()}
+        ctx64.close()
+    else:
+        fp64 = None
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        fields = ["x", "y", "z", "vx", "vy", "vz", "u", "h"]
+        pinned = {f: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for f in fields}
+        for f in fields:
+            pinned[f][:] = ctx.get(f)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            for f in fields:
+                ctx.set(f, pinned[f])
+            ctx.step(1)
+            for f in fields:
+                pinned[f][:] = ctx.get(f)
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * n * a.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": 8 * n * len(fields), "d2h_bytes_per_step": 8 * n * len(fields),
+               "api": "sph_set_field x8 (pinned host) + sph_step + sph_get_field x8 per step"}
+
+    # ---- CPU baseline (rank 0, one GPU only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        step_s, info = cpu_reference_sample(n, 64)
+        cpu = {"value": n / step_s, "unit": UNIT, "cores": info["threads"], "kind": "port",
+               "sample": (f"{info['rows']} rows x {n} sources per phase (6 phases of the reference "
+                          f"CPU step), extrapolated x{n / info['rows']:.0f}; {info['sample_s']} s "
+                          "of CPU work"),
+               "phase_s_extrapolated": info["phase_s"]}
+
+    final_status = ctx.status()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64 (mixed)",
+        "data": "synthetic (seeded Evrard sphere, numpy default_rng)",
+        "config": {"workload": "evrard_1M_mixed" if n == 1_000_000 else f"evrard_{n}_mixed",
+                   "n": n, "theta": a.theta, "leaf_size": a.leaf, "ngb_lanes": a.lanes,
+                   "n_ngb": 64, "eps": 1e-2, "av": "monaghan-gingold alpha=1 beta=2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "working set > L2 (neighbour rows ~0.3 GB + tree ~0.5 GB per step)",
+                   "graph": "CUDA graph per step"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": kernels_per_step * a.steps,
+        "clocks": clocks,
+        "fp64_plain": fp64,
+        "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+        "accel_err": err,
+        "phases_ms": phases,
+        "status": final_status,
+        "device_gb": ctx.device_bytes() / 1e9,
+    }
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

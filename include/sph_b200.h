@@ -1,0 +1,297 @@
+/*
+ * sph_b200.h -- C ABI of libsphb200.so, the B200 (sm_100a) per-step hot path
+ * of a self-gravitating SPH code (Evrard collapse, cooling cloud collapse).
+ *
+ * The reference (hassanfv/SPH_2) exposes this path in two forms: numba
+ * functions over caller-owned NumPy arrays with a row range [nbeg, nend)
+ * (MPI_sph/sph_code/libsx.py, shear.py) and CUDA __global__ kernels over
+ * caller-owned float* SoA device arrays (Particles_in_BH_Tree_II/Evrard_test/
+ * hfvCLibs_v7_hfv_v2.h, bh_tree_iteration_v2.h, ngb_v3.h).  Each entry point
+ * below names the reference functions it replaces.
+ *
+ * Conventions
+ *  - Every call returns SPH_OK (0) or a negative SPH_ERR_* code; nothing in
+ *    the library exits, aborts, traps or prints.  Data-dependent device loops
+ *    are bounded and report through status counters (sph_get_status).
+ *  - Work is queued on the context's stream (sph_set_stream); calls return
+ *    before the GPU has finished unless they copy data to the host.
+ *  - Particle state lives on the device in FP64 (positions, velocities, u,
+ *    h, masses).  The context reorders particles along Morton keys at every
+ *    sph_sort; sph_get_field / sph_set_field take and give arrays in the
+ *    caller's ORIGINAL particle order unless `storage_order` is set.
+ *  - Pointers flagged `host` are host memory (pageable or pinned); otherwise
+ *    device memory of the context's device.
+ *  - One context per host thread at a time.
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SPH_OK 0
+#define SPH_ERR_ARG (-1)        /* bad argument (null pointer, size, enum)            */
+#define SPH_ERR_CUDA (-2)       /* a CUDA runtime call failed (see sph_last_error)     */
+#define SPH_ERR_CAPACITY (-3)   /* n or a cloud count above the context's capacity     */
+#define SPH_ERR_NOCONV (-4)     /* smoothing-length iteration did not converge         */
+#define SPH_ERR_OVERFLOW (-5)   /* neighbour list or traversal stack overflow          */
+#define SPH_ERR_NONFINITE (-6)  /* NaN/Inf found in positions or results               */
+#define SPH_ERR_STATE (-7)      /* call order violated (e.g. forces before density)    */
+#define SPH_ERR_NOMEM (-8)      /* device allocation failed                            */
+
+/* ---- enums ---- */
+#define SPH_PREC_FP64 0   /* every sum and the gravity walk in FP64                  */
+#define SPH_PREC_MIXED 1  /* FP32 walk and SPH sums with Kahan compensation; FP64
+                             positions, integration, h convergence, reductions       */
+#define SPH_AV_MG83 0     /* Monaghan & Gingold 1983 (libsx.py:185-262)              */
+#define SPH_AV_GADGET 1   /* signal-velocity form (shear.py:243-330, hfvCLibs:705)   */
+
+/* fields for sph_get_field / sph_set_field (FP64 unless noted) */
+#define SPH_F_X 0
+#define SPH_F_Y 1
+#define SPH_F_Z 2
+#define SPH_F_VX 3
+#define SPH_F_VY 4
+#define SPH_F_VZ 5
+#define SPH_F_M 6
+#define SPH_F_H 7
+#define SPH_F_U 8
+#define SPH_F_RHO 9
+#define SPH_F_P 10
+#define SPH_F_C 11
+#define SPH_F_DIVV 12
+#define SPH_F_CURLV 13
+#define SPH_F_AX_SPH 14
+#define SPH_F_AY_SPH 15
+#define SPH_F_AZ_SPH 16
+#define SPH_F_AX_GRAV 17
+#define SPH_F_AY_GRAV 18
+#define SPH_F_AZ_GRAV 19
+#define SPH_F_DUDT 20
+#define SPH_F_VSIG 21
+#define SPH_F_POT 22
+#define SPH_F_DUDT_PREV 23
+#define SPH_F_U_PREV 24
+#define SPH_NFIELDS 25
+
+/* status counters (sph_get_status) */
+#define SPH_S_H_NOCONV 0      /* particles whose Newton h iteration hit the cap   */
+#define SPH_S_NGB_OVERFLOW 1  /* rows longer than max_ngb (truncated)            */
+#define SPH_S_STACK_OVERFLOW 2/* traversal stack overflows (walk or search)      */
+#define SPH_S_H_RETRY 3       /* candidate searches repeated for growing h       */
+#define SPH_S_COOL_NOCONV 4   /* cooling solves that hit the iteration cap       */
+#define SPH_S_MLP_FALLBACK 5  /* surrogate rows sent back to the exact solver    */
+#define SPH_S_NONFINITE 6     /* non-finite inputs seen                          */
+#define SPH_S_WALK_STACK_MAX 7/* deepest traversal stack seen in the gravity walk */
+#define SPH_NSTATUS 8
+
+#define SPH_FLAG_DUDT_FUSED 1  /* du/dt in the force pass (one pass) instead of the
+                                  reference order (after the closing kick)          */
+#define SPH_FLAG_COOLING 2     /* apply the implicit cooling in sph_step            */
+#define SPH_FLAG_COOLING_MLP 4 /* use the MLP surrogate (exact fallback)            */
+#define SPH_FLAG_NO_GRAPH 8    /* run sph_step eagerly, without CUDA graph replay   */
+#define SPH_FLAG_POTENTIAL 16  /* compute the gravitational potential in the walk   */
+#define SPH_FLAG_TIMING 32     /* record CUDA events between the phases of sph_step */
+
+typedef struct sph_config {
+    int32_t n_max;        /* particle capacity                                    */
+    int32_t n_cloud_max;  /* cloud capacity (ensemble); 1 for a single sphere     */
+    int32_t precision;    /* SPH_PREC_*                                           */
+    int32_t av_mode;      /* SPH_AV_*                                             */
+    int32_t balsara;      /* 1: multiply the viscosity by the Balsara factor      */
+    int32_t leaf_size;    /* tree bucket size, 1..64                              */
+    int32_t ngb_lanes;    /* lanes per particle in neighbour sums: 4, 8, 16, 32   */
+    int32_t block_size;   /* threads per block of the neighbour-sum passes        */
+    int32_t max_ngb;      /* neighbour-list row capacity                          */
+    int32_t h_max_iter;   /* Newton iteration cap                                 */
+    int32_t flags;        /* SPH_FLAG_*                                           */
+    int32_t walk_warps;   /* warps per block of the gravity walk                  */
+    double n_ngb;         /* target (4pi/3)(2h)^3 rho / m                         */
+    double h_tol;         /* |dh/h| convergence of the Newton iteration           */
+    double gamma, alpha, beta, eta; /* EOS and viscosity (libsx.py:22-26)         */
+    double G, eps;        /* gravity constant and Plummer softening               */
+    double theta;         /* opening angle                                        */
+    double courant;       /* dt = courant * min(h/v_sig, sqrt(h/|a|))             */
+    double dt_max;        /* upper bound on dt (0: none)                          */
+    double dt_fixed;      /* >0: fixed step (reference drivers), no Courant dt    */
+} sph_config;
+
+typedef struct sph_ctx sph_ctx;
+
+/* cooling problem (physical units) for the implicit solve and the surrogate */
+typedef struct sph_cooling_params {
+    int32_t n_bins;        /* bins of the log-log Lambda(T) table (table has n_bins+1) */
+    int32_t max_iter;      /* bisection cap                                           */
+    double logT0, logT1;   /* table range, log10 K                                    */
+    double mu, gamma, XH;  /* mean molecular weight, adiabatic index, H mass fraction */
+    double gamma_heat;     /* heating per H atom, erg/s                               */
+    double tol;            /* |du/u| stopping test of the bisection                   */
+    double unit_rho, unit_u, unit_t; /* code -> cgs factors                           */
+    double mlp_err_tol;    /* surrogate rows with estimated |du/u| above this fall back */
+} sph_cooling_params;
+
+/* ---- context ---- */
+int sph_default_config(sph_config *cfg);
+int sph_ctx_create(const sph_config *cfg, sph_ctx **out);
+void sph_ctx_destroy(sph_ctx *ctx);
+int sph_set_stream(sph_ctx *ctx, void *cuda_stream);
+int sph_sync(sph_ctx *ctx);
+const char *sph_last_error(sph_ctx *ctx);
+int sph_get_config(sph_ctx *ctx, sph_config *out);
+int sph_set_params(sph_ctx *ctx, const sph_config *cfg); /* physics scalars only */
+int64_t sph_device_bytes(sph_ctx *ctx);
+
+/* Load n particles (replaces readVectorsFromFile + cudaMemcpy H2D,
+ * hfvCLibs_v7_hfv_v2.h:59, EVR.cu:508-556, and the pickle IC of
+ * sph_mpi4_v4.py:44-53).  cloud may be NULL (one cloud).  Arrays in host or
+ * device memory (host != 0: host). */
+int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, const double *y,
+             const double *z, const double *vx, const double *vy, const double *vz,
+             const double *m, const double *h, const double *u, int32_t host);
+int32_t sph_count(sph_ctx *ctx);
+int32_t sph_cloud_count(sph_ctx *ctx);
+int sph_get_field(sph_ctx *ctx, int32_t field, double *out, int32_t host, int32_t storage_order);
+int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host, int32_t storage_order);
+/* original id of each stored particle (storage order) */
+int sph_get_ids(sph_ctx *ctx, int32_t *out, int32_t host);
+int sph_get_status(sph_ctx *ctx, int64_t *out /* SPH_NSTATUS */, int32_t reset);
+int sph_get_dt(sph_ctx *ctx, double *dt /* per cloud */);
+int sph_set_dt(sph_ctx *ctx, const double *dt /* per cloud */);
+
+/* ---- phases (each queued on the context stream) ---- */
+
+/* Per-cloud bounding box (compute_bounding_box_kernel, bh_tree_iteration_v2.h:
+ * 76-145), 63-bit Morton keys and a stable LSD radix sort of the storage order
+ * (replaces CountBodies/ComputeOffset/GroupBodies, ngb_v3.h:58-117), then the
+ * particle state is permuted into key order. */
+int sph_sort(sph_ctx *ctx);
+/* keys of the CURRENT storage order (before permutation) and the stable
+ * permutation perm (new slot s holds old slot perm[s]), from the last sort */
+int sph_get_sort(sph_ctx *ctx, uint64_t *keys, int32_t *perm, int32_t host);
+
+/* Karras radix tree over the sorted keys with FP64 bottom-up mass, centre of
+ * mass, quadrupole, box and h_max (replaces reset_arrays_kernel,
+ * build_tree_kernel, centre_of_mass_kernel, sort_kernel,
+ * bh_tree_iteration_v2.h:29-450). */
+int sph_build_tree(sph_ctx *ctx);
+/* FP64 node records (16 doubles each: com xyz, mass, Qxx Qyy Qzz Qxy Qxz Qyz,
+ * box min xyz, box max xyz), child pairs, particle ranges, opening radii^2 */
+int sph_get_tree(sph_ctx *ctx, double *node, int32_t *child, int32_t *first, int32_t *last,
+                 double *open_r2, double *hmax, int32_t host);
+
+/* Newton smoothing-length iteration (replaces smoothing_h_ngb,
+ * hfvCLibs_v7_hfv_v2.h:367-455, and h_smooth_fast_mpi, libsx.py:854-902).
+ * Needs sph_build_tree. */
+int sph_smoothing_h(sph_ctx *ctx);
+/* Exact neighbour lists |r_ij|^2 <= (h_i+h_j)^2 (replaces ngbDB_new_v2,
+ * ngb_v3.h:124-238).  Needs sph_build_tree (h_max is refitted here). */
+int sph_neighbours(sph_ctx *ctx);
+/* canonical export: CSR over storage order, rows sorted ascending by
+ * storage index; off has n+1 entries; lst capacity cap */
+int sph_get_neighbours(sph_ctx *ctx, int64_t *off, int32_t *lst, int64_t cap, int32_t host);
+
+/* rho = sum m_j W(r_ij, h_ij) and the EOS epilogue P, c (getDensity_ngb,
+ * getPressure_Adiabatic, getCsound_Adiabatic, hfvCLibs_v7_hfv_v2.h:474-612;
+ * getDensity_mpi, libsx.py:52-86) */
+int sph_density(sph_ctx *ctx);
+/* div v, |curl v| (div_curlVel_ngb, hfvCLibs:617-700; div_curlVel_mpi,
+ * shear.py:78-142) */
+int sph_divcurl(sph_ctx *ctx);
+/* pressure + viscous acceleration and signal velocity (acc_sph_ngb,
+ * hfvCLibs:705-801; getAcc_sph_shear_mpi, shear.py:243-330;
+ * getAcc_sph_mpiXXX, libsx.py:185-262); with SPH_FLAG_DUDT_FUSED also du/dt */
+int sph_forces(sph_ctx *ctx);
+/* du/dt (get_dU_ngb, hfvCLibs:825-916; get_dU_shear_mpi, shear.py:413-485) */
+int sph_dudt(sph_ctx *ctx);
+/* Barnes-Hut walk, monopole + quadrupole, Plummer softening (replaces
+ * compute_forces_kernel, bh_tree_iteration_v2.h:454-588).  Counts the
+ * interactions (sph_get_counters). */
+int sph_gravity(sph_ctx *ctx);
+/* FP64 direct Plummer sum onto ntarget particles (storage indices) from all
+ * particles of their cloud (replaces acc_g, hfvCLibs:532-584, and
+ * getAcc_g_smth_mimj_mpi, libsx.py:910-947).  out: ntarget*4 (ax,ay,az,pot). */
+int sph_gravity_direct(sph_ctx *ctx, int32_t ntarget, const int32_t *targets, double *out,
+                       int32_t host);
+/* spline-softened direct sum of libsx.py:910-947 with per-particle eps
+ * (eps_ij = (eps_i+eps_j)/2), FP64, out: ntarget*3 */
+int sph_gravity_direct_spline(sph_ctx *ctx, const double *eps, int32_t ntarget,
+                              const int32_t *targets, double *out, int32_t host);
+/* v += a dt * fac with a = a_sph + a_grav (v_evolve, hfvCLibs:936-949) */
+int sph_kick(sph_ctx *ctx, double fac);
+/* x += v dt (r_evolveT, hfvCLibs:981-994) */
+int sph_drift(sph_ctx *ctx);
+/* u = u_prev + dt/2 (dudt + dudt_prev); u_prev = u; dudt_prev = dudt
+ * (u_updater, hfvCLibs:921-931; sph_mpi4_v4.py:413-424).  first != 0: the
+ * prologue form u += dudt dt (sph_mpi4_v4.py:240-244). */
+int sph_update_u(sph_ctx *ctx, int32_t first);
+/* Courant step per cloud dt = courant * min_i min(h/v_sig, sqrt(h/|a|))
+ * (dt_array_indiv_dt, hfvCLibs:999-1078, over neighbours only); stored as
+ * the step of the next sph_step and returned in dt (per cloud) if not NULL */
+int sph_cfl_dt(sph_ctx *ctx, double *dt);
+/* totals: [KE, U, PE, px, py, pz, Lx, Ly, Lz, M] (getKE/getPE, libsx.py:571-620);
+ * PE needs SPH_FLAG_POTENTIAL in the last gravity call */
+int sph_energies(sph_ctx *ctx, double *out10);
+/* interaction counters of the last gravity call: [cells, particles] */
+int sph_get_counters(sph_ctx *ctx, int64_t *out2);
+
+/* ---- cooling (DoCooling, myPhotoLibsGPU.h:615-686; hcoolingx, hfvCLibs:1240) ---- */
+int sph_cooling_setup(sph_ctx *ctx, const sph_cooling_params *p, const double *log_lambda);
+/* implicit solve for every particle over dt (code units) */
+int sph_cooling_exact(sph_ctx *ctx);
+/* MLP surrogate + error estimate + exact fallback */
+int sph_cooling_mlp(sph_ctx *ctx);
+/* Standalone batched solves on arrays (physical cgs units).  u_new may alias
+ * u_old.  iters may be NULL. */
+int sph_cool_solve(sph_ctx *ctx, int32_t n, const double *rho, const double *u_old,
+                   const double *dt, double *u_new, int32_t *iters, int32_t host);
+
+/* ---- cooling-surrogate MLP 3->64->64->1 (GELU), BF16 weights ---- */
+/* parameters in FP32: W1[3*64] b1[64] W2[64*64] b2[64] W3[64] b3[1] and the
+ * input/output normalisation norm[8] = (mean[3], scale[3], y_mean, y_scale) */
+#define SPH_MLP_NPARAM (3 * 64 + 64 + 64 * 64 + 64 + 64 + 1)
+int sph_mlp_set(sph_ctx *ctx, const float *params, const float *norm, int32_t host);
+int sph_mlp_get(sph_ctx *ctx, float *params, float *norm, int32_t host);
+/* forward on n rows of normalised inputs X[n*3] -> y[n] (tensor cores) */
+int sph_mlp_forward(sph_ctx *ctx, int32_t n, const float *X, float *y, int32_t host);
+/* gradient of 0.5*mean((y - t)^2) over n rows -> grad[SPH_MLP_NPARAM], and
+ * the loss; forward+backward on tensor cores */
+int sph_mlp_grad(sph_ctx *ctx, int32_t n, const float *X, const float *t, float *grad,
+                 float *loss, int32_t host);
+/* nsteps of Adam (lr, b1, b2, eps) on minibatches of size batch drawn in
+ * order from device arrays X[n*3], t[n]; writes the mean loss of the last
+ * epoch to loss */
+int sph_mlp_train(sph_ctx *ctx, int32_t n, const float *X, const float *t, int32_t batch,
+                  int32_t nsteps, float lr, float *loss);
+
+/* ---- full step ---- */
+/* The prologue of the reference loop (sph_mpi4_v4.py:106-265): h, rho, forces,
+ * gravity, du/dt, u += du/dt dt, and the first dt. */
+int sph_prologue(sph_ctx *ctx);
+/* nsteps of kick-drift-(sort, tree, h, lists, rho, div/curl, forces | gravity)
+ * -kick-du/dt-u-[cooling]-dt (sph_mpi4_v4.py:278-442; EVR.cu:1139-1782),
+ * replayed from a CUDA graph unless SPH_FLAG_NO_GRAPH. */
+int sph_step(sph_ctx *ctx, int32_t nsteps);
+
+/* ---- measurement ---- */
+/* Phase durations of the last sph_step (needs SPH_FLAG_TIMING), in ms:
+ * [kick+drift, sort, tree, h, lists, density, div/curl, forces, wait+kick,
+ *  du/dt, u(+cooling)+dt, gravity (own stream)]; returns the count (12). */
+#define SPH_NPHASE 12
+int sph_get_phase_times(sph_ctx *ctx, float *ms);
+/* kernel nodes in the captured step graph (0 before the first graph step) */
+int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
+/* FP32 FMA throughput of this GPU measured by a dependent-chain kernel,
+ * TFLOP/s (2 flops per FMA), the denominator for FP32-bound kernels */
+int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
+
+/* The same entry points a single GPU runs, for a rank of a multi-GPU job
+ * that owns a slice of the ensemble: nothing here talks to other ranks. */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_B200_H */

@@ -555,9 +555,12 @@ int orc_newton_h(int N, const double *x, const double *y, const double *z, const
             if (f < 0.0) lo = h; else hi = h;
             double hn;
             if (fp > 0.0) hn = h - f / fp; else hn = -1.0;
+            /* at most a factor 1.25 per iteration */
+            if (hn > 1.25 * h) hn = 1.25 * h;
+            if (hn > 0.0 && hn < h / 1.25) hn = h / 1.25;
             if (!(hn > lo && hn < hi)) {
-                if (hi == INFINITY) hn = 1.26 * h;
-                else if (lo == 0.0) hn = h / 1.26;
+                if (hi == INFINITY) hn = 1.25 * h;
+                else if (lo == 0.0) hn = h / 1.25;
                 else hn = 0.5 * (lo + hi);
             }
             double dh = hn - h;

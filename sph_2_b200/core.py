@@ -1,0 +1,329 @@
+"""Host side of the B200 SPH step: a thin owner of one libsphb200 context.
+
+The methods keep the reference's step-level vocabulary (smoothing length,
+density, div/curl, SPH acceleration, du/dt, gravity, kick/drift; see
+MPI_sph/sph_code/sph_mpi4_v4.py:278-442 for the reference's loop) and move
+NumPy arrays in and out in the caller's original particle order.  All compute
+runs in the CUDA library; nothing here computes physics.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import asdict, dataclass, field, fields
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class Config:
+    """Mirror of ``sph_config`` (include/sph_b200.h); defaults follow the
+    Evrard workload: N_ngb = 64, Monaghan-Gingold viscosity alpha = 1,
+    beta = 2, eta = 0.1 (sph_mpi4_v4.py:22-26), Plummer eps = 1e-2,
+    theta = 0.5, Courant 0.25, gamma = 5/3, G = 1."""
+    n_max: int = 1 << 20
+    n_cloud_max: int = 1
+    precision: str = "mixed"
+    av_mode: str = "mg83"
+    balsara: bool = False
+    leaf_size: int = 16
+    ngb_lanes: int = 8
+    block_size: int = 256
+    max_ngb: int = 256
+    h_max_iter: int = 64
+    flags: int = 0
+    walk_warps: int = 4
+    n_ngb: float = 64.0
+    h_tol: float = 1e-3
+    gamma: float = 5.0 / 3.0
+    alpha: float = 1.0
+    beta: float = 2.0
+    eta: float = 0.1
+    G: float = 1.0
+    eps: float = 1e-2
+    theta: float = 0.5
+    courant: float = 0.25
+    dt_max: float = 0.0
+    dt_fixed: float = 0.0
+
+    def to_c(self) -> L.SphConfig:
+        c = L.SphConfig()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if f.name == "precision":
+                v = L.PREC[v]
+            elif f.name == "av_mode":
+                v = L.AV[v]
+            elif f.name == "balsara":
+                v = int(bool(v))
+            setattr(c, f.name, v)
+        return c
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One device context (capacity n_max particles, n_cloud_max clouds)."""
+
+    def __init__(self, config: Config | None = None, **kw):
+        self.config = config or Config(**kw)
+        self._L = L.load()
+        self._h = C.c_void_p()
+        cfg = self.config.to_c()
+        L.check(self._L.sph_ctx_create(C.byref(cfg), C.byref(self._h)), "sph_ctx_create")
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self._h:
+            self._L.sph_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc, where):
+        return L.check(rc, where, self._h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def n(self) -> int:
+        return self._L.sph_count(self._h)
+
+    @property
+    def n_clouds(self) -> int:
+        return self._L.sph_cloud_count(self._h)
+
+    def device_bytes(self) -> int:
+        return int(self._L.sph_device_bytes(self._h))
+
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            setattr(self.config, k, v)
+        cfg = self.config.to_c()
+        self._chk(self._L.sph_set_params(self._h, C.byref(cfg)), "sph_set_params")
+
+    # -- data ---------------------------------------------------------------
+    def load(self, pos, vel=None, m=None, h=None, u=None, cloud=None):
+        pos = _f64(pos)
+        n = pos.shape[0]
+        x, y, z = (_f64(pos[:, k]) for k in range(3))
+        vel = np.zeros((n, 3)) if vel is None else _f64(vel)
+        vx, vy, vz = (_f64(vel[:, k]) for k in range(3))
+        m = _f64(np.full(n, 1.0 / max(n, 1)) if m is None else m)
+        h = _f64(np.full(n, 0.05) if h is None else h)
+        u = _f64(np.zeros(n) if u is None else u)
+        cl = None if cloud is None else np.ascontiguousarray(cloud, dtype=np.int32)
+        self._keep = (x, y, z, vx, vy, vz, m, h, u, cl)
+        self._chk(self._L.sph_load(self._h, n, _ptr(cl), _ptr(x), _ptr(y), _ptr(z), _ptr(vx),
+                                   _ptr(vy), _ptr(vz), _ptr(m), _ptr(h), _ptr(u), 1), "sph_load")
+
+    def get(self, name: str, storage_order=False) -> np.ndarray:
+        out = np.zeros(self.n)
+        self._chk(self._L.sph_get_field(self._h, L.FIELD[name], _ptr(out), 1, int(storage_order)),
+                  f"get {name}")
+        return out
+
+    def set(self, name: str, arr, storage_order=False):
+        a = _f64(arr)
+        self._chk(self._L.sph_set_field(self._h, L.FIELD[name], _ptr(a), 1, int(storage_order)),
+                  f"set {name}")
+
+    def get_pos(self, storage_order=False):
+        return np.stack([self.get(k, storage_order) for k in "xyz"], 1)
+
+    def get_vel(self, storage_order=False):
+        return np.stack([self.get(k, storage_order) for k in ("vx", "vy", "vz")], 1)
+
+    def get_acc(self, which="sph", storage_order=False):
+        return np.stack([self.get(f"a{k}_{which}", storage_order) for k in "xyz"], 1)
+
+    def ids(self) -> np.ndarray:
+        out = np.zeros(self.n, np.int32)
+        self._chk(self._L.sph_get_ids(self._h, _ptr(out), 1), "ids")
+        return out
+
+    def status(self, reset=False) -> dict:
+        out = np.zeros(8, np.int64)
+        self._chk(self._L.sph_get_status(self._h, _ptr(out), int(reset)), "status")
+        return dict(zip(L.STATUS, out.tolist()))
+
+    @property
+    def dt(self) -> np.ndarray:
+        out = np.zeros(max(self.n_clouds, 1))
+        self._chk(self._L.sph_get_dt(self._h, _ptr(out)), "dt")
+        return out
+
+    @dt.setter
+    def dt(self, v):
+        a = _f64(np.broadcast_to(v, (max(self.n_clouds, 1),)))
+        self._chk(self._L.sph_set_dt(self._h, _ptr(a)), "set dt")
+
+    # -- phases -------------------------------------------------------------
+    def sort(self):
+        self._chk(self._L.sph_sort(self._h), "sph_sort")
+
+    def sort_info(self):
+        keys = np.zeros(self.n, np.uint64)
+        perm = np.zeros(self.n, np.int32)
+        self._chk(self._L.sph_get_sort(self._h, _ptr(keys), _ptr(perm), 1), "sort_info")
+        return keys, perm
+
+    def build_tree(self):
+        self._chk(self._L.sph_build_tree(self._h), "sph_build_tree")
+
+    def tree(self):
+        nn = 2 * self.n - 1
+        node = np.zeros((nn, 16))
+        child = np.zeros(2 * nn, np.int32)
+        first = np.zeros(nn, np.int32)
+        last = np.zeros(nn, np.int32)
+        r2 = np.zeros(nn)
+        hmax = np.zeros(nn)
+        self._chk(self._L.sph_get_tree(self._h, _ptr(node), _ptr(child), _ptr(first), _ptr(last),
+                                       _ptr(r2), _ptr(hmax), 1), "tree")
+        return dict(node=node, child=child, first=first, last=last, open_r2=r2, hmax=hmax)
+
+    def smoothing_h(self):
+        self._chk(self._L.sph_smoothing_h(self._h), "sph_smoothing_h")
+
+    def neighbours(self):
+        self._chk(self._L.sph_neighbours(self._h), "sph_neighbours")
+
+    def neighbour_lists(self):
+        """Canonical CSR over storage order, rows sorted ascending."""
+        off = np.zeros(self.n + 1, np.int64)
+        self._chk(self._L.sph_get_neighbours(self._h, _ptr(off), None, 0, 1), "ngb count")
+        lst = np.zeros(max(int(off[-1]), 1), np.int32)
+        self._chk(self._L.sph_get_neighbours(self._h, _ptr(off), _ptr(lst), len(lst), 1),
+                  "ngb lists")
+        return off, lst[: off[-1]]
+
+    def density(self):
+        self._chk(self._L.sph_density(self._h), "sph_density")
+
+    def divcurl(self):
+        self._chk(self._L.sph_divcurl(self._h), "sph_divcurl")
+
+    def forces(self):
+        self._chk(self._L.sph_forces(self._h), "sph_forces")
+
+    def dudt(self):
+        self._chk(self._L.sph_dudt(self._h), "sph_dudt")
+
+    def gravity(self):
+        self._chk(self._L.sph_gravity(self._h), "sph_gravity")
+
+    def gravity_direct(self, targets):
+        """FP64 Plummer direct sum onto storage indices -> (acc[n,3], pot[n])."""
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        out = np.zeros(4 * len(t))
+        self._chk(self._L.sph_gravity_direct(self._h, len(t), _ptr(t), _ptr(out), 1),
+                  "gravity_direct")
+        out = out.reshape(-1, 4)
+        return out[:, :3].copy(), out[:, 3].copy()
+
+    def gravity_direct_spline(self, eps, targets):
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        e = _f64(eps)
+        out = np.zeros(3 * len(t))
+        self._chk(self._L.sph_gravity_direct_spline(self._h, _ptr(e), len(t), _ptr(t), _ptr(out), 1),
+                  "gravity_direct_spline")
+        return out.reshape(-1, 3)
+
+    def counters(self):
+        out = np.zeros(2, np.int64)
+        self._chk(self._L.sph_get_counters(self._h, _ptr(out)), "counters")
+        return {"cells": int(out[0]), "particles": int(out[1])}
+
+    def kick(self, fac=0.5):
+        self._chk(self._L.sph_kick(self._h, fac), "sph_kick")
+
+    def drift(self):
+        self._chk(self._L.sph_drift(self._h), "sph_drift")
+
+    def update_u(self, first=False):
+        self._chk(self._L.sph_update_u(self._h, int(first)), "sph_update_u")
+
+    def cfl_dt(self):
+        out = np.zeros(max(self.n_clouds, 1))
+        self._chk(self._L.sph_cfl_dt(self._h, _ptr(out)), "sph_cfl_dt")
+        return out
+
+    def energies(self) -> dict:
+        out = np.zeros(10)
+        self._chk(self._L.sph_energies(self._h, _ptr(out)), "sph_energies")
+        keys = ["KE", "U", "PE", "px", "py", "pz", "Lx", "Ly", "Lz", "M"]
+        return dict(zip(keys, out.tolist()))
+
+    def prologue(self):
+        self._chk(self._L.sph_prologue(self._h), "sph_prologue")
+
+    def step(self, nsteps=1):
+        self._chk(self._L.sph_step(self._h, nsteps), "sph_step")
+
+    def phase_times(self) -> dict:
+        ms = (C.c_float * 12)()
+        rc = self._L.sph_get_phase_times(self._h, ms)
+        if rc < 0:
+            L.check(rc, "phase_times", self._h)
+        return dict(zip(L.PHASES, [float(v) for v in ms]))
+
+    def graph_kernel_count(self) -> int:
+        c = C.c_int32()
+        self._chk(self._L.sph_graph_kernel_count(self._h, C.byref(c)), "graph_kernel_count")
+        return int(c.value)
+
+    def fp32_peak_tflops(self) -> float:
+        v = C.c_double()
+        self._chk(self._L.sph_measure_fp32_peak(self._h, C.byref(v)), "fp32 peak")
+        return float(v.value)
+
+    def sync(self):
+        self._chk(self._L.sph_sync(self._h), "sph_sync")
+
+    def set_stream(self, stream_handle: int):
+        """Queue all work on an existing CUDA stream (e.g. a torch stream's
+        ``cuda_stream``); the library stops using its own stream."""
+        self._chk(self._L.sph_set_stream(self._h, C.c_void_p(stream_handle)), "sph_set_stream")
+
+    # -- cooling --------------------------------------------------------------
+    def cooling_setup(self, params: dict, log_lambda):
+        p = L.SphCoolingParams()
+        for k, v in params.items():
+            setattr(p, k, v)
+        ll = _f64(log_lambda)
+        self._chk(self._L.sph_cooling_setup(self._h, C.byref(p), _ptr(ll)), "cooling_setup")
+
+    def cooling_exact(self):
+        self._chk(self._L.sph_cooling_exact(self._h), "cooling_exact")
+
+    def cooling_mlp(self):
+        self._chk(self._L.sph_cooling_mlp(self._h), "cooling_mlp")
+
+    def cool_solve(self, rho, u_old, dt):
+        rho, u_old = _f64(rho), _f64(u_old)
+        dt = _f64(np.broadcast_to(dt, rho.shape))
+        out = np.zeros_like(rho)
+        it = np.zeros(len(rho), np.int32)
+        self._chk(self._L.sph_cool_solve(self._h, len(rho), _ptr(rho), _ptr(u_old), _ptr(dt),
+                                         _ptr(out), _ptr(it), 1), "cool_solve")
+        return out, it

@@ -1,0 +1,890 @@
+// capi.cu -- the extern "C" boundary of libsphb200.so (include/sph_b200.h):
+// context lifetime, device memory (allocated once at context creation; the
+// reference allocates and frees the neighbour list and tree every step,
+// EVR.cu:1148, 1417-1446), field transfer in original particle order, the
+// phase entry points, the prologue and the CUDA-graph step.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "sph_internal.cuh"
+
+int ctx_fail(sph_ctx *ctx, cudaError_t e, const char *what, int line) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s failed (%s) at capi line %d", what, cudaGetErrorString(e), line);
+    if (ctx) ctx->err = buf;
+    return e == cudaErrorMemoryAllocation ? SPH_ERR_NOMEM : SPH_ERR_CUDA;
+}
+
+int ctx_check_launch(sph_ctx *ctx, const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_fail(ctx, e, what, 0);
+    return SPH_OK;
+}
+
+int launch_dt_commit(sph_ctx *ctx);
+
+namespace {
+
+template <class T>
+int dalloc(sph_ctx *ctx, T **p, size_t count) {
+    size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaMalloc", __LINE__);
+    ctx->allocs.push_back(q);
+    ctx->dev_bytes += (int64_t)bytes;
+    *p = (T *)q;
+    return SPH_OK;
+}
+
+#define DA(ptr, count)                          \
+    do {                                        \
+        int r_ = dalloc(ctx, &(ptr), (count));  \
+        if (r_) return r_;                      \
+    } while (0)
+
+__global__ void k_iota(int n, int *a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+__global__ void k_scatter_by_id(int n, const int *__restrict__ id, const double *__restrict__ src,
+                                double *__restrict__ dst) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[id[s]] = src[s];
+}
+__global__ void k_gather_by_id(int n, const int *__restrict__ id, const double *__restrict__ src,
+                               double *__restrict__ dst) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[s] = src[id[s]];
+}
+
+bool valid_lanes(int l) { return l == 4 || l == 8 || l == 16 || l == 32; }
+
+int check_cfg(const sph_config *c) {
+    if (c->n_max < 1 || c->n_cloud_max < 1) return SPH_ERR_ARG;
+    if (c->n_cloud_max > (1 << 20)) return SPH_ERR_ARG;
+    if (c->precision != SPH_PREC_FP64 && c->precision != SPH_PREC_MIXED) return SPH_ERR_ARG;
+    if (c->av_mode != SPH_AV_MG83 && c->av_mode != SPH_AV_GADGET) return SPH_ERR_ARG;
+    if (c->leaf_size < 1 || c->leaf_size > 64) return SPH_ERR_ARG;
+    if (!valid_lanes(c->ngb_lanes)) return SPH_ERR_ARG;
+    if (c->block_size < 64 || c->block_size > 1024 || c->block_size % 32) return SPH_ERR_ARG;
+    if (c->max_ngb < 32 || c->max_ngb > 512) return SPH_ERR_ARG;
+    if (c->h_max_iter < 1 || c->h_max_iter > 1000) return SPH_ERR_ARG;
+    if (!(c->theta > 0.0 && c->theta <= 1.0)) return SPH_ERR_ARG;
+    if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
+    if (!(c->courant > 0.0)) return SPH_ERR_ARG;
+    return SPH_OK;
+}
+
+double *field_ptr(sph_ctx *ctx, int f) {
+    const int c = ctx->cur;
+    const size_t n = ctx->n;
+    switch (f) {
+        case SPH_F_X: return ctx->st[c][ST_X];
+        case SPH_F_Y: return ctx->st[c][ST_Y];
+        case SPH_F_Z: return ctx->st[c][ST_Z];
+        case SPH_F_VX: return ctx->st[c][ST_VX];
+        case SPH_F_VY: return ctx->st[c][ST_VY];
+        case SPH_F_VZ: return ctx->st[c][ST_VZ];
+        case SPH_F_M: return ctx->st[c][ST_M];
+        case SPH_F_H: return ctx->st[c][ST_H];
+        case SPH_F_U: return ctx->st[c][ST_U];
+        case SPH_F_U_PREV: return ctx->st[c][ST_U];
+        case SPH_F_DUDT_PREV: return ctx->st[c][ST_DUDT_PREV];
+        case SPH_F_RHO: return ctx->rho;
+        case SPH_F_P: return ctx->P;
+        case SPH_F_C: return ctx->c;
+        case SPH_F_DIVV: return ctx->divV;
+        case SPH_F_CURLV: return ctx->curlV;
+        case SPH_F_AX_SPH: return ctx->asph;
+        case SPH_F_AY_SPH: return ctx->asph + n;
+        case SPH_F_AZ_SPH: return ctx->asph + 2 * n;
+        case SPH_F_AX_GRAV: return ctx->agrav;
+        case SPH_F_AY_GRAV: return ctx->agrav + n;
+        case SPH_F_AZ_GRAV: return ctx->agrav + 2 * n;
+        case SPH_F_DUDT: return ctx->dudt;
+        case SPH_F_VSIG: return ctx->vsig;
+        case SPH_F_POT: return ctx->pot;
+        default: return nullptr;
+    }
+}
+
+void drop_graphs(sph_ctx *ctx) {
+    for (int k = 0; k < 2; k++)
+        if (ctx->graph[k]) {
+            cudaGraphExecDestroy(ctx->graph[k]);
+            ctx->graph[k] = nullptr;
+        }
+    ctx->graph_valid = false;
+}
+
+int enter(sph_ctx *ctx) {
+    if (!ctx) return SPH_ERR_ARG;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaSetDevice", __LINE__);
+    return SPH_OK;
+}
+
+int ensure_timing(sph_ctx *ctx) {
+    if (ctx->tev_ok) return SPH_OK;
+    for (int k = 0; k < 16; k++) CK(cudaEventCreate(&ctx->tev[k]));
+    ctx->tev_ok = true;
+    return SPH_OK;
+}
+
+#define MARK(k, strm)                                                          \
+    do {                                                                       \
+        if (timing) CK(cudaEventRecord(ctx->tev[k], (strm)));                  \
+    } while (0)
+
+// the body of one step, queued on ctx->stream
+int step_body(sph_ctx *ctx) {
+    int rc;
+    const bool fused = ctx->cfg.flags & SPH_FLAG_DUDT_FUSED;
+    const bool pot = ctx->cfg.flags & SPH_FLAG_POTENTIAL;
+    const bool timing = ctx->cfg.flags & SPH_FLAG_TIMING;
+    if (timing && (rc = ensure_timing(ctx))) return rc;
+    MARK(0, ctx->stream);
+    if ((rc = launch_kick_drift(ctx))) return rc;
+    MARK(1, ctx->stream);
+    if ((rc = launch_sort(ctx))) return rc;
+    MARK(2, ctx->stream);
+    if ((rc = launch_tree(ctx))) return rc;
+    MARK(3, ctx->stream);
+    // gravity depends only on the tree: run it beside the SPH passes
+    CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->stream_g, ctx->ev_fork, 0));
+    MARK(13, ctx->stream_g);
+    if ((rc = launch_gravity(ctx, ctx->stream_g, pot))) return rc;
+    MARK(14, ctx->stream_g);
+    CK(cudaEventRecord(ctx->ev_join, ctx->stream_g));
+    if ((rc = launch_smoothing_h(ctx))) return rc;
+    MARK(4, ctx->stream);
+    if ((rc = launch_neighbours(ctx))) return rc;
+    MARK(5, ctx->stream);
+    if ((rc = launch_density(ctx))) return rc;
+    MARK(6, ctx->stream);
+    if ((rc = launch_divcurl(ctx))) return rc;
+    MARK(7, ctx->stream);
+    if ((rc = launch_forces(ctx, true, fused, false))) return rc;
+    MARK(8, ctx->stream);
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    if ((rc = launch_kick(ctx, 0.5, ctx->cfg.dt_fixed <= 0.0))) return rc;
+    MARK(9, ctx->stream);
+    if (!fused)
+        if ((rc = launch_forces(ctx, false, true, false))) return rc;
+    MARK(10, ctx->stream);
+    if ((rc = launch_update_u(ctx, false))) return rc;
+    if (ctx->cfg.flags & SPH_FLAG_COOLING) {
+        if (ctx->cfg.flags & SPH_FLAG_COOLING_MLP) rc = launch_cooling_mlp(ctx);
+        else rc = launch_cooling_exact(ctx);
+        if (rc) return rc;
+    }
+    rc = launch_dt_commit(ctx);
+    MARK(11, ctx->stream);
+    return rc;
+}
+
+__global__ void k_fma_peak(float *out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1234.5f) out[0] = s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_default_config(sph_config *c) {
+    if (!c) return SPH_ERR_ARG;
+    memset(c, 0, sizeof *c);
+    c->n_max = 1 << 20;
+    c->n_cloud_max = 1;
+    c->precision = SPH_PREC_MIXED;
+    c->av_mode = SPH_AV_MG83;
+    c->balsara = 0;
+    c->leaf_size = 16;
+    c->ngb_lanes = 8;
+    c->block_size = 256;
+    c->max_ngb = 256;
+    c->h_max_iter = 64;
+    c->flags = 0;
+    c->walk_warps = 4;
+    c->n_ngb = 64.0;
+    c->h_tol = 1e-3;
+    c->gamma = 5.0 / 3.0;
+    c->alpha = 1.0;
+    c->beta = 2.0;
+    c->eta = 0.1;
+    c->G = 1.0;
+    c->eps = 1e-2;
+    c->theta = 0.5;
+    c->courant = 0.25;
+    c->dt_max = 0.0;
+    c->dt_fixed = 0.0;
+    return SPH_OK;
+}
+
+int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
+    if (!cfg || !out) return SPH_ERR_ARG;
+    *out = nullptr;
+    int rc = check_cfg(cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SPH_ERR_CUDA;
+    sph_ctx *ctx = new sph_ctx();
+    ctx->cfg = *cfg;
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    auto fail = [&](int r) {
+        sph_ctx_destroy(ctx);
+        return r;
+    };
+    const size_t N = cfg->n_max, NN = 2 * N, K = cfg->max_ngb, C = cfg->n_cloud_max;
+    const size_t rs = cfg->precision == SPH_PREC_MIXED ? 16 : 32;  // Real4 bytes
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(SPH_ERR_CUDA);
+    ctx->own_stream = true;
+    if (cudaStreamCreateWithFlags(&ctx->stream_g, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(SPH_ERR_CUDA);
+    cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+#define DAF(ptr, count)                            \
+    do {                                           \
+        int r_ = dalloc(ctx, &(ptr), (count));     \
+        if (r_) return fail(r_);                   \
+    } while (0)
+    for (int b = 0; b < 2; b++) {
+        for (int k = 0; k < ST_N; k++) DAF(ctx->st[b][k], N);
+        DAF(ctx->id[b], N);
+        DAF(ctx->cloud[b], N);
+    }
+    DAF(ctx->rho, N); DAF(ctx->P, N); DAF(ctx->c, N); DAF(ctx->divV, N); DAF(ctx->curlV, N);
+    DAF(ctx->asph, 3 * N); DAF(ctx->agrav, 3 * N);
+    DAF(ctx->dudt, N); DAF(ctx->vsig, N); DAF(ctx->pot, N);
+    DAF(ctx->p0, N);
+    unsigned char *tmpb;
+    DAF(tmpb, rs * N); ctx->p1 = tmpb;
+    DAF(tmpb, rs * N); ctx->p2 = tmpb;
+    DAF(tmpb, rs * N); ctx->pw = tmpb;
+    DAF(ctx->key[0], N); DAF(ctx->key[1], N); DAF(ctx->key_in, N);
+    DAF(ctx->val[0], N); DAF(ctx->val[1], N);
+    ctx->sort_blocks = div_up(N, 2048);
+    DAF(ctx->hist, 256 * (size_t)ctx->sort_blocks + 256);
+    DAF(ctx->box, 6 * C);
+    DAF(ctx->cloud_start, C + 1);
+    DAF(ctx->child, 2 * NN); DAF(ctx->parent, NN); DAF(ctx->first, NN); DAF(ctx->last, NN);
+    DAF(ctx->flag, NN);
+    DAF(ctx->node, 16 * NN); DAF(ctx->hmax, NN); DAF(ctx->ropen2, NN);
+    double4 *nb4;
+    DAF(nb4, 2 * NN); ctx->node_box = nb4;
+    DAF(tmpb, rs * NN); ctx->wA = tmpb;
+    DAF(tmpb, rs * NN); ctx->wB = tmpb;
+    DAF(tmpb, rs * NN); ctx->wC = tmpb;
+    DAF(ctx->croot, C);
+    const size_t G = N / 32 + C + 1;
+    DAF(ctx->gstart, G); DAF(ctx->gcount, G); DAF(ctx->groot_g, G);
+    DAF(ctx->ngb, K * N); DAF(ctx->ngb_cnt, N);
+    DAF(ctx->cand, K * N); DAF(ctx->cand_cnt, N);
+    DAF(ctx->retry, N); DAF(ctx->hcand, N);
+    DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
+    DAF(ctx->status, SPH_NSTATUS);
+    DAF(ctx->counters, 2);
+    DAF(ctx->work, 16);
+    DAF(ctx->red, std::max<size_t>(N, 8192));
+    if (cudaMemsetAsync(ctx->status, 0, SPH_NSTATUS * sizeof(long long), ctx->stream) ||
+        cudaMemsetAsync(ctx->pot, 0, N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->agrav, 0, 3 * N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->asph, 0, 3 * N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->dt_bits, 0xff, C * sizeof(unsigned long long), ctx->stream) ||
+        cudaMemsetAsync(ctx->dt, 0, C * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->divV, 0, N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->curlV, 0, N * sizeof(double), ctx->stream))
+        return fail(SPH_ERR_CUDA);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(SPH_ERR_CUDA);
+#undef DAF
+    *out = ctx;
+    return SPH_OK;
+}
+
+void sph_ctx_destroy(sph_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    drop_graphs(ctx);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream_g) cudaStreamSynchronize(ctx->stream_g);
+    for (void *p : ctx->allocs) cudaFree(p);
+    if (ctx->tev_ok)
+        for (int k = 0; k < 16; k++) cudaEventDestroy(ctx->tev[k]);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->stream_g) cudaStreamDestroy(ctx->stream_g);
+    delete ctx;
+}
+
+int sph_set_stream(sph_ctx *ctx, void *s) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = (cudaStream_t)s;
+    ctx->own_stream = false;
+    drop_graphs(ctx);
+    return SPH_OK;
+}
+
+int sph_sync(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+const char *sph_last_error(sph_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int sph_get_config(sph_ctx *ctx, sph_config *out) {
+    if (!ctx || !out) return SPH_ERR_ARG;
+    *out = ctx->cfg;
+    return SPH_OK;
+}
+
+int sph_set_params(sph_ctx *ctx, const sph_config *c) {
+    if (!ctx || !c) return SPH_ERR_ARG;
+    sph_config t = ctx->cfg;
+    t.av_mode = c->av_mode; t.balsara = c->balsara; t.flags = c->flags;
+    t.n_ngb = c->n_ngb; t.h_tol = c->h_tol; t.h_max_iter = c->h_max_iter;
+    t.gamma = c->gamma; t.alpha = c->alpha; t.beta = c->beta; t.eta = c->eta;
+    t.G = c->G; t.eps = c->eps; t.theta = c->theta; t.courant = c->courant;
+    t.dt_max = c->dt_max; t.dt_fixed = c->dt_fixed;
+    t.ngb_lanes = c->ngb_lanes; t.block_size = c->block_size; t.leaf_size = c->leaf_size;
+    int rc = check_cfg(&t);
+    if (rc) return rc;
+    if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size) ctx->tree_ok = false;
+    ctx->cfg = t;
+    drop_graphs(ctx);
+    ctx->p2_dirty = true;
+    return SPH_OK;
+}
+
+int64_t sph_device_bytes(sph_ctx *ctx) { return ctx ? ctx->dev_bytes : 0; }
+
+int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, const double *y,
+             const double *z, const double *vx, const double *vy, const double *vz,
+             const double *m, const double *h, const double *u, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!x || !y || !z || !m || !h || !u))) return SPH_ERR_ARG;
+    if (n > ctx->cfg.n_max) return SPH_ERR_CAPACITY;
+    drop_graphs(ctx);
+    CK(cudaStreamSynchronize(ctx->stream));
+    // clouds: counts per id on the host
+    std::vector<int> cl(n > 0 ? n : 1, 0);
+    if (cloud) {
+        if (host) memcpy(cl.data(), cloud, sizeof(int) * n);
+        else CK(cudaMemcpy(cl.data(), cloud, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    }
+    int ncl = 1;
+    for (int i = 0; i < n; i++) {
+        if (cl[i] < 0 || cl[i] >= ctx->cfg.n_cloud_max) return SPH_ERR_CAPACITY;
+        ncl = std::max(ncl, cl[i] + 1);
+    }
+    std::vector<int> cnt(ncl, 0);
+    for (int i = 0; i < n; i++) cnt[cl[i]]++;
+    ctx->cloud_start_h.assign(ncl + 1, 0);
+    for (int k = 0; k < ncl; k++) ctx->cloud_start_h[k + 1] = ctx->cloud_start_h[k] + cnt[k];
+    std::vector<int> gs, gc, gk;
+    for (int k = 0; k < ncl; k++)
+        for (int s = ctx->cloud_start_h[k]; s < ctx->cloud_start_h[k + 1]; s += 32) {
+            gs.push_back(s);
+            gc.push_back(std::min(32, ctx->cloud_start_h[k + 1] - s));
+            gk.push_back(k);
+        }
+    ctx->n = n;
+    ctx->ncloud = ncl;
+    ctx->ngroup = (int)gs.size();
+    ctx->cur = 0;
+    cudaStream_t s = ctx->stream;
+    cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const double *src[ST_N] = {x, y, z, vx, vy, vz, m, h, u, nullptr};
+    for (int k = 0; k < ST_N; k++) {
+        if (n == 0) break;
+        if (src[k]) CK(cudaMemcpyAsync(ctx->st[0][k], src[k], sizeof(double) * n, kind, s));
+        else CK(cudaMemsetAsync(ctx->st[0][k], 0, sizeof(double) * n, s));
+    }
+    if (n > 0) {
+        CK(cudaMemcpyAsync(ctx->cloud[0], cl.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        k_iota<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[0]);
+    }
+    CK(cudaMemcpyAsync(ctx->cloud_start, ctx->cloud_start_h.data(), sizeof(int) * (ncl + 1),
+                       cudaMemcpyHostToDevice, s));
+    if (ctx->ngroup) {
+        CK(cudaMemcpyAsync(ctx->gstart, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->gcount, gc.data(), sizeof(int) * gc.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->groot_g, gk.data(), sizeof(int) * gk.size(), cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaMemsetAsync(ctx->dt_bits, 0xff, sizeof(unsigned long long) * ncl, s));
+    {
+        std::vector<double> dt0(ncl, ctx->cfg.dt_fixed > 0 ? ctx->cfg.dt_fixed : 0.0);
+        CK(cudaMemcpyAsync(ctx->dt, dt0.data(), sizeof(double) * ncl, cudaMemcpyHostToDevice, s));
+    }
+    if (n > 0) {
+        CK(cudaMemsetAsync(ctx->asph, 0, 3 * sizeof(double) * n, s));
+        CK(cudaMemsetAsync(ctx->agrav, 0, 3 * sizeof(double) * n, s));
+        CK(cudaMemsetAsync(ctx->divV, 0, sizeof(double) * n, s));
+        CK(cudaMemsetAsync(ctx->curlV, 0, sizeof(double) * n, s));
+        CK(cudaMemsetAsync(ctx->pot, 0, sizeof(double) * n, s));
+        rc = launch_pack_p1(ctx);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(s));
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = false;
+    ctx->p2_dirty = true;
+    ctx->prologue_done = false;
+    ctx->step_count = 0;
+    return ctx_check_launch(ctx, "load");
+}
+
+int32_t sph_count(sph_ctx *ctx) { return ctx ? ctx->n : -1; }
+int32_t sph_cloud_count(sph_ctx *ctx) { return ctx ? ctx->ncloud : -1; }
+
+int sph_get_field(sph_ctx *ctx, int32_t field, double *out, int32_t host, int32_t storage_order) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    double *src = field_ptr(ctx, field);
+    if (!src || !out) return SPH_ERR_ARG;
+    const int n = ctx->n;
+    if (n == 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    const double *from = src;
+    if (!storage_order) {
+        k_scatter_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur], src, ctx->red);
+        from = ctx->red;
+    }
+    CK(cudaMemcpyAsync(out, from, sizeof(double) * n,
+                       host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "get_field");
+}
+
+int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host,
+                  int32_t storage_order) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    double *dst = field_ptr(ctx, field);
+    if (!dst || !in) return SPH_ERR_ARG;
+    const int n = ctx->n;
+    if (n == 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (storage_order) {
+        CK(cudaMemcpyAsync(dst, in, sizeof(double) * n, kind, s));
+    } else {
+        CK(cudaMemcpyAsync(ctx->red, in, sizeof(double) * n, kind, s));
+        k_gather_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur], ctx->red, dst);
+    }
+    if (field <= SPH_F_H) {
+        rc = launch_pack_p1(ctx);
+        if (rc) return rc;
+        if (field <= SPH_F_Z || field == SPH_F_M) ctx->tree_ok = false;
+    }
+    if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "set_field");
+}
+
+int sph_get_ids(sph_ctx *ctx, int32_t *out, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out) return SPH_ERR_ARG;
+    if (ctx->n == 0) return SPH_OK;
+    CK(cudaMemcpyAsync(out, ctx->id[ctx->cur], sizeof(int) * ctx->n,
+                       host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_get_status(sph_ctx *ctx, int64_t *out, int32_t reset) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaMemcpyAsync(out, ctx->status, sizeof(long long) * SPH_NSTATUS, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    if (reset) CK(cudaMemsetAsync(ctx->status, 0, sizeof(long long) * SPH_NSTATUS, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_get_dt(sph_ctx *ctx, double *dt) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!dt) return SPH_ERR_ARG;
+    CK(cudaMemcpyAsync(dt, ctx->dt, sizeof(double) * ctx->ncloud, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_set_dt(sph_ctx *ctx, const double *dt) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!dt) return SPH_ERR_ARG;
+    CK(cudaMemcpyAsync(ctx->dt, dt, sizeof(double) * ctx->ncloud, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_sort(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    drop_graphs(ctx);
+    rc = launch_sort(ctx);
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = false;
+    ctx->p2_dirty = true;
+    return rc;
+}
+
+int sph_get_sort(sph_ctx *ctx, uint64_t *keys, int32_t *perm, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    const int n = ctx->n;
+    if (n == 0) return SPH_OK;
+    cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (keys) CK(cudaMemcpyAsync(keys, ctx->key_in, sizeof(uint64_t) * n, k, ctx->stream));
+    if (perm) CK(cudaMemcpyAsync(perm, ctx->val[0], sizeof(int) * n, k, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_build_tree(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    return launch_tree(ctx);
+}
+
+int sph_get_tree(sph_ctx *ctx, double *node, int32_t *child, int32_t *first, int32_t *last,
+                 double *open_r2, double *hmax, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    const size_t nn = ctx->n > 0 ? 2 * (size_t)ctx->n - 1 : 0;
+    if (nn == 0) return SPH_OK;
+    cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    cudaStream_t s = ctx->stream;
+    if (node) CK(cudaMemcpyAsync(node, ctx->node, 16 * sizeof(double) * nn, k, s));
+    if (child) CK(cudaMemcpyAsync(child, ctx->child, 2 * sizeof(int) * nn, k, s));
+    if (first) CK(cudaMemcpyAsync(first, ctx->first, sizeof(int) * nn, k, s));
+    if (last) CK(cudaMemcpyAsync(last, ctx->last, sizeof(int) * nn, k, s));
+    if (open_r2) CK(cudaMemcpyAsync(open_r2, ctx->ropen2, sizeof(double) * nn, k, s));
+    if (hmax) CK(cudaMemcpyAsync(hmax, ctx->hmax, sizeof(double) * nn, k, s));
+    CK(cudaStreamSynchronize(s));
+    return SPH_OK;
+}
+
+int sph_smoothing_h(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    drop_graphs(ctx);
+    return launch_smoothing_h(ctx);
+}
+
+int sph_neighbours(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    return launch_neighbours(ctx);
+}
+
+int sph_get_neighbours(sph_ctx *ctx, int64_t *off, int32_t *lst, int64_t cap, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok) return SPH_ERR_STATE;
+    if (!off) return SPH_ERR_ARG;
+    const int n = ctx->n;
+    std::vector<int> cnt(n);
+    std::vector<long long> o(n + 1, 0);
+    if (n) CK(cudaMemcpyAsync(cnt.data(), ctx->ngb_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                              ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < n; i++) o[i + 1] = o[i] + cnt[i];
+    if (host) memcpy(off, o.data(), sizeof(long long) * (n + 1));
+    else CK(cudaMemcpy(off, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice));
+    if (!lst) return SPH_OK;
+    if (o[n] > cap) return SPH_ERR_CAPACITY;
+    long long *doff = nullptr;
+    int *dl = nullptr;
+    CK(cudaMalloc(&doff, sizeof(long long) * (n + 1)));
+    CK(cudaMalloc(&dl, sizeof(int) * std::max<long long>(o[n], 1)));
+    CK(cudaMemcpy(doff, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice));
+    rc = launch_export_neighbours(ctx, (int64_t *)doff, dl, o[n]);
+    if (!rc) {
+        CK(cudaMemcpyAsync(lst, dl, sizeof(int) * o[n],
+                           host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    cudaFree(doff);
+    cudaFree(dl);
+    return rc;
+}
+
+int sph_density(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok) return SPH_ERR_STATE;
+    return launch_density(ctx);
+}
+
+int sph_divcurl(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok) return SPH_ERR_STATE;
+    if (ctx->p2_dirty) {
+        rc = launch_repack_p2(ctx);
+        if (rc) return rc;
+    }
+    return launch_divcurl(ctx);
+}
+
+int sph_forces(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok) return SPH_ERR_STATE;
+    return launch_forces(ctx, true, (ctx->cfg.flags & SPH_FLAG_DUDT_FUSED) != 0, false);
+}
+
+int sph_dudt(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok) return SPH_ERR_STATE;
+    return launch_forces(ctx, false, true, false);
+}
+
+int sph_gravity(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    return launch_gravity(ctx, ctx->stream, (ctx->cfg.flags & SPH_FLAG_POTENTIAL) != 0);
+}
+
+static int direct_common(sph_ctx *ctx, const double *eps, int32_t nt, const int32_t *targets,
+                         double *out, int32_t host, int width) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (nt < 0 || (nt > 0 && (!targets || !out))) return SPH_ERR_ARG;
+    if (nt == 0) return SPH_OK;
+    for (int t = 0; host && t < nt; t++)
+        if (targets[t] < 0 || targets[t] >= ctx->n) return SPH_ERR_ARG;
+    int *dt_ = nullptr;
+    double *dout = nullptr, *deps = nullptr;
+    CK(cudaMalloc(&dt_, sizeof(int) * nt));
+    CK(cudaMalloc(&dout, sizeof(double) * width * nt));
+    cudaMemcpyKind kin = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpy(dt_, targets, sizeof(int) * nt, kin));
+    if (eps) {
+        CK(cudaMalloc(&deps, sizeof(double) * ctx->n));
+        CK(cudaMemcpy(deps, eps, sizeof(double) * ctx->n, kin));
+        // eps is given in the caller's original order: bring it to storage order
+        k_gather_by_id<<<div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->id[ctx->cur],
+                                                                      deps, ctx->red);
+        rc = launch_gravity_direct_spline(ctx, ctx->red, nt, dt_, dout);
+    } else {
+        rc = launch_gravity_direct(ctx, nt, dt_, dout);
+    }
+    if (!rc) {
+        CK(cudaMemcpyAsync(out, dout, sizeof(double) * width * nt,
+                           host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    cudaFree(dt_);
+    cudaFree(dout);
+    if (deps) cudaFree(deps);
+    return rc;
+}
+
+int sph_gravity_direct(sph_ctx *ctx, int32_t nt, const int32_t *targets, double *out, int32_t host) {
+    return direct_common(ctx, nullptr, nt, targets, out, host, 4);
+}
+
+int sph_gravity_direct_spline(sph_ctx *ctx, const double *eps, int32_t nt, const int32_t *targets,
+                              double *out, int32_t host) {
+    if (!eps) return SPH_ERR_ARG;
+    return direct_common(ctx, eps, nt, targets, out, host, 3);
+}
+
+int sph_kick(sph_ctx *ctx, double fac) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    return launch_kick(ctx, fac, false);
+}
+
+int sph_drift(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    ctx->tree_ok = ctx->lists_ok = false;
+    return launch_drift(ctx);
+}
+
+int sph_update_u(sph_ctx *ctx, int32_t first) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    return launch_update_u(ctx, first != 0);
+}
+
+int sph_cfl_dt(sph_ctx *ctx, double *dt) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = launch_cfl(ctx);
+    if (rc) return rc;
+    if (dt) return sph_get_dt(ctx, dt);
+    return SPH_OK;
+}
+
+int sph_energies(sph_ctx *ctx, double *out10) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out10) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    return launch_energies(ctx, out10);
+}
+
+int sph_get_counters(sph_ctx *ctx, int64_t *out2) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out2) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaMemcpyAsync(out2, ctx->counters, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int sph_prologue(sph_ctx *ctx) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    drop_graphs(ctx);
+    const bool pot = ctx->cfg.flags & SPH_FLAG_POTENTIAL;
+    ctx->prologue_done = false;
+    if ((rc = launch_sort(ctx))) return rc;
+    if ((rc = launch_tree(ctx))) return rc;
+    if ((rc = launch_gravity(ctx, ctx->stream, pot))) return rc;
+    if ((rc = launch_smoothing_h(ctx))) return rc;
+    if ((rc = launch_neighbours(ctx))) return rc;
+    if ((rc = launch_density(ctx))) return rc;
+    if ((rc = launch_divcurl(ctx))) return rc;
+    if ((rc = launch_forces(ctx, true, true, false))) return rc;
+    // first dt (fixed or Courant), then u += du/dt dt (sph_mpi4_v4.py:240-244)
+    if ((rc = launch_cfl(ctx))) return rc;
+    if ((rc = launch_update_u(ctx, true))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->prologue_done = true;
+    return ctx_check_launch(ctx, "prologue");
+}
+
+int sph_step(sph_ctx *ctx, int32_t nsteps) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (nsteps < 0) return SPH_ERR_ARG;
+    if (!ctx->prologue_done) return SPH_ERR_STATE;
+    if (ctx->n == 0) return SPH_OK;
+    const bool eager = ctx->cfg.flags & SPH_FLAG_NO_GRAPH;
+    for (int k = 0; k < nsteps; k++) {
+        if (eager) {
+            if ((rc = step_body(ctx))) return rc;
+        } else {
+            const int par = ctx->cur;
+            if (!ctx->graph[par]) {
+                cudaGraph_t g = nullptr;
+                CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                rc = step_body(ctx);
+                cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+                if (rc) {
+                    if (g) cudaGraphDestroy(g);
+                    ctx->cur = par;
+                    return rc;
+                }
+                if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
+                e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
+                {
+                    size_t nn = 0;
+                    cudaGraphGetNodes(g, nullptr, &nn);
+                    std::vector<cudaGraphNode_t> nodes(nn);
+                    if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+                    int kc = 0;
+                    for (size_t q = 0; q < nn; q++) {
+                        cudaGraphNodeType t;
+                        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
+                            t == cudaGraphNodeTypeKernel)
+                            kc++;
+                    }
+                    ctx->graph_kernels = kc;
+                }
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaGraphInstantiate", __LINE__);
+                ctx->cur = par;  // capture did not run anything: restore the parity
+            }
+            CK(cudaGraphLaunch(ctx->graph[par], ctx->stream));
+            ctx->cur = par ^ 1;
+        }
+        ctx->step_count++;
+    }
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;
+    return ctx_check_launch(ctx, "step");
+}
+
+int sph_get_phase_times(sph_ctx *ctx, float *ms) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ms) return SPH_ERR_ARG;
+    if (!ctx->tev_ok) return SPH_ERR_STATE;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 11; k++) CK(cudaEventElapsedTime(&ms[k], ctx->tev[k], ctx->tev[k + 1]));
+    CK(cudaEventElapsedTime(&ms[11], ctx->tev[13], ctx->tev[14]));
+    return SPH_NPHASE;
+}
+
+int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count) {
+    if (!ctx || !count) return SPH_ERR_ARG;
+    *count = ctx->graph_kernels;
+    return SPH_OK;
+}
+
+int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!tflops) return SPH_ERR_ARG;
+    const int blocks = ctx->num_sms * 8, threads = 256, iters = 4096;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float *dummy = (float *)ctx->red;
+    k_fma_peak<<<blocks, threads, 0, ctx->stream>>>(dummy, 64, 0.999f, 0.001f);  // warm-up
+    CK(cudaEventRecord(a, ctx->stream));
+    k_fma_peak<<<blocks, threads, 0, ctx->stream>>>(dummy, iters, 0.999f, 0.001f);
+    CK(cudaEventRecord(b, ctx->stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return ctx_check_launch(ctx, "fp32_peak");
+}
+
+}  // extern "C"

@@ -1,0 +1,397 @@
+// gravity.cu -- Barnes-Hut walk (monopole + quadrupole, Plummer softening)
+// and FP64 direct summation.
+//
+// Replaces compute_forces_kernel (bh_tree_iteration_v2.h:454-588): one warp
+// stack per warp of 64 entries, a per-thread __all_sync opening vote with
+// dp = 0.25 depth (theta_eff ~ 0.707), monopole only, spline softening with
+// eps_i only, G = 1.  And the O(N^2) direct sums acc_g (hfvCLibs_v7_hfv_v2.h:
+// 532-584) / getAcc_g_smth_mimj_mpi (MPI_sph/sph_code/libsx.py:910-947).
+//
+// Walk: a persistent kernel; each warp takes groups of 32 consecutive
+// Morton-ordered particles from a work counter.  The warp walks the tree 32
+// nodes per round (LIFO stack in shared memory) testing each node against the
+// group's box: a node is accepted when the squared distance from its centre of
+// mass to the box is >= r_open^2 (r_open = l/theta + |com - box centre|),
+// opened otherwise; opened buckets (<= leaf_size particles) go to a particle
+// list.  Accepted nodes and bucket particles are staged 32 at a time in shared
+// memory and every lane evaluates all 32 against its own particle, so the
+// interaction loop is branch-free FP32 (mixed) or FP64 (plain) FMA work with
+// one reciprocal square root per interaction.  Each 32-term chunk is summed
+// plainly and folded into a Kahan accumulator (mixed).
+#include "sph_internal.cuh"
+
+namespace {
+
+constexpr int WALK_WARPS = 4;
+constexpr int WSTK = 2048;
+constexpr unsigned FULL = 0xffffffffu;
+
+template <class R> __device__ __forceinline__ R rsq(R x);
+template <> __device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double rsq<double>(double x) { return rsqrt(x); }
+
+template <class R> struct WalkSmem {
+    int stk[WSTK];
+    int clist[64];
+    int plist[96];
+    typename R4<R>::T sa[32], sb[32], sc[32];
+};
+
+template <class R> __device__ __forceinline__ R wmin(R v) {
+    for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+template <class R> __device__ __forceinline__ R wmax(R v) {
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+// squared distance from point c to the box, rounding as the oracle's box_dist2
+__device__ __forceinline__ double box_d2(double x0, double y0, double z0, double x1, double y1,
+                                         double z1, double cx, double cy, double cz) {
+    double a, b, v, tx, ty, tz;
+    a = xsub(x0, cx); b = xsub(cx, x1); v = a > b ? a : b; tx = v > 0.0 ? v : 0.0;
+    a = xsub(y0, cy); b = xsub(cy, y1); v = a > b ? a : b; ty = v > 0.0 ? v : 0.0;
+    a = xsub(z0, cz); b = xsub(cz, z1); v = a > b ? a : b; tz = v > 0.0 ? v : 0.0;
+    double s = xadd(xmul(tx, tx), xmul(ty, ty));
+    return xadd(s, xmul(tz, tz));
+}
+__device__ __forceinline__ float box_d2(float x0, float y0, float z0, float x1, float y1, float z1,
+                                        float cx, float cy, float cz) {
+    float tx = fmaxf(fmaxf(x0 - cx, cx - x1), 0.f);
+    float ty = fmaxf(fmaxf(y0 - cy, cy - y1), 0.f);
+    float tz = fmaxf(fmaxf(z0 - cz, cz - z1), 0.f);
+    return tx * tx + ty * ty + tz * tz;
+}
+
+template <class R, bool POT>
+__global__ void __launch_bounds__(WALK_WARPS * 32)
+    k_walk(int ngroup, const int *__restrict__ gstart, const int *__restrict__ gcount,
+           const int *__restrict__ gcloud, const int *__restrict__ croot,
+           const typename R4<R>::T *__restrict__ pw, const typename R4<R>::T *__restrict__ wA,
+           const typename R4<R>::T *__restrict__ wB, const typename R4<R>::T *__restrict__ wC,
+           const int *__restrict__ first, const int *__restrict__ last,
+           const int *__restrict__ child, int leaf_size, R eps2, double G, int n,
+           double *__restrict__ agrav, double *__restrict__ pot, unsigned *work,
+           unsigned long long *counters, long long *status) {
+    typedef typename R4<R>::T V4;
+    __shared__ WalkSmem<R> smem[WALK_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WalkSmem<R> &S = smem[w];
+    const unsigned lt = (1u << lane) - 1u;
+    int maxsp = 0;
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(work, 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= ngroup) break;
+        const int s0 = gstart[g], gc = gcount[g];
+        const bool act = lane < gc;
+        const int i = s0 + (act ? lane : 0);
+        const V4 pi = pw[i];
+        const R bx0 = wmin<R>(act ? pi.x : R(INFINITY)), by0 = wmin<R>(act ? pi.y : R(INFINITY)),
+                bz0 = wmin<R>(act ? pi.z : R(INFINITY));
+        const R bx1 = wmax<R>(act ? pi.x : R(-INFINITY)), by1 = wmax<R>(act ? pi.y : R(-INFINITY)),
+                bz1 = wmax<R>(act ? pi.z : R(-INFINITY));
+        KSum<R> ax, ay, az, ph;
+        long long nC = 0, nP = 0;
+        int sp = 1, nc = 0, np = 0;
+        bool overflow = false;
+        if (lane == 0) S.stk[0] = croot[gcloud[g]];
+        __syncwarp();
+
+        auto flush_cells = [&](int m) {
+            if (lane < m) {
+                int nd = S.clist[lane];
+                S.sa[lane] = wA[nd];
+                S.sb[lane] = wB[nd];
+                S.sc[lane] = wC[nd];
+            }
+            __syncwarp();
+            R sx = 0, sy = 0, sz = 0, sp_ = 0;
+#pragma unroll 4
+            for (int k = 0; k < m; k++) {
+                const V4 a = S.sa[k], b = S.sb[k], c = S.sc[k];
+                const R dx = pi.x - a.x, dy = pi.y - a.y, dz = pi.z - a.z;
+                const R r2 = dx * dx + dy * dy + dz * dz + eps2;
+                const R rinv = rsq<R>(r2);
+                const R ri2 = rinv * rinv;
+                const R g3 = rinv * ri2, g5 = g3 * ri2, g7 = g5 * ri2;
+                const R qx = b.x * dx + c.x * dy + c.y * dz;
+                const R qy = c.x * dx + b.y * dy + c.z * dz;
+                const R qz = c.y * dx + c.z * dy + b.z * dz;
+                const R dqd = dx * qx + dy * qy + dz * qz;
+                const R tr = b.x + b.y + b.z;
+                const R s = -a.w * g3 + R(1.5) * tr * g5 - R(7.5) * dqd * g7;
+                const R t5 = R(3) * g5;
+                sx += s * dx + t5 * qx;
+                sy += s * dy + t5 * qy;
+                sz += s * dz + t5 * qz;
+                if (POT) sp_ -= a.w * rinv + R(0.5) * (R(3) * dqd * g5 - tr * g3);
+            }
+            ax.add(sx); ay.add(sy); az.add(sz);
+            if (POT) ph.add(sp_);
+            nC += m;
+            __syncwarp();
+        };
+        auto flush_parts = [&](int m) {
+            if (lane < m) S.sa[lane] = pw[S.plist[lane]];
+            __syncwarp();
+            R sx = 0, sy = 0, sz = 0, sp_ = 0;
+#pragma unroll 8
+            for (int k = 0; k < m; k++) {
+                const V4 a = S.sa[k];
+                const R dx = pi.x - a.x, dy = pi.y - a.y, dz = pi.z - a.z;
+                const R r2 = dx * dx + dy * dy + dz * dz + eps2;
+                const R rinv = rsq<R>(r2);
+                const R gg = a.w * rinv * rinv * rinv;
+                sx -= gg * dx;
+                sy -= gg * dy;
+                sz -= gg * dz;
+                if (POT) sp_ -= a.w * rinv;
+            }
+            ax.add(sx); ay.add(sy); az.add(sz);
+            if (POT) ph.add(sp_);
+            nP += m;
+            __syncwarp();
+        };
+
+        while (sp > 0 || nc > 0 || np > 0) {
+            if (sp > 0) {
+                const int take = min(sp, 32);
+                sp -= take;
+                int nd = 0, f = 0, cn = 0;
+                bool accept = false, open = false;
+                if (lane < take) {
+                    nd = S.stk[sp + lane];
+                    const V4 a = wA[nd];
+                    const R r2o = wB[nd].w;
+                    f = first[nd];
+                    cn = last[nd] - f + 1;
+                    const R d2 = box_d2(bx0, by0, bz0, bx1, by1, bz1, a.x, a.y, a.z);
+                    accept = d2 >= r2o && cn > 1;
+                    open = !accept;
+                }
+                __syncwarp();
+                const bool bucket = open && cn <= leaf_size;
+                const bool inner = open && cn > leaf_size;
+                // accepted cells
+                const unsigned am = __ballot_sync(FULL, accept);
+                if (accept) S.clist[nc + __popc(am & lt)] = nd;
+                nc += __popc(am);
+                // children of opened inner nodes
+                const unsigned im = __ballot_sync(FULL, inner);
+                const int npush = 2 * __popc(im);
+                if (sp + npush <= WSTK) {
+                    if (inner) {
+                        const int pos = sp + 2 * __popc(im & lt);
+                        S.stk[pos] = child[2 * nd + 1];
+                        S.stk[pos + 1] = child[2 * nd];
+                    }
+                    sp += npush;
+                    maxsp = max(maxsp, sp);
+                } else {
+                    overflow = true;
+                }
+                unsigned bm = __ballot_sync(FULL, bucket);
+                __syncwarp();
+                while (nc >= 32) {
+                    flush_cells(32);
+                    int v = S.clist[32 + lane];
+                    __syncwarp();
+                    if (lane + 32 < nc) S.clist[lane] = v;
+                    nc -= 32;
+                    __syncwarp();
+                }
+                while (bm) {
+                    const int src = __ffs(bm) - 1;
+                    bm &= bm - 1;
+                    const int ff = __shfl_sync(FULL, f, src), cc = __shfl_sync(FULL, cn, src);
+                    for (int b0 = 0; b0 < cc; b0 += 32)
+                        if (b0 + lane < cc) S.plist[np + b0 + lane] = ff + b0 + lane;
+                    np += cc;
+                    __syncwarp();
+                    while (np >= 32) {
+                        flush_parts(32);
+                        int v0 = S.plist[32 + lane], v1 = S.plist[64 + lane];
+                        __syncwarp();
+                        if (lane + 32 < np) S.plist[lane] = v0;
+                        if (lane + 64 < np) S.plist[32 + lane] = v1;
+                        np -= 32;
+                        __syncwarp();
+                    }
+                }
+            }
+            if (sp == 0) {
+                if (nc > 0) { flush_cells(nc); nc = 0; }
+                if (np > 0) { flush_parts(np); np = 0; }
+            }
+        }
+        if (act) {
+            const double self = POT ? (double)(pi.w * rsq<R>(eps2)) : 0.0;
+            agrav[i] = G * ax.value();
+            agrav[(size_t)n + i] = G * ay.value();
+            agrav[2 * (size_t)n + i] = G * az.value();
+            if (POT) pot[i] = G * (ph.value() + self);
+        }
+        if (lane == 0) {
+            atomicAdd(&counters[0], (unsigned long long)(nC * gc));
+            atomicAdd(&counters[1], (unsigned long long)(nP * gc));
+            if (overflow) status_add(status, SPH_S_STACK_OVERFLOW, 1);
+        }
+    }
+    if (lane == 0) atomicMax((unsigned long long *)&status[7], (unsigned long long)maxsp);
+}
+
+// FP64 Plummer direct sum onto targets from all particles of the same cloud
+__global__ void __launch_bounds__(256)
+    k_direct(int nt, const int *__restrict__ targets, const double4 *__restrict__ p0,
+             const double *__restrict__ m, const int *__restrict__ cloud,
+             const int *__restrict__ cstart, double eps2, double G, double *__restrict__ out) {
+    __shared__ double4 sh[256];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = t < nt;
+    const int i = ok ? targets[t] : targets[0];
+    // all targets of a block must share a cloud for the tiling; loop over the
+    // union of the clouds present (normally one)
+    const int ci = cloud[i];
+    const double4 pi = p0[i];
+    double ax = 0, ay = 0, az = 0, ph = 0;
+    int cmin = ci, cmax = ci;
+    for (int o = 16; o; o >>= 1) {
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    __shared__ int bmin, bmax;
+    if (threadIdx.x == 0) { bmin = 1 << 30; bmax = -1; }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) { atomicMin(&bmin, cmin); atomicMax(&bmax, cmax); }
+    __syncthreads();
+    const int j0 = cstart[bmin], j1 = cstart[bmax + 1];
+    for (int base = j0; base < j1; base += 256) {
+        const int j = base + threadIdx.x;
+        if (j < j1) {
+            double4 q = p0[j];
+            q.w = m[j];
+            sh[threadIdx.x] = q;
+        }
+        __syncthreads();
+        const int lim = min(256, j1 - base);
+        for (int k = 0; k < lim; k++) {
+            const int jj = base + k;
+            if (jj == i || cloud[jj] != ci) continue;
+            const double4 q = sh[k];
+            const double dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+            const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+            const double rinv = 1.0 / sqrt(r2);
+            const double gg = q.w * rinv * rinv * rinv;
+            ax -= gg * dx; ay -= gg * dy; az -= gg * dz;
+            ph -= q.w * rinv;
+        }
+        __syncthreads();
+    }
+    if (ok) {
+        out[4 * t] = G * ax; out[4 * t + 1] = G * ay; out[4 * t + 2] = G * az; out[4 * t + 3] = G * ph;
+    }
+}
+
+// spline-softened pair factor of libsx.py:924-934 (eps_ij = mean of eps)
+__device__ __forceinline__ double fk_spline(double rr, double e) {
+    const double q = rr / e;
+    const double inv_r3 = 1.0 / (rr * rr * rr);
+    if (q <= 1.0) return (1.0 / (e * e * e)) * ((4.0 / 3.0) - (6.0 / 5.0) * q * q + 0.5 * q * q * q);
+    if (q <= 2.0) {
+        const double q3 = q * q * q;
+        return inv_r3 * ((-1.0 / 15.0) + (8.0 / 3.0) * q3 - 3.0 * q3 * q + (6.0 / 5.0) * q3 * q * q -
+                         (1.0 / 6.0) * q3 * q3);
+    }
+    return inv_r3;
+}
+
+__global__ void __launch_bounds__(256)
+    k_direct_spline(int nt, const int *__restrict__ targets, const double4 *__restrict__ p0,
+                    const double *__restrict__ m, const double *__restrict__ eps, int n, double G,
+                    double *__restrict__ out) {
+    __shared__ double4 sh[256];
+    __shared__ double se[256];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = t < nt;
+    const int i = ok ? targets[t] : targets[0];
+    const double4 pi = p0[i];
+    const double ei = eps[i];
+    double ax = 0, ay = 0, az = 0;
+    for (int base = 0; base < n; base += 256) {
+        const int j = base + threadIdx.x;
+        if (j < n) {
+            double4 q = p0[j];
+            q.w = m[j];
+            sh[threadIdx.x] = q;
+            se[threadIdx.x] = eps[j];
+        }
+        __syncthreads();
+        const int lim = min(256, n - base);
+        for (int k = 0; k < lim; k++) {
+            if (base + k == i) continue;
+            const double4 q = sh[k];
+            const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+            const double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const double fk = fk_spline(rr, 0.5 * (ei + se[k]));
+            ax += fk * dx * q.w; ay += fk * dy * q.w; az += fk * dz * q.w;
+        }
+        __syncthreads();
+    }
+    if (ok) { out[3 * t] = G * ax; out[3 * t + 1] = G * ay; out[3 * t + 2] = G * az; }
+}
+
+template <class R, bool POT>
+int run_walk(sph_ctx *ctx, cudaStream_t s) {
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_walk<R, POT>,
+                                                          WALK_WARPS * 32, 0) != cudaSuccess ||
+            blocks_per_sm < 1)
+            blocks_per_sm = 1;
+    }
+    int grid = ctx->num_sms * blocks_per_sm;
+    grid = min(grid, div_up(ctx->ngroup, WALK_WARPS));
+    if (grid < 1) grid = 1;
+    const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
+    k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
+        ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
+        (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
+        (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->first,
+        ctx->last, ctx->child, ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
+        ctx->work, ctx->counters, ctx->status);
+    return SPH_OK;
+}
+
+}  // namespace
+
+int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot) {
+    if (ctx->n <= 0) return SPH_OK;
+    CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned), s));
+    CK(cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), s));
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED)
+        rc = pot ? run_walk<float, true>(ctx, s) : run_walk<float, false>(ctx, s);
+    else
+        rc = pot ? run_walk<double, true>(ctx, s) : run_walk<double, false>(ctx, s);
+    if (rc) return rc;
+    return ctx_check_launch(ctx, "gravity");
+}
+
+int launch_gravity_direct(sph_ctx *ctx, int nt, const int *targets, double *out) {
+    if (nt <= 0) return SPH_OK;
+    k_direct<<<div_up(nt, 256), 256, 0, ctx->stream>>>(nt, targets, ctx->p0, ctx->st[ctx->cur][ST_M],
+                                                       ctx->cloud[ctx->cur], ctx->cloud_start,
+                                                       ctx->cfg.eps * ctx->cfg.eps, ctx->cfg.G, out);
+    return ctx_check_launch(ctx, "gravity_direct");
+}
+
+int launch_gravity_direct_spline(sph_ctx *ctx, const double *eps, int nt, const int *targets,
+                                 double *out) {
+    if (nt <= 0) return SPH_OK;
+    k_direct_spline<<<div_up(nt, 256), 256, 0, ctx->stream>>>(
+        nt, targets, ctx->p0, ctx->st[ctx->cur][ST_M], eps, ctx->n, ctx->cfg.G, out);
+    return ctx_check_launch(ctx, "gravity_direct_spline");
+}

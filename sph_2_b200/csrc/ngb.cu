@@ -1,0 +1,370 @@
+// ngb.cu -- neighbour search over the radix tree and the Newton
+// smoothing-length iteration.
+//
+// Replaces ngbDB_new_v2 (ngb_v3.h:124-238: a per-thread scan of 27 cells of a
+// 10^3 grid, radius grown until 70-190 candidates, atomics-ordered output,
+// host exit on failure) and smoothing_h_ngb (hfvCLibs_v7_hfv_v2.h:367-455: a
+// count-based +-coeff*2h iteration of up to 200 rounds over the list).
+//
+// Search: one warp per group of 32 consecutive (Morton-ordered) particles of
+// one cloud.  The warp walks the tree 32 nodes at a time with the group's box
+// (LIFO stack in shared memory); buckets that can hold neighbours are
+// flattened into a shared list of candidate particles, staged 32 at a time in
+// shared memory, and every lane tests the staged candidates against its own
+// particle with the exact FP64 predicate.  Rows are written in traversal order
+// (deterministic); sph_get_neighbours exports them sorted.
+//
+// h iteration: one warp per particle keeps the candidate distances and masses
+// in registers and runs a bracketed Newton iteration on
+// (4pi/3)(2h)^3 rho(h) = n_ngb m  with FP64 updates and convergence test.
+#include "sph_internal.cuh"
+
+namespace {
+
+constexpr int SEARCH_WARPS = 4;
+constexpr int SSTK = 512;
+constexpr unsigned FULL = 0xffffffffu;
+
+struct SearchSmem {
+    int stk[SSTK];
+    int flat[96];
+    double4 stage[32];
+};
+
+__device__ __forceinline__ double wmin(double v) {
+    for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+__device__ __forceinline__ double wmax(double v) {
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+// MODE 0: candidates r^2 <= (2 hc_i)^2 (gather radius of the h iteration)
+// MODE 1: exact lists |r|^2 <= (h_i + h_j)^2
+template <int MODE>
+__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+    k_search(int ngroup, const int *__restrict__ gstart, const int *__restrict__ gcount,
+             const int *__restrict__ gcloud, const int *__restrict__ croot,
+             const double4 *__restrict__ p0,
+             const double *__restrict__ hc, const int *__restrict__ need,
+             const double4 *__restrict__ sA, const double4 *__restrict__ sB,
+             const int *__restrict__ first, const int *__restrict__ last,
+             const int *__restrict__ child, int leaf_size, int K, int *__restrict__ rows,
+             int *__restrict__ cnt, long long *status) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = blockIdx.x * SEARCH_WARPS + w;
+    if (g >= ngroup) return;  // warp-uniform
+    SearchSmem &S = smem[w];
+    const unsigned lt = (1u << lane) - 1u;
+    const int s0 = gstart[g], gc = gcount[g];
+    bool act = lane < gc;
+    const int i = s0 + (act ? lane : 0);
+    if (need) act = act && need[i];
+    if (!__any_sync(FULL, act)) return;
+    const double4 pi = p0[i];
+    const double ri = MODE == 0 ? 2.0 * hc[i] : pi.w;
+    const double gx0 = wmin(act ? pi.x : INFINITY), gy0 = wmin(act ? pi.y : INFINITY),
+                 gz0 = wmin(act ? pi.z : INFINITY);
+    const double gx1 = wmax(act ? pi.x : -INFINITY), gy1 = wmax(act ? pi.y : -INFINITY),
+                 gz1 = wmax(act ? pi.z : -INFINITY);
+    const double rmax = wmax(act ? ri : 0.0);
+    const double ri2 = ri * ri;
+    int count = 0;
+    int sp = 1, nflat = 0;
+    bool overflow = false;
+    if (lane == 0) S.stk[0] = croot[gcloud[g]];
+    __syncwarp();
+
+    auto process = [&](int m) {
+        int j = 0;
+        if (lane < m) {
+            j = S.flat[lane];
+            S.stage[lane] = p0[j];
+        }
+        __syncwarp();
+        for (int k = 0; k < m; k++) {
+            const double4 pj = S.stage[k];
+            const int jj = __shfl_sync(FULL, j, k);
+            bool hit;
+            if (MODE == 0) {
+                double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                hit = dx * dx + dy * dy + dz * dz <= ri2;
+            } else {
+                hit = ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w);
+            }
+            if (act && hit) {
+                if (count < K) rows[(size_t)i * K + count] = jj;
+                count++;
+            }
+        }
+        __syncwarp();
+    };
+
+    while (sp > 0 || nflat > 0) {
+        if (sp > 0) {
+            const int take = min(sp, 32);
+            sp -= take;
+            int nd = 0, f = 0, cn = 0;
+            bool open = false;
+            if (lane < take) {
+                nd = S.stk[sp + lane];
+                const double4 a = sA[nd], b = sB[nd];
+                f = first[nd];
+                cn = last[nd] - f + 1;
+                double ex = fmax(fmax(a.x - gx1, gx0 - b.x), 0.0);
+                double ey = fmax(fmax(a.y - gy1, gy0 - b.y), 0.0);
+                double ez = fmax(fmax(a.z - gz1, gz0 - b.z), 0.0);
+                double d2 = ex * ex + ey * ey + ez * ez;
+                double reach = MODE == 0 ? rmax : (a.w + rmax);
+                open = d2 <= reach * reach * (1.0 + 1e-12);
+            }
+            __syncwarp();
+            const bool leafy = cn <= leaf_size;
+            const unsigned pm = __ballot_sync(FULL, open && !leafy);
+            const int npush = 2 * __popc(pm);
+            if (sp + npush <= SSTK) {
+                if (open && !leafy) {
+                    int pos = sp + 2 * __popc(pm & lt);
+                    S.stk[pos] = child[2 * nd + 1];
+                    S.stk[pos + 1] = child[2 * nd];
+                }
+                sp += npush;
+            } else {
+                overflow = true;
+            }
+            unsigned lm = __ballot_sync(FULL, open && leafy);
+            __syncwarp();
+            while (lm) {
+                const int src = __ffs(lm) - 1;
+                lm &= lm - 1;
+                const int ff = __shfl_sync(FULL, f, src), cc = __shfl_sync(FULL, cn, src);
+                for (int b0 = 0; b0 < cc; b0 += 32)
+                    if (b0 + lane < cc) S.flat[nflat + b0 + lane] = ff + b0 + lane;
+                nflat += cc;
+                __syncwarp();
+                while (nflat >= 32) {
+                    process(32);
+                    int v0 = S.flat[32 + lane], v1 = lane + 64 < 96 ? S.flat[64 + lane] : 0;
+                    __syncwarp();
+                    if (lane + 32 < nflat) S.flat[lane] = v0;
+                    if (lane + 64 < nflat) S.flat[32 + lane] = v1;
+                    nflat -= 32;
+                    __syncwarp();
+                }
+            }
+        }
+        if (sp == 0 && nflat > 0) {
+            process(nflat);
+            nflat = 0;
+        }
+    }
+    if (act) {
+        cnt[i] = min(count, K);
+        if (count > K) status_add(status, SPH_S_NGB_OVERFLOW, 1);
+    }
+    if (overflow && lane == 0) status_add(status, SPH_S_STACK_OVERFLOW, 1);
+}
+
+__global__ void k_h_init(int n, const double *__restrict__ h, double *__restrict__ hc,
+                         int *__restrict__ retry, double grow) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    hc[i] = h[i] * grow;
+    retry[i] = 1;
+}
+
+// one warp per particle; SLOTS candidates per lane
+template <class R, int SLOTS>
+__global__ void __launch_bounds__(128)
+    k_newton(int n, double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
+             const int *__restrict__ rows, const int *__restrict__ cnt, int K,
+             double *__restrict__ h_out, double *__restrict__ hc, int *__restrict__ retry,
+             double n_ngb, double tol, int max_iter, double grow, int last_round,
+             long long *status) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    bool act = i < n && retry[i];
+    if (!__any_sync(FULL, act)) return;  // warp-uniform (one particle per warp)
+    const double4 pi = p0[i];
+    const int c = cnt[i];
+    const double mi = (double)p1[i].w;
+    R rj[SLOTS], mj[SLOTS];
+#pragma unroll
+    for (int s = 0; s < SLOTS; s++) {
+        int k = lane + 32 * s;
+        rj[s] = R(1e30);
+        mj[s] = R(0);
+        if (k < c) {
+            int j = rows[(size_t)i * K + k];
+            double4 pj = p0[j];
+            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            rj[s] = (R)sqrt(dx * dx + dy * dy + dz * dz);
+            mj[s] = (R)p1[j].w;
+        }
+    }
+    const double cap = hc[i];
+    const double cfac = 4.0 * SPH_PI / 3.0 * 8.0;
+    double h = pi.w, lo = 0.0, hi = INFINITY;
+    bool ok = false, need = false;
+    for (int it = 1; it <= max_iter; it++) {
+        if (h > cap) {  // 2h would pass the candidate radius 2*cap
+            need = true;
+            break;
+        }
+        const R inv_h = R(1.0 / h);
+        KSum<R> S, D;
+#pragma unroll
+        for (int s = 0; s < SLOTS; s++) {
+            R q = rj[s] * inv_h;
+            if (q < R(2)) {
+                R w, dw;
+                if (q <= R(1)) {
+                    w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
+                    dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
+                } else {
+                    R t = R(2) - q;
+                    w = R(0.25) * t * t * t;
+                    dw = R(1.5) * t * t * (R(1) - q);
+                }
+                S.add(mj[s] * w);
+                D.add(mj[s] * dw);
+            }
+        }
+        const double Ssum = seg_sum<32>(S.value()), Dsum = seg_sum<32>(D.value());
+        const double h3 = h * h * h;
+        const double rho = SPH_SIG / h3 * Ssum;
+        const double drho = -SPH_SIG / (h3 * h) * Dsum;
+        const double f = cfac * h3 * rho - n_ngb * mi;
+        const double fp = cfac * h * h * (3.0 * rho + h * drho);
+        if (f < 0.0) lo = h; else hi = h;
+        double hn = fp > 0.0 ? h - f / fp : -1.0;
+        // at most a factor 1.25 per iteration (keeps retries inside the rows)
+        if (hn > 1.25 * h) hn = 1.25 * h;
+        if (hn > 0.0 && hn < h / 1.25) hn = h / 1.25;
+        if (!(hn > lo && hn < hi)) {
+            if (hi == INFINITY) hn = 1.25 * h;
+            else if (lo == 0.0) hn = h / 1.25;
+            else hn = 0.5 * (lo + hi);
+        }
+        const double dh = hn - h;
+        h = hn;
+        if (fabs(dh) < tol * fabs(h - dh)) {
+            ok = true;
+            break;
+        }
+    }
+    if (lane == 0) {
+        if (need && !last_round) {
+            hc[i] = h * grow;
+            retry[i] = 1;
+        } else {
+            retry[i] = 0;
+            if (!ok) status_add(status, SPH_S_H_NOCONV, 1);
+        }
+        if (need) status_add(status, SPH_S_H_RETRY, 1);
+        if (!need) {
+            h_out[i] = h;
+            p0[i].w = h;
+        } else {
+            // keep the last evaluated h (inside the candidate radius) for the restart
+            double hk = fmin(h, cap);
+            h_out[i] = hk;
+            p0[i].w = hk;
+        }
+    }
+}
+
+// canonical CSR export, each row sorted ascending
+__global__ void k_export(int n, const int *__restrict__ rows, const int *__restrict__ cnt, int K,
+                         const long long *__restrict__ off, int *__restrict__ lst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = cnt[i];
+    int *o = lst + off[i];
+    for (int k = 0; k < c; k++) {
+        int v = rows[(size_t)i * K + k];
+        int p = k;
+        while (p > 0 && o[p - 1] > v) {
+            o[p] = o[p - 1];
+            p--;
+        }
+        o[p] = v;
+    }
+}
+
+}  // namespace
+
+static const double H_GROW = 1.15;
+
+int launch_smoothing_h(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int c = ctx->cur;
+    const int K = ctx->cfg.max_ngb;
+    const double4 *boxA = (const double4 *)ctx->node_box;
+    const double4 *boxB = boxA + 2 * (size_t)ctx->cfg.n_max;
+    k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->hcand, ctx->retry, H_GROW);
+    const int rounds = ctx->prologue_done ? 3 : 8;
+    for (int r = 0; r < rounds; r++) {
+        k_search<0><<<div_up(ctx->ngroup, SEARCH_WARPS), SEARCH_WARPS * 32, 0, s>>>(
+            ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot, ctx->p0, ctx->hcand, ctx->retry,
+            boxA, boxB, ctx->first, ctx->last, ctx->child, ctx->cfg.leaf_size, K, ctx->cand,
+            ctx->cand_cnt, ctx->status);
+        const int last = r == rounds - 1;
+        const int slots = (K + 31) / 32;
+        if (ctx->cfg.precision == SPH_PREC_MIXED) {
+            if (slots <= 8)
+                k_newton<float, 8><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
+                    n, ctx->p0, (const float4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
+                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
+                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+            else
+                k_newton<float, 16><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
+                    n, ctx->p0, (const float4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
+                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
+                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+        } else {
+            if (slots <= 8)
+                k_newton<double, 8><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
+                    n, ctx->p0, (const double4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
+                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
+                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+            else
+                k_newton<double, 16><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
+                    n, ctx->p0, (const double4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
+                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
+                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+        }
+    }
+    ctx->lists_ok = false;
+    return ctx_check_launch(ctx, "smoothing_h");
+}
+
+int launch_neighbours(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    int rc = launch_refit_hmax(ctx);
+    if (rc) return rc;
+    cudaStream_t s = ctx->stream;
+    const double4 *boxA = (const double4 *)ctx->node_box;
+    const double4 *boxB = boxA + 2 * (size_t)ctx->cfg.n_max;
+    k_search<1><<<div_up(ctx->ngroup, SEARCH_WARPS), SEARCH_WARPS * 32, 0, s>>>(
+        ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot, ctx->p0, nullptr, nullptr, boxA, boxB,
+        ctx->first, ctx->last, ctx->child, ctx->cfg.leaf_size, ctx->cfg.max_ngb, ctx->ngb,
+        ctx->ngb_cnt, ctx->status);
+    ctx->lists_ok = true;
+    ctx->rho_ok = ctx->divcurl_ok = false;
+    return ctx_check_launch(ctx, "neighbours");
+}
+
+int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap) {
+    (void)cap;
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    k_export<<<div_up(n, 128), 128, 0, ctx->stream>>>(n, ctx->ngb, ctx->ngb_cnt, ctx->cfg.max_ngb,
+                                                       (const long long *)off_dev, lst_dev);
+    return ctx_check_launch(ctx, "export_neighbours");
+}

@@ -1,0 +1,328 @@
+// sph.cu -- the neighbour-sum passes: density (+ EOS), div/curl (+ Balsara
+// factor), pressure/viscous acceleration with the signal velocity, du/dt.
+//
+// Replaces getDensity_ngb / getPressure_Adiabatic / getCsound_Adiabatic /
+// div_curlVel_ngb / acc_sph_ngb / get_dU_ngb (hfvCLibs_v7_hfv_v2.h:474-916),
+// each a thread per particle looping over a -1 padded row of 200 int slots
+// with uncoalesced float loads, and the all-pairs numba loops of
+// MPI_sph/sph_code/libsx.py:52-262 and shear.py:78-485 (same formulas).
+//
+// Mapping: LANES consecutive lanes own one particle (LANES = ngb_lanes, the
+// "neighbour chunk width", 4..32).  They read that particle's row of the
+// neighbour list contiguously and gather the neighbours' packed records
+// (p0 = double4 x,y,z,h; p1 = Real4 v,m; p2 = Real4 rho,P/rho^2,c,f); rows are
+// spatially local in Morton order so the gathers mostly hit L1/L2.  Partial
+// sums are Kahan-compensated in FP32 (mixed) and reduced across the lanes in
+// FP64.  Coordinate differences are always taken in FP64.
+#include "sph_internal.cuh"
+
+namespace {
+
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_density(int n, const double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
+              typename R4<R>::T *__restrict__ p2, const int *__restrict__ rows,
+              const int *__restrict__ cnt, int K, const double *__restrict__ u, double gamma,
+              double *__restrict__ rho_out, double *__restrict__ P_out, double *__restrict__ c_out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    const bool valid = i < n;
+    KSum<R> S;
+    if (valid) {
+        const double4 pi = p0[i];
+        const int c = cnt[i];
+        const int *row = rows + (size_t)i * K;
+        for (int k = sl; k < c; k += LANES) {
+            const int j = row[k];
+            const double4 pj = p0[j];
+            const R mj = p1[j].w;
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R hij = (R)(0.5 * (pi.w + pj.w));
+            const R inv = R(1) / hij;
+            S.add(mj * kern_w<R>(rr * inv, inv * inv * inv));
+        }
+    }
+    const double rho = seg_sum<LANES>(S.value());
+    if (valid && sl == 0) {
+        const double ui = u[i];
+        const double P = (gamma - 1.0) * rho * ui;
+        const double cs = sqrt(gamma * (gamma - 1.0) * ui);
+        rho_out[i] = rho;
+        P_out[i] = P;
+        c_out[i] = cs;
+        typename R4<R>::T q = p2[i];
+        q.x = (R)rho;
+        q.y = (R)(P / (rho * rho));
+        q.z = (R)cs;
+        p2[i] = q;
+    }
+}
+
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_divcurl(int n, const double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
+              typename R4<R>::T *__restrict__ p2, const int *__restrict__ rows,
+              const int *__restrict__ cnt, int K, const double *__restrict__ rho,
+              const double *__restrict__ csnd, int balsara, double *__restrict__ divV,
+              double *__restrict__ curlV) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    const bool valid = i < n;
+    KSum<R> s, cx, cy, cz;
+    if (valid) {
+        const double4 pi = p0[i];
+        const typename R4<R>::T vi = p1[i];
+        const int c = cnt[i];
+        const int *row = rows + (size_t)i * K;
+        for (int k = sl; k < c; k += LANES) {
+            const int j = row[k];
+            const double4 pj = p0[j];
+            const typename R4<R>::T vj = p1[j];
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R hij = (R)(0.5 * (pi.w + pj.w));
+            const R inv = R(1) / hij;
+            const R i2 = inv * inv;
+            const R nW = kern_nw<R>(rr * inv, i2 * i2 * inv);
+            const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+            const R ux = vi.x - vj.x, uy = vi.y - vj.y, uz = vi.z - vj.z;
+            const R mj = vj.w;
+            s.add(-mj * (ux * gx + uy * gy + uz * gz));
+            cx.add(mj * (uy * gz - uz * gy));
+            cy.add(mj * (uz * gx - ux * gz));
+            cz.add(mj * (ux * gy - uy * gx));
+        }
+    }
+    const double S = seg_sum<LANES>(s.value());
+    const double X = seg_sum<LANES>(cx.value()), Y = seg_sum<LANES>(cy.value()),
+                 Z = seg_sum<LANES>(cz.value());
+    if (valid && sl == 0) {
+        const double inv_rho = 1.0 / rho[i];
+        const double d = fabs(S * inv_rho);
+        const double cv = sqrt(X * X + Y * Y + Z * Z) * inv_rho;
+        divV[i] = d;
+        curlV[i] = cv;
+        typename R4<R>::T q = p2[i];
+        q.w = balsara ? (R)(d / (d + cv + 0.0001 * csnd[i] / p0[i].w)) : R(0);
+        p2[i] = q;
+    }
+}
+
+// acc_i = -sum m_j (P_i/rho_i^2 + P_j/rho_j^2 + PI_ij) gradW_ij,
+// du_i  =  sum m_j (P_i/rho_i^2 + PI_ij/2) v_ij . gradW_ij,
+// vsig_i = max_j (c_i + c_j - 3 w_ij), w_ij = v_ij.r_ij/(r_ij + 1e-5).
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_force(int n, const double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
+            const typename R4<R>::T *__restrict__ p2, const int *__restrict__ rows,
+            const int *__restrict__ cnt, int K, int av_mode, int balsara, R alpha, R beta, R eta,
+            int want_acc, int want_du, double *__restrict__ acc, double *__restrict__ dudt,
+            double *__restrict__ vsig) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    const bool valid = i < n;
+    KSum<R> ax, ay, az, du;
+    R vs = R(0);
+    if (valid) {
+        const double4 pi = p0[i];
+        const typename R4<R>::T vi = p1[i], qi = p2[i];
+        const int c = cnt[i];
+        const int *row = rows + (size_t)i * K;
+        const R eta2 = eta * eta;
+        for (int k = sl; k < c; k += LANES) {
+            const int j = row[k];
+            const double4 pj = p0[j];
+            const typename R4<R>::T vj = p1[j], qj = p2[j];
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R hij = (R)(0.5 * (pi.w + pj.w));
+            const R inv = R(1) / hij;
+            const R i2 = inv * inv;
+            const R nW = kern_nw<R>(rr * inv, i2 * i2 * inv);
+            const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+            const R ux = vi.x - vj.x, uy = vi.y - vj.y, uz = vi.z - vj.z;
+            const R vr = ux * dx + uy * dy + uz * dz;
+            const R w = vr / (rr + R(1e-5));
+            R PI = R(0);
+            if (vr <= R(0)) {
+                const R rhoij = R(0.5) * (qi.x + qj.x);
+                if (av_mode == SPH_AV_MG83) {
+                    const R cij = R(0.5) * (qi.z + qj.z);
+                    const R mu = hij * vr / (rr * rr + hij * hij * eta2);
+                    PI = (-alpha * cij * mu + beta * mu * mu) / rhoij;
+                } else {
+                    const R sig = qi.z + qj.z - R(3) * w;
+                    PI = R(-0.5) * alpha * sig * w / rhoij;
+                }
+            }
+            if (balsara) PI = R(0.5) * (qi.w + qj.w) * PI;
+            const R mj = vj.w;
+            if (want_acc) {
+                const R tt = mj * (qi.y + qj.y + PI);
+                ax.add(-tt * gx);
+                ay.add(-tt * gy);
+                az.add(-tt * gz);
+                vs = fmax(vs, qi.z + qj.z - R(3) * w);
+            }
+            if (want_du) du.add(mj * (qi.y + R(0.5) * PI) * (ux * gx + uy * gy + uz * gz));
+        }
+    }
+    if (want_acc) {
+        const double X = seg_sum<LANES>(ax.value()), Y = seg_sum<LANES>(ay.value()),
+                     Z = seg_sum<LANES>(az.value());
+        const double V = seg_max<LANES>((double)vs);
+        if (valid && sl == 0) {
+            acc[i] = X;
+            acc[(size_t)n + i] = Y;
+            acc[2 * (size_t)n + i] = Z;
+            vsig[i] = V;
+        }
+    }
+    if (want_du) {
+        const double D = seg_sum<LANES>(du.value());
+        if (valid && sl == 0) dudt[i] = D;
+    }
+}
+
+template <class R>
+__global__ void k_repack_p2(int n, const double *__restrict__ rho, const double *__restrict__ P,
+                            const double *__restrict__ c, const double *__restrict__ divV,
+                            const double *__restrict__ curlV, const double4 *__restrict__ p0,
+                            int balsara, typename R4<R>::T *__restrict__ p2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    typename R4<R>::T q;
+    const double r = rho[i];
+    q.x = (R)r;
+    q.y = (R)(P[i] / (r * r));
+    q.z = (R)c[i];
+    const double d = divV[i], cv = curlV[i];
+    q.w = balsara ? (R)(d / (d + cv + 0.0001 * c[i] / p0[i].w)) : R(0);
+    p2[i] = q;
+}
+
+template <class R>
+__global__ void k_pack_p1(int n, const double *__restrict__ vx, const double *__restrict__ vy,
+                          const double *__restrict__ vz, const double *__restrict__ m,
+                          const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, const double *__restrict__ h,
+                          typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ pw,
+                          double4 *__restrict__ p0) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    typename R4<R>::T a, b;
+    a.x = (R)vx[i]; a.y = (R)vy[i]; a.z = (R)vz[i]; a.w = (R)m[i];
+    b.x = (R)x[i]; b.y = (R)y[i]; b.z = (R)z[i]; b.w = (R)m[i];
+    p1[i] = a;
+    pw[i] = b;
+    p0[i] = make_double4(x[i], y[i], z[i], h[i]);
+}
+
+template <class R, int L>
+int run_density(sph_ctx *ctx) {
+    const int n = ctx->n, c = ctx->cur;
+    const int bs = ctx->cfg.block_size;
+    k_density<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb,
+        ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->st[c][ST_U], ctx->cfg.gamma, ctx->rho, ctx->P, ctx->c);
+    return SPH_OK;
+}
+template <class R, int L>
+int run_divcurl(sph_ctx *ctx) {
+    const int n = ctx->n;
+    const int bs = ctx->cfg.block_size;
+    k_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb,
+        ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->rho, ctx->c, ctx->cfg.balsara, ctx->divV, ctx->curlV);
+    return SPH_OK;
+}
+template <class R, int L>
+int run_force(sph_ctx *ctx, bool acc, bool du) {
+    const int n = ctx->n;
+    const int bs = ctx->cfg.block_size;
+    k_force<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (const typename R4<R>::T *)ctx->p2,
+        ctx->ngb, ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->cfg.av_mode, ctx->cfg.balsara,
+        (R)ctx->cfg.alpha, (R)ctx->cfg.beta, (R)ctx->cfg.eta, acc ? 1 : 0, du ? 1 : 0, ctx->asph,
+        ctx->dudt, ctx->vsig);
+    return SPH_OK;
+}
+
+template <template <class, int> class F, class R>
+struct Dispatch;
+
+#define SPH_DISPATCH_LANES(FN, R, ctx, ...)                 \
+    switch ((ctx)->cfg.ngb_lanes) {                         \
+        case 4: rc = FN<R, 4>(ctx, ##__VA_ARGS__); break;   \
+        case 8: rc = FN<R, 8>(ctx, ##__VA_ARGS__); break;   \
+        case 16: rc = FN<R, 16>(ctx, ##__VA_ARGS__); break; \
+        default: rc = FN<R, 32>(ctx, ##__VA_ARGS__); break; \
+    }
+
+}  // namespace
+
+int launch_density(sph_ctx *ctx) {
+    if (ctx->n <= 0) return SPH_OK;
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_density, float, ctx); }
+    else { SPH_DISPATCH_LANES(run_density, double, ctx); }
+    if (rc) return rc;
+    ctx->rho_ok = true;
+    return ctx_check_launch(ctx, "density");
+}
+
+int launch_divcurl(sph_ctx *ctx) {
+    if (ctx->n <= 0) return SPH_OK;
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_divcurl, float, ctx); }
+    else { SPH_DISPATCH_LANES(run_divcurl, double, ctx); }
+    if (rc) return rc;
+    ctx->divcurl_ok = true;
+    ctx->p2_dirty = false;
+    return ctx_check_launch(ctx, "divcurl");
+}
+
+int launch_repack_p2(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    if (ctx->cfg.precision == SPH_PREC_MIXED)
+        k_repack_p2<float><<<div_up(n, 256), 256, 0, ctx->stream>>>(
+            n, ctx->rho, ctx->P, ctx->c, ctx->divV, ctx->curlV, ctx->p0, ctx->cfg.balsara,
+            (float4 *)ctx->p2);
+    else
+        k_repack_p2<double><<<div_up(n, 256), 256, 0, ctx->stream>>>(
+            n, ctx->rho, ctx->P, ctx->c, ctx->divV, ctx->curlV, ctx->p0, ctx->cfg.balsara,
+            (double4 *)ctx->p2);
+    ctx->p2_dirty = false;
+    return ctx_check_launch(ctx, "repack_p2");
+}
+
+int launch_pack_p1(sph_ctx *ctx) {
+    const int n = ctx->n, c = ctx->cur;
+    if (n <= 0) return SPH_OK;
+    double *const *st = ctx->st[c];
+    if (ctx->cfg.precision == SPH_PREC_MIXED)
+        k_pack_p1<float><<<div_up(n, 256), 256, 0, ctx->stream>>>(
+            n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
+            (float4 *)ctx->p1, (float4 *)ctx->pw, ctx->p0);
+    else
+        k_pack_p1<double><<<div_up(n, 256), 256, 0, ctx->stream>>>(
+            n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
+            (double4 *)ctx->p1, (double4 *)ctx->pw, ctx->p0);
+    return ctx_check_launch(ctx, "pack_p1");
+}
+
+int launch_forces(sph_ctx *ctx, bool want_acc, bool want_du, bool update_u) {
+    (void)update_u;
+    if (ctx->n <= 0) return SPH_OK;
+    if (ctx->p2_dirty) {
+        int r = launch_repack_p2(ctx);
+        if (r) return r;
+    }
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_force, float, ctx, want_acc, want_du); }
+    else { SPH_DISPATCH_LANES(run_force, double, ctx, want_acc, want_du); }
+    if (rc) return rc;
+    return ctx_check_launch(ctx, "forces");
+}

@@ -1,0 +1,256 @@
+// sph_internal.cuh -- shared definitions of libsphb200 (sm_100a).
+//
+// Layout of the particle state in HBM (storage order = Morton order after
+// every sph_sort):
+//   * FP64 SoA masters, double-buffered for the permutation at each sort:
+//       x y z vx vy vz m h u dudt_prev  + int32 id (original index), cloud
+//   * FP64 SoA results of the current step (single buffer):
+//       rho P c divV curlV a_sph[3] a_grav[3] dudt vsig pot
+//   * packed j-records read by the neighbour passes (one sector or less per
+//     neighbour gather):
+//       p0 = double4 (x, y, z, h)              -- FP64 in both precisions
+//       p1 = Real4   (vx, vy, vz, m)
+//       p2 = Real4   (rho, P/rho^2, c, f_balsara)
+//       pw = Real4   (x, y, z, m)              -- gravity walk particles
+//   * tree: 2N-1 nodes (internal 0..N-2, leaf of particle p at N-1+p), FP64
+//     records of 16 doubles for the build, Real4 x3 walk records.
+//   * neighbour rows: int32 [N][max_ngb] row-major + counts.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sph_b200.h"
+
+#define SPH_PI 3.14159265358979323846
+#define SPH_SIG (1.0 / SPH_PI)
+
+#define CK(call)                                                         \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) return ctx_fail(ctx, e_, #call, __LINE__); \
+    } while (0)
+
+// ---- state field indices of the double-buffered persistent SoA ----
+enum { ST_X, ST_Y, ST_Z, ST_VX, ST_VY, ST_VZ, ST_M, ST_H, ST_U, ST_DUDT_PREV, ST_N };
+
+struct sph_ctx {
+    sph_config cfg;
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr, stream_g = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    std::string err;
+    int n = 0, ncloud = 0;
+    std::vector<int> cloud_start_h;  // ncloud+1
+    int64_t dev_bytes = 0;
+    std::vector<void *> allocs;
+
+    // persistent state, double buffered
+    double *st[2][ST_N] = {};
+    int *id[2] = {}, *cloud[2] = {};
+    int cur = 0;
+
+    // per-step results
+    double *rho = nullptr, *P = nullptr, *c = nullptr, *divV = nullptr, *curlV = nullptr;
+    double *asph = nullptr, *agrav = nullptr;  // 3*N each (x block, y block, z block)
+    double *dudt = nullptr, *vsig = nullptr, *pot = nullptr;
+
+    // packed records
+    double4 *p0 = nullptr;
+    void *p1 = nullptr, *p2 = nullptr, *pw = nullptr;
+    bool p2_dirty = true;
+
+    // sort
+    unsigned long long *key[2] = {};
+    int *val[2] = {};
+    unsigned long long *key_in = nullptr;  // keys of the storage order before the last sort
+    int *perm = nullptr;         // permutation of the last sort
+    unsigned *hist = nullptr;    // radix histograms
+    int sort_blocks = 0;
+    unsigned long long *box = nullptr;  // per cloud 6 ordered-uint64 (min xyz, max xyz)
+    int *cloud_start = nullptr;         // device copy
+
+    // tree
+    int *child = nullptr, *parent = nullptr, *first = nullptr, *last = nullptr, *flag = nullptr;
+    double *node = nullptr, *hmax = nullptr, *ropen2 = nullptr;
+    void *node_box = nullptr;  // double4 [2][2*n_max]: (box min, h_max), (box max, 0)
+    void *wA = nullptr, *wB = nullptr, *wC = nullptr;  // Real4 walk records
+    int *croot = nullptr;                              // per cloud root node
+    int *gstart = nullptr, *gcount = nullptr, *groot_g = nullptr;  // groups: start, size, cloud id
+    int ngroup = 0;
+    bool tree_ok = false;
+
+    // neighbours
+    int *ngb = nullptr, *ngb_cnt = nullptr;
+    int *cand = nullptr, *cand_cnt = nullptr;
+    int *retry = nullptr;        // per particle: 1 = candidate radius too small
+    double *hcand = nullptr;     // candidate radius / 2 used per particle
+    bool lists_ok = false, rho_ok = false, divcurl_ok = false;
+
+    // time step, status, counters
+    double *dt = nullptr, *dt_next = nullptr;  // per cloud
+    unsigned long long *dt_bits = nullptr;     // per cloud ordered min
+    long long *status = nullptr;               // SPH_NSTATUS
+    unsigned long long *counters = nullptr;    // walk: cells, particles
+    unsigned *work = nullptr;                  // work counters for persistent kernels (16)
+    double *red = nullptr;                     // reduction scratch
+
+    // cooling
+    bool cool_ok = false;
+    sph_cooling_params cool{};
+    double *cool_table = nullptr;  // n_bins+1
+    float *mlp = nullptr;          // FP32 master params (SPH_MLP_NPARAM) + norm (8)
+    void *mlp_bf16 = nullptr;      // packed BF16 weights for the tensor-core kernels
+    float *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr;
+    float *mlp_scratch = nullptr;
+    int mlp_step = 0;
+    bool mlp_ok = false;
+
+    // phase timing events of sph_step (SPH_FLAG_TIMING)
+    cudaEvent_t tev[16] = {};
+    bool tev_ok = false;
+    int graph_kernels = 0;
+
+    // step graphs (one per buffer parity)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_valid = false;
+    bool prologue_done = false;
+    int64_t step_count = 0;
+};
+
+int ctx_fail(sph_ctx *ctx, cudaError_t e, const char *what, int line);
+int ctx_check_launch(sph_ctx *ctx, const char *what);
+
+// ----------------------------------------------------------------------------
+// device helpers
+// ----------------------------------------------------------------------------
+template <class R> struct R4;
+template <> struct R4<float> { typedef float4 T; };
+template <> struct R4<double> { typedef double4 T; };
+
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// ordered mapping double <-> uint64 (monotone), for atomic min/max of doubles
+__device__ __forceinline__ unsigned long long dbl_to_ord(double d) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(d);
+    return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+}
+__host__ __device__ __forceinline__ double ord_to_dbl(unsigned long long o) {
+    unsigned long long b = (o & 0x8000000000000000ULL) ? (o & 0x7fffffffffffffffULL) : ~o;
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double d;
+    memcpy(&d, &b, 8);
+    return d;
+#endif
+}
+
+// exact neighbour predicate |r|^2 <= (hi+hj)^2, rounding as written
+__device__ __forceinline__ bool ngb_pred(double xi, double yi, double zi, double hi, double xj,
+                                         double yj, double zj, double hj) {
+    double dx = xsub(xi, xj), dy = xsub(yi, yj), dz = xsub(zi, zj);
+    double r2 = xadd(xmul(dx, dx), xmul(dy, dy));
+    r2 = xadd(r2, xmul(dz, dz));
+    double s = xadd(hi, hj);
+    return r2 <= xmul(s, s);
+}
+
+// M4 cubic spline (sigma = 1/pi, support 2h): W and nW with gradW = nW * dr
+// (libsx.py:69-80, shear.py:109-121; the q+1e-20 guard of the reference)
+template <class R>
+__device__ __forceinline__ R kern_w(R q, R inv_h3) {
+    if (q <= R(1)) return R(SPH_SIG) * inv_h3 * (R(1) - R(1.5) * q * q + R(0.75) * q * q * q);
+    if (q <= R(2)) {
+        R t = R(2) - q;
+        return R(SPH_SIG) * inv_h3 * R(0.25) * t * t * t;
+    }
+    return R(0);
+}
+template <class R>
+__device__ __forceinline__ R kern_nw(R q, R inv_h5) {
+    if (q <= R(1)) return R(SPH_SIG) * inv_h5 * (R(-3) + R(2.25) * q);
+    if (q <= R(2)) {
+        R t = R(2) - q;
+        return R(-0.75 * SPH_SIG) * inv_h5 * t * t / (q + R(1e-20));
+    }
+    return R(0);
+}
+
+// Kahan-compensated accumulator for FP32, plain sum for FP64
+template <class R> struct KSum {
+    R s = R(0);
+    __device__ __forceinline__ void add(R x) { s += x; }
+    __device__ __forceinline__ double value() const { return (double)s; }
+};
+template <> struct KSum<float> {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        float y = __fsub_rn(x, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// sum over the `lanes`-wide segment (lanes a power of two <= 32), all lanes
+// of the warp must call; result identical on every lane of the segment
+template <int LANES>
+__device__ __forceinline__ double seg_sum(double v) {
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31;
+    return __shfl_sync(0xffffffffu, v, lane & ~(LANES - 1));
+}
+template <int LANES>
+__device__ __forceinline__ double seg_max(double v) {
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ void status_add(long long *status, int which, long long v) {
+    atomicAdd((unsigned long long *)&status[which], (unsigned long long)v);
+}
+
+// ---- host-side launch helpers implemented per translation unit ----
+int launch_sort(sph_ctx *ctx);
+int launch_tree(sph_ctx *ctx);
+int launch_refit_hmax(sph_ctx *ctx);
+int launch_smoothing_h(sph_ctx *ctx);
+int launch_neighbours(sph_ctx *ctx);
+int launch_density(sph_ctx *ctx);
+int launch_divcurl(sph_ctx *ctx);
+int launch_forces(sph_ctx *ctx, bool want_acc, bool want_du, bool update_u);
+int launch_repack_p2(sph_ctx *ctx);
+int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot);
+int launch_gravity_direct(sph_ctx *ctx, int nt, const int *targets_dev, double *out_dev);
+int launch_gravity_direct_spline(sph_ctx *ctx, const double *eps_dev, int nt,
+                                 const int *targets_dev, double *out_dev);
+int launch_kick(sph_ctx *ctx, double fac, bool cfl);
+int launch_drift(sph_ctx *ctx);
+int launch_kick_drift(sph_ctx *ctx);
+int launch_update_u(sph_ctx *ctx, bool first);
+int launch_cfl(sph_ctx *ctx);
+int launch_energies(sph_ctx *ctx, double *out10_host);
+int launch_pack_p1(sph_ctx *ctx);
+int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap);
+int launch_cooling_exact(sph_ctx *ctx);
+int launch_cooling_mlp(sph_ctx *ctx);
+int launch_cool_solve(sph_ctx *ctx, int n, const double *rho, const double *u_old,
+                      const double *dt, double *u_new, int *iters);
+int mlp_forward_dev(sph_ctx *ctx, int n, const float *X, float *y);
+int mlp_grad_dev(sph_ctx *ctx, int n, const float *X, const float *t, float *grad, float *loss);
+int mlp_train_dev(sph_ctx *ctx, int n, const float *X, const float *t, int batch, int nsteps,
+                  float lr, float *loss);
+int mlp_pack(sph_ctx *ctx);
+
+static inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

@@ -1,0 +1,248 @@
+// tree.cu -- Karras (2012) binary radix tree over the sorted Morton keys and
+// the deterministic FP64 bottom-up pass (mass, centre of mass, quadrupole
+// second moments, particle box, h_max, opening radius).
+//
+// Replaces the reference octree (bh_tree_iteration_v2.h:29-450): a single
+// <<<1,256>>> block inserting bodies under atomicCAS child locks with
+// atomicAdd'ed masses (nondeterministic), a separate centre-of-mass kernel and
+// a busy-waiting tree-order sort.  Here the build is one thread per internal
+// node, the moments are combined bottom-up with the left child always first
+// (so every node record is the same bit pattern on every run and equals the
+// oracle's), and the Morton order is the walk order.
+#include "sph_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ int delta_pref(const unsigned long long *__restrict__ k, int n, int i,
+                                          int j) {
+    if (j < 0 || j > n - 1) return -1;
+    unsigned long long a = k[i], b = k[j];
+    if (a == b) return 64 + __clz((unsigned)i ^ (unsigned)j);
+    return __clzll(a ^ b);
+}
+
+__global__ void k_karras(const unsigned long long *__restrict__ key, const int *__restrict__ cloud,
+                         int n, int *__restrict__ child, int *__restrict__ parent,
+                         int *__restrict__ first, int *__restrict__ last, int *__restrict__ croot) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta_pref(key, n, i, i + 1) - delta_pref(key, n, i, i - 1)) > 0 ? 1 : -1;
+    int dmin = delta_pref(key, n, i, i - d);
+    int lmax = 2;
+    while (delta_pref(key, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta_pref(key, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta_pref(key, n, i, j);
+    int s = 0;
+    for (int t = (l + 1) / 2;; t = (t + 1) / 2) {
+        if (delta_pref(key, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+    }
+    int gam = i + s * d + (d < 0 ? -1 : 0);
+    int lo = min(i, j), hi = max(i, j);
+    int L = (lo == gam) ? n - 1 + gam : gam;
+    int R = (hi == gam + 1) ? n - 1 + gam + 1 : gam + 1;
+    child[2 * i] = L;
+    child[2 * i + 1] = R;
+    parent[L] = i;
+    parent[R] = i;
+    first[i] = lo;
+    last[i] = hi;
+    int c = cloud[lo];
+    if (cloud[hi] == c && (lo == 0 || cloud[lo - 1] != c) && (hi == n - 1 || cloud[hi + 1] != c))
+        croot[c] = i;
+}
+
+// clouds of one particle: their root is the leaf
+__global__ void k_single_roots(const int *__restrict__ cstart, int ncloud, int n, int *croot) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ncloud) return;
+    if (cstart[k + 1] - cstart[k] == 1) croot[k] = n - 1 + cstart[k];
+}
+
+template <class R>
+__device__ __forceinline__ void write_walk(int nd, const double *o, double r2, double hm,
+                                           typename R4<R>::T *wA, typename R4<R>::T *wB,
+                                           typename R4<R>::T *wC) {
+    typename R4<R>::T a, b, c;
+    a.x = (R)o[0]; a.y = (R)o[1]; a.z = (R)o[2]; a.w = (R)o[3];
+    b.x = (R)o[4]; b.y = (R)o[5]; b.z = (R)o[6]; b.w = (R)r2;
+    c.x = (R)o[7]; c.y = (R)o[8]; c.z = (R)o[9]; c.w = (R)hm;
+    wA[nd] = a;
+    wB[nd] = b;
+    wC[nd] = c;
+}
+
+// opening radius^2 of a node: (l/theta + |com - box centre|)^2, l = largest side
+__device__ __forceinline__ double open_r2(const double *o, double theta) {
+    double l = fmax(xsub(o[13], o[10]), fmax(xsub(o[14], o[11]), xsub(o[15], o[12])));
+    double cx = xmul(xadd(o[10], o[13]), 0.5), cy = xmul(xadd(o[11], o[14]), 0.5),
+           cz = xmul(xadd(o[12], o[15]), 0.5);
+    double ex = xsub(o[0], cx), ey = xsub(o[1], cy), ez = xsub(o[2], cz);
+    double d2 = xadd(xmul(ex, ex), xmul(ey, ey));
+    d2 = xadd(d2, xmul(ez, ez));
+    double r = xadd(xdiv(l, theta), __dsqrt_rn(d2));
+    return xmul(r, r);
+}
+
+template <class R>
+__global__ void k_leaves(int n, const double *__restrict__ x, const double *__restrict__ y,
+                         const double *__restrict__ z, const double *__restrict__ m,
+                         const double *__restrict__ h, double *__restrict__ node,
+                         double *__restrict__ hmax, double *__restrict__ ropen2,
+                         double4 *__restrict__ sA, double4 *__restrict__ sB, int *__restrict__ flag,
+                         int *__restrict__ first, int *__restrict__ last, int *__restrict__ child,
+                         typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int nd = n - 1 + p;
+    double o[16];
+    o[0] = x[p]; o[1] = y[p]; o[2] = z[p]; o[3] = m[p];
+    for (int q = 4; q < 10; q++) o[q] = 0.0;
+    o[10] = o[13] = x[p]; o[11] = o[14] = y[p]; o[12] = o[15] = z[p];
+    double *dst = node + (size_t)16 * nd;
+    for (int q = 0; q < 16; q++) dst[q] = o[q];
+    hmax[nd] = h[p];
+    ropen2[nd] = 0.0;
+    sA[nd] = make_double4(o[10], o[11], o[12], h[p]);
+    sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
+    first[nd] = p;
+    last[nd] = p;
+    child[2 * nd] = -1;
+    child[2 * nd + 1] = -1;
+    write_walk<R>(nd, o, 0.0, h[p], wA, wB, wC);
+    if (p < n - 1) flag[p] = 0;
+}
+
+__device__ __forceinline__ void combine(double *o, const double *a, const double *b) {
+    double M = xadd(a[3], b[3]);
+    double c[3];
+    for (int d = 0; d < 3; d++) c[d] = xdiv(xadd(xmul(a[3], a[d]), xmul(b[3], b[d])), M);
+    double da[3] = {xsub(a[0], c[0]), xsub(a[1], c[1]), xsub(a[2], c[2])};
+    double db[3] = {xsub(b[0], c[0]), xsub(b[1], c[1]), xsub(b[2], c[2])};
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double ta = xadd(a[4 + q], xmul(xmul(a[3], da[ia[q]]), da[ib[q]]));
+        double tb = xadd(b[4 + q], xmul(xmul(b[3], db[ia[q]]), db[ib[q]]));
+        o[4 + q] = xadd(ta, tb);
+    }
+    o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; o[3] = M;
+    for (int d = 0; d < 3; d++) {
+        o[10 + d] = fmin(a[10 + d], b[10 + d]);
+        o[13 + d] = fmax(a[13 + d], b[13 + d]);
+    }
+}
+
+// one thread per leaf climbs; the second child to finish combines its parent
+template <class R>
+__global__ void k_bottom_up(int n, const int *__restrict__ parent, const int *__restrict__ child,
+                            double *node, double *hmax, double *ropen2, double4 *sA, double4 *sB,
+                            int *flag, double theta, typename R4<R>::T *wA, typename R4<R>::T *wB,
+                            typename R4<R>::T *wC) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n || n < 2) return;
+    int nd = parent[n - 1 + p];
+    while (nd >= 0) {
+        __threadfence();
+        if (atomicAdd(&flag[nd], 1) == 0) return;
+        __threadfence();
+        int L = child[2 * nd], Rr = child[2 * nd + 1];
+        double a[16], b[16], o[16];
+        const double *pa = node + (size_t)16 * L, *pb = node + (size_t)16 * Rr;
+        for (int q = 0; q < 16; q++) {
+            a[q] = __ldcg(pa + q);
+            b[q] = __ldcg(pb + q);
+        }
+        combine(o, a, b);
+        double hm = fmax(__ldcg(hmax + L), __ldcg(hmax + Rr));
+        double r2 = open_r2(o, theta);
+        double *dst = node + (size_t)16 * nd;
+        for (int q = 0; q < 16; q++) dst[q] = o[q];
+        hmax[nd] = hm;
+        ropen2[nd] = r2;
+        sA[nd] = make_double4(o[10], o[11], o[12], hm);
+        sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
+        write_walk<R>(nd, o, r2, hm, wA, wB, wC);
+        nd = parent[nd];
+    }
+}
+
+// h_max refit after the smoothing lengths changed
+__global__ void k_refit_leaves(int n, const double *__restrict__ h, double *hmax, double4 *sA,
+                               int *flag) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    hmax[n - 1 + p] = h[p];
+    sA[n - 1 + p].w = h[p];
+    if (p < n - 1) flag[p] = 0;
+}
+
+__global__ void k_refit_up(int n, const int *__restrict__ parent, const int *__restrict__ child,
+                           double *hmax, double4 *sA, int *flag) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n || n < 2) return;
+    int nd = parent[n - 1 + p];
+    while (nd >= 0) {
+        __threadfence();
+        if (atomicAdd(&flag[nd], 1) == 0) return;
+        __threadfence();
+        double hm = fmax(__ldcg(hmax + child[2 * nd]), __ldcg(hmax + child[2 * nd + 1]));
+        hmax[nd] = hm;
+        sA[nd].w = hm;
+        nd = parent[nd];
+    }
+}
+
+}  // namespace
+
+int launch_tree(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int c = ctx->cur;
+    const unsigned long long *key = ctx->key[0];
+    const bool mixed = ctx->cfg.precision == SPH_PREC_MIXED;
+    if (n > 1)
+        k_karras<<<div_up(n - 1, 256), 256, 0, s>>>(key, ctx->cloud[c], n, ctx->child, ctx->parent,
+                                                    ctx->first, ctx->last, ctx->croot);
+    k_single_roots<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->cloud_start, ctx->ncloud, n,
+                                                            ctx->croot);
+    // leaf records; the root has no parent
+    CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
+    double4 *boxA = (double4 *)ctx->node_box;
+    double4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
+    if (mixed) {
+        k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
+            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
+            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
+            ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
+        k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
+            n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
+            ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
+    } else {
+        k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
+            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
+            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
+            ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
+        k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
+            n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
+            ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
+    }
+    ctx->tree_ok = true;
+    return ctx_check_launch(ctx, "tree");
+}
+
+int launch_refit_hmax(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    double4 *boxA = (double4 *)ctx->node_box;
+    k_refit_leaves<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[ctx->cur][ST_H], ctx->hmax, boxA,
+                                                  ctx->flag);
+    k_refit_up<<<div_up(n, 256), 256, 0, s>>>(n, ctx->parent, ctx->child, ctx->hmax, boxA,
+                                              ctx->flag);
+    return ctx_check_launch(ctx, "refit");
+}
