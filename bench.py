@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--theta", type=float, default=0.4)
-    ap.add_argument("--leaf", type=int, default=16)
+    ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -212,7 +212,9 @@ def main():
 
     n = a.n
     d = ic.evrard(n, seed=42 + rank)
-    stream = torch.cuda.Stream()
+    # high priority for the SPH passes; the library runs gravity on its own
+    # low-priority stream beside them
+    stream = torch.cuda.Stream(priority=-10)
 
     def make(precision, flags=0):
         cfg = Config(n_max=n, precision=precision, theta=a.theta, leaf_size=a.leaf,

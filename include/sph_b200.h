@@ -183,6 +183,10 @@ int sph_build_tree(sph_ctx *ctx);
 int sph_get_tree(sph_ctx *ctx, double *node, int32_t *child, int32_t *first, int32_t *last,
                  double *open_r2, double *hmax, int32_t host);
 
+/* The walk/search groups of the last tree build: maximal tree nodes with at
+ * most 32 particles of one cloud, in Morton order (start index, size). */
+int sph_get_groups(sph_ctx *ctx, int32_t *ngroup, int32_t *gstart, int32_t *gcount, int32_t host);
+
 /* Newton smoothing-length iteration (replaces smoothing_h_ngb,
  * hfvCLibs_v7_hfv_v2.h:367-455, and h_smooth_fast_mpi, libsx.py:854-902).
  * Needs sph_build_tree. */
@@ -275,6 +279,12 @@ int sph_prologue(sph_ctx *ctx);
  * -kick-du/dt-u-[cooling]-dt (sph_mpi4_v4.py:278-442; EVR.cu:1139-1782),
  * replayed from a CUDA graph unless SPH_FLAG_NO_GRAPH. */
 int sph_step(sph_ctx *ctx, int32_t nsteps);
+
+/* internal per-particle arrays for diagnostics, storage order:
+ * 0 candidate count (int32), 1 list count (int32), 2 retry flag (int32),
+ * 3 candidate radius / 2 (double), 4 h of the packed position record,
+ * 5 mass of the packed velocity record (both as double) */
+int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host);
 
 /* ---- measurement ---- */
 /* Phase durations of the last sph_step (needs SPH_FLAG_TIMING), in ms:

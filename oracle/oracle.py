@@ -325,15 +325,21 @@ def open_r2(node, theta):
     return out
 
 
-def make_groups(cloud_start, group_size=32):
-    gs, gc, gk = [], [], []
-    for k in range(len(cloud_start) - 1):
-        a, b = int(cloud_start[k]), int(cloud_start[k + 1])
-        for s in range(a, b, group_size):
-            gs.append(s)
-            gc.append(min(group_size, b - s))
-            gk.append(k)
-    return (np.array(gs, np.int32), np.array(gc, np.int32), np.array(gk, np.int32))
+def tree_groups(first, last, parent, cloud, gmax=32):
+    """Walk/search groups: maximal tree nodes with at most gmax particles of
+    one cloud, ordered by their first particle (project definition; the
+    reference walks one particle per thread, bh_tree_iteration_v2.h:454)."""
+    first, last, parent = np.asarray(first), np.asarray(last), np.asarray(parent)
+    cloud = np.asarray(cloud)
+    cnt = last - first + 1
+    ok = (cnt <= gmax) & (cloud[first] == cloud[last])
+    pp = np.where(parent < 0, 0, parent)
+    top = ok & ((parent < 0) | ~ok[pp])
+    idx = np.nonzero(top)[0]
+    order = np.argsort(first[idx], kind="stable")
+    idx = idx[order]
+    return (first[idx].astype(np.int32), cnt[idx].astype(np.int32),
+            cloud[first[idx]].astype(np.int32))
 
 
 def cloud_roots(first, last, cloud_start, n):
@@ -361,7 +367,8 @@ def bh_walk(x, y, z, m, h, keys_sorted, theta, eps, G=1.0, leaf_size=16, group_s
     child, parent, first, last = build_radix_tree(keys_sorted)
     node, hmax = tree_moments(child, x, y, z, m, h)
     r2 = open_r2(node, theta)
-    gs, gc, gk = make_groups(cloud_start, group_size)
+    cloud = np.repeat(np.arange(len(cloud_start) - 1), np.diff(cloud_start))
+    gs, gc, gk = tree_groups(first, last, parent, cloud, group_size)
     roots = cloud_roots(first, last, cloud_start, n)
     groot = roots[gk].astype(np.int32)
     ax, ay, az = np.zeros(n), np.zeros(n), np.zeros(n)

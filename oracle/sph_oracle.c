@@ -555,6 +555,9 @@ int orc_newton_h(int N, const double *x, const double *y, const double *z, const
             if (f < 0.0) lo = h; else hi = h;
             double hn;
             if (fp > 0.0) hn = h - f / fp; else hn = -1.0;
+            /* a Newton step below the tolerance is accepted before any bracket
+             * test: in FP64 it can round to exactly h (= a bracket end) */
+            if (fp > 0.0 && fabs(f / fp) < tol * h) { h = hn; ok = 1; break; }
             /* at most a factor 1.25 per iteration */
             if (hn > 1.25 * h) hn = 1.25 * h;
             if (hn > 0.0 && hn < h / 1.25) hn = h / 1.25;

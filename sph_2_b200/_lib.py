@@ -87,6 +87,7 @@ SIGNATURES = [
     ("sph_get_sort", C.c_int, [_P, _P, _P, _I]),
     ("sph_build_tree", C.c_int, [_P]),
     ("sph_get_tree", C.c_int, [_P, _P, _P, _P, _P, _P, _P, _I]),
+    ("sph_get_groups", C.c_int, [_P, _P, _P, _P, _I]),
     ("sph_smoothing_h", C.c_int, [_P]),
     ("sph_neighbours", C.c_int, [_P]),
     ("sph_get_neighbours", C.c_int, [_P, _P, _P, C.c_int64, _I]),
@@ -112,6 +113,7 @@ SIGNATURES = [
     ("sph_mlp_forward", C.c_int, [_P, _I, _P, _P, _I]),
     ("sph_mlp_grad", C.c_int, [_P, _I, _P, _P, _P, _P, _I]),
     ("sph_mlp_train", C.c_int, [_P, _I, _P, _P, _I, _I, _F, _P]),
+    ("sph_debug_copy", C.c_int, [_P, _I, _P, _I]),
     ("sph_get_phase_times", C.c_int, [_P, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),

@@ -27,7 +27,7 @@ class Config:
     precision: str = "mixed"
     av_mode: str = "mg83"
     balsara: bool = False
-    leaf_size: int = 16
+    leaf_size: int = 8
     ngb_lanes: int = 8
     block_size: int = 256
     max_ngb: int = 256
@@ -202,6 +202,15 @@ class Context:
                                        _ptr(r2), _ptr(hmax), 1), "tree")
         return dict(node=node, child=child, first=first, last=last, open_r2=r2, hmax=hmax)
 
+    def groups(self):
+        """(count, start, size) of the walk/search groups of the last tree."""
+        ng = C.c_int32()
+        self._chk(self._L.sph_get_groups(self._h, C.byref(ng), None, None, 1), "groups")
+        gs = np.zeros(max(ng.value, 1), np.int32)
+        gc = np.zeros(max(ng.value, 1), np.int32)
+        self._chk(self._L.sph_get_groups(self._h, C.byref(ng), _ptr(gs), _ptr(gc), 1), "groups")
+        return ng.value, gs[: ng.value], gc[: ng.value]
+
     def smoothing_h(self):
         self._chk(self._L.sph_smoothing_h(self._h), "sph_smoothing_h")
 
@@ -279,6 +288,12 @@ class Context:
 
     def step(self, nsteps=1):
         self._chk(self._L.sph_step(self._h, nsteps), "sph_step")
+
+    def debug_array(self, which: str) -> np.ndarray:
+        k = {"cand_cnt": 0, "ngb_cnt": 1, "retry": 2, "hcand": 3, "p0_h": 4, "p1_m": 5}[which]
+        out = np.zeros(self.n, np.float64 if k >= 3 else np.int32)
+        self._chk(self._L.sph_debug_copy(self._h, k, _ptr(out), 1), "debug_copy")
+        return out
 
     def phase_times(self) -> dict:
         ms = (C.c_float * 12)()

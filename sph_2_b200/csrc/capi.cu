@@ -25,6 +25,15 @@ int ctx_check_launch(sph_ctx *ctx, const char *what) {
 
 int launch_dt_commit(sph_ctx *ctx);
 
+// blocks for a persistent kernel: every SM filled to its occupancy limit
+int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return ctx->num_sms * per_sm;
+}
+
 namespace {
 
 template <class T>
@@ -136,7 +145,7 @@ int ensure_timing(sph_ctx *ctx) {
 
 #define MARK(k, strm)                                                          \
     do {                                                                       \
-        if (timing) CK(cudaEventRecord(ctx->tev[k], (strm)));                  \
+        if (timing) CK(cudaEventRecordWithFlags(ctx->tev[k], (strm), cudaEventRecordExternal)); \
     } while (0)
 
 // the body of one step, queued on ctx->stream
@@ -164,9 +173,8 @@ int step_body(sph_ctx *ctx) {
     MARK(4, ctx->stream);
     if ((rc = launch_neighbours(ctx))) return rc;
     MARK(5, ctx->stream);
-    if ((rc = launch_density(ctx))) return rc;
+    if ((rc = launch_density_divcurl(ctx))) return rc;
     MARK(6, ctx->stream);
-    if ((rc = launch_divcurl(ctx))) return rc;
     MARK(7, ctx->stream);
     if ((rc = launch_forces(ctx, true, fused, false))) return rc;
     MARK(8, ctx->stream);
@@ -213,7 +221,7 @@ int sph_default_config(sph_config *c) {
     c->precision = SPH_PREC_MIXED;
     c->av_mode = SPH_AV_MG83;
     c->balsara = 0;
-    c->leaf_size = 16;
+    c->leaf_size = 8;
     c->ngb_lanes = 8;
     c->block_size = 256;
     c->max_ngb = 256;
@@ -252,10 +260,15 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     };
     const size_t N = cfg->n_max, NN = 2 * N, K = cfg->max_ngb, C = cfg->n_cloud_max;
     const size_t rs = cfg->precision == SPH_PREC_MIXED ? 16 : 32;  // Real4 bytes
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    // the SPH passes (latency/memory bound) get the high-priority stream, the
+    // compute-bound gravity walk the low-priority one, so the block scheduler
+    // feeds the SPH passes first and fills the rest of each SM with the walk
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess)
         return fail(SPH_ERR_CUDA);
     ctx->own_stream = true;
-    if (cudaStreamCreateWithFlags(&ctx->stream_g, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithPriority(&ctx->stream_g, cudaStreamNonBlocking, prio_low) != cudaSuccess)
         return fail(SPH_ERR_CUDA);
     cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
@@ -292,8 +305,11 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(tmpb, rs * NN); ctx->wB = tmpb;
     DAF(tmpb, rs * NN); ctx->wC = tmpb;
     DAF(ctx->croot, C);
-    const size_t G = N / 32 + C + 1;
-    DAF(ctx->gstart, G); DAF(ctx->gcount, G); DAF(ctx->groot_g, G);
+    const size_t G = N + C + 1;
+    DAF(ctx->gstart, G); DAF(ctx->gcount, G); DAF(ctx->groot_g, G); DAF(ctx->gnode, G);
+    DAF(ctx->gmark, N); DAF(ctx->gpos, N); DAF(ctx->gnode_at, N);
+    DAF(ctx->scan_tmp, N / 1024 + 64);
+    DAF(ctx->d_ngroup, 1);
     DAF(ctx->ngb, K * N); DAF(ctx->ngb_cnt, N);
     DAF(ctx->cand, K * N); DAF(ctx->cand_cnt, N);
     DAF(ctx->retry, N); DAF(ctx->hcand, N);
@@ -301,7 +317,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->status, SPH_NSTATUS);
     DAF(ctx->counters, 2);
     DAF(ctx->work, 16);
-    DAF(ctx->red, std::max<size_t>(N, 8192));
+    DAF(ctx->red, std::max<size_t>(2 * N, 8192));
     if (cudaMemsetAsync(ctx->status, 0, SPH_NSTATUS * sizeof(long long), ctx->stream) ||
         cudaMemsetAsync(ctx->pot, 0, N * sizeof(double), ctx->stream) ||
         cudaMemsetAsync(ctx->agrav, 0, 3 * N * sizeof(double), ctx->stream) ||
@@ -404,16 +420,9 @@ int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, con
     for (int i = 0; i < n; i++) cnt[cl[i]]++;
     ctx->cloud_start_h.assign(ncl + 1, 0);
     for (int k = 0; k < ncl; k++) ctx->cloud_start_h[k + 1] = ctx->cloud_start_h[k] + cnt[k];
-    std::vector<int> gs, gc, gk;
-    for (int k = 0; k < ncl; k++)
-        for (int s = ctx->cloud_start_h[k]; s < ctx->cloud_start_h[k + 1]; s += 32) {
-            gs.push_back(s);
-            gc.push_back(std::min(32, ctx->cloud_start_h[k + 1] - s));
-            gk.push_back(k);
-        }
     ctx->n = n;
     ctx->ncloud = ncl;
-    ctx->ngroup = (int)gs.size();
+    ctx->ngroup = n + ncl;
     ctx->cur = 0;
     cudaStream_t s = ctx->stream;
     cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
@@ -429,11 +438,7 @@ int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, con
     }
     CK(cudaMemcpyAsync(ctx->cloud_start, ctx->cloud_start_h.data(), sizeof(int) * (ncl + 1),
                        cudaMemcpyHostToDevice, s));
-    if (ctx->ngroup) {
-        CK(cudaMemcpyAsync(ctx->gstart, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->gcount, gc.data(), sizeof(int) * gc.size(), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(ctx->groot_g, gk.data(), sizeof(int) * gk.size(), cudaMemcpyHostToDevice, s));
-    }
+    CK(cudaMemsetAsync(ctx->d_ngroup, 0, sizeof(int), s));
     CK(cudaMemsetAsync(ctx->dt_bits, 0xff, sizeof(unsigned long long) * ncl, s));
     {
         std::vector<double> dt0(ncl, ctx->cfg.dt_fixed > 0 ? ctx->cfg.dt_fixed : 0.0);
@@ -784,8 +789,7 @@ int sph_prologue(sph_ctx *ctx) {
     if ((rc = launch_gravity(ctx, ctx->stream, pot))) return rc;
     if ((rc = launch_smoothing_h(ctx))) return rc;
     if ((rc = launch_neighbours(ctx))) return rc;
-    if ((rc = launch_density(ctx))) return rc;
-    if ((rc = launch_divcurl(ctx))) return rc;
+    if ((rc = launch_density_divcurl(ctx))) return rc;
     if ((rc = launch_forces(ctx, true, true, false))) return rc;
     // first dt (fixed or Courant), then u += du/dt dt (sph_mpi4_v4.py:240-244)
     if ((rc = launch_cfl(ctx))) return rc;
@@ -856,6 +860,38 @@ int sph_get_phase_times(sph_ctx *ctx, float *ms) {
     for (int k = 0; k < 11; k++) CK(cudaEventElapsedTime(&ms[k], ctx->tev[k], ctx->tev[k + 1]));
     CK(cudaEventElapsedTime(&ms[11], ctx->tev[13], ctx->tev[14]));
     return SPH_NPHASE;
+}
+
+__global__ void k_dbg_w(int n, const double4 *p0, const void *p1, int mixed, double *out0,
+                        double *out1) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out0[i] = p0[i].w;
+    out1[i] = mixed ? (double)((const float4 *)p1)[i].w : ((const double4 *)p1)[i].w;
+}
+
+int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out || which < 0 || which > 5) return SPH_ERR_ARG;
+    if (which >= 4) {
+        const int n = ctx->n;
+        k_dbg_w<<<div_up(n, 256), 256, 0, ctx->stream>>>(n, ctx->p0, ctx->p1,
+                                                        ctx->cfg.precision == SPH_PREC_MIXED,
+                                                        ctx->red, ctx->red + n);
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaMemcpy(out, ctx->red + (which == 4 ? 0 : n), sizeof(double) * n,
+                      host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+        return SPH_OK;
+    }
+    const void *src = which == 0 ? (const void *)ctx->cand_cnt
+                      : which == 1 ? (const void *)ctx->ngb_cnt
+                      : which == 2 ? (const void *)ctx->retry
+                                   : (const void *)ctx->hcand;
+    const size_t bytes = (which == 3 ? sizeof(double) : sizeof(int)) * ctx->n;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(out, src, bytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    return SPH_OK;
 }
 
 int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count) {

@@ -23,7 +23,7 @@
 namespace {
 
 constexpr int WALK_WARPS = 4;
-constexpr int WSTK = 2048;
+constexpr int WSTK = 1024;
 constexpr unsigned FULL = 0xffffffffu;
 
 template <class R> __device__ __forceinline__ R rsq(R x);
@@ -66,7 +66,7 @@ __device__ __forceinline__ float box_d2(float x0, float y0, float z0, float x1, 
 
 template <class R, bool POT>
 __global__ void __launch_bounds__(WALK_WARPS * 32)
-    k_walk(int ngroup, const int *__restrict__ gstart, const int *__restrict__ gcount,
+    k_walk(const int *__restrict__ ngroup_p, const int *__restrict__ gstart, const int *__restrict__ gcount,
            const int *__restrict__ gcloud, const int *__restrict__ croot,
            const typename R4<R>::T *__restrict__ pw, const typename R4<R>::T *__restrict__ wA,
            const typename R4<R>::T *__restrict__ wB, const typename R4<R>::T *__restrict__ wC,
@@ -80,11 +80,11 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
     WalkSmem<R> &S = smem[w];
     const unsigned lt = (1u << lane) - 1u;
     int maxsp = 0;
-    for (;;) {
-        int g = 0;
-        if (lane == 0) g = (int)atomicAdd(work, 1u);
-        g = __shfl_sync(FULL, g, 0);
-        if (g >= ngroup) break;
+    const int ngroup = *ngroup_p;
+    // grid-stride over groups: many short blocks, so the block scheduler can
+    // interleave this compute-bound walk with the memory-bound SPH passes
+    // running on the other stream
+    for (int g = blockIdx.x * WALK_WARPS + w; g < ngroup; g += gridDim.x * WALK_WARPS) {
         const int s0 = gstart[g], gc = gcount[g];
         const bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
@@ -345,19 +345,12 @@ __global__ void __launch_bounds__(256)
 
 template <class R, bool POT>
 int run_walk(sph_ctx *ctx, cudaStream_t s) {
-    static int blocks_per_sm = -1;
-    if (blocks_per_sm < 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_walk<R, POT>,
-                                                          WALK_WARPS * 32, 0) != cudaSuccess ||
-            blocks_per_sm < 1)
-            blocks_per_sm = 1;
-    }
-    int grid = ctx->num_sms * blocks_per_sm;
-    grid = min(grid, div_up(ctx->ngroup, WALK_WARPS));
-    if (grid < 1) grid = 1;
+    // groups hold 1..32 particles (about 20 on average); size the grid for
+    // one group per warp at 16 particles per group, the rest by grid stride
+    int grid = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
     const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
     k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
-        ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
+        ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
         (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
         (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->first,
         ctx->last, ctx->child, ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
@@ -369,7 +362,6 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
 
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot) {
     if (ctx->n <= 0) return SPH_OK;
-    CK(cudaMemsetAsync(ctx->work, 0, sizeof(unsigned), s));
     CK(cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), s));
     int rc;
     if (ctx->cfg.precision == SPH_PREC_MIXED)

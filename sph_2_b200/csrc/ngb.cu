@@ -6,17 +6,20 @@
 // host exit on failure) and smoothing_h_ngb (hfvCLibs_v7_hfv_v2.h:367-455: a
 // count-based +-coeff*2h iteration of up to 200 rounds over the list).
 //
-// Search: one warp per group of 32 consecutive (Morton-ordered) particles of
-// one cloud.  The warp walks the tree 32 nodes at a time with the group's box
-// (LIFO stack in shared memory); buckets that can hold neighbours are
-// flattened into a shared list of candidate particles, staged 32 at a time in
-// shared memory, and every lane tests the staged candidates against its own
-// particle with the exact FP64 predicate.  Rows are written in traversal order
-// (deterministic); sph_get_neighbours exports them sorted.
+// Search: one warp per group (a tree node of at most 32 Morton-contiguous
+// particles of one cloud).  The warp walks the tree 32 nodes at a time with the
+// group's box (LIFO stack in shared memory); buckets that can hold neighbours
+// are flattened into a shared list of candidate particles, staged 32 at a time
+// in shared memory, and every lane tests the staged candidates against its own
+// particle.  Rows are written in traversal order (deterministic);
+// sph_get_neighbours exports them sorted.
 //
-// h iteration: one warp per particle keeps the candidate distances and masses
-// in registers and runs a bracketed Newton iteration on
-// (4pi/3)(2h)^3 rho(h) = n_ngb m  with FP64 updates and convergence test.
+// h iteration (fused with the candidate search): after a group's candidate rows
+// are written, the same warp takes the group's particles one at a time, keeps
+// that particle's candidate distances and masses in registers (a few per lane)
+// and runs a bracketed Newton iteration on (4pi/3)(2h)^3 rho(h) = n_ngb m with
+// FP64 updates and convergence test.  Particles whose h outgrows the candidate
+// radius are flagged and searched again in the next round.
 #include "sph_internal.cuh"
 
 namespace {
@@ -40,48 +43,42 @@ __device__ __forceinline__ double wmax(double v) {
     return v;
 }
 
-// MODE 0: candidates r^2 <= (2 hc_i)^2 (gather radius of the h iteration)
+struct SearchArgs {
+    const int *gstart, *gcount, *gcloud, *croot;
+    double4 *p0;
+    const double4 *sA, *sB;  // node box min (+h_max), box max
+    const int *first, *last, *child;
+    int leaf_size, K;
+    int *rows, *cnt;
+    long long *status;
+};
+
+// Walk the tree for group g and write the rows of the active lanes.
+// MODE 0: candidates r^2 <= ri^2 (ri = 2 hc_i, the h iteration's gather radius)
 // MODE 1: exact lists |r|^2 <= (h_i + h_j)^2
 template <int MODE>
-__global__ void __launch_bounds__(SEARCH_WARPS * 32)
-    k_search(int ngroup, const int *__restrict__ gstart, const int *__restrict__ gcount,
-             const int *__restrict__ gcloud, const int *__restrict__ croot,
-             const double4 *__restrict__ p0,
-             const double *__restrict__ hc, const int *__restrict__ need,
-             const double4 *__restrict__ sA, const double4 *__restrict__ sB,
-             const int *__restrict__ first, const int *__restrict__ last,
-             const int *__restrict__ child, int leaf_size, int K, int *__restrict__ rows,
-             int *__restrict__ cnt, long long *status) {
-    __shared__ SearchSmem smem[SEARCH_WARPS];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = blockIdx.x * SEARCH_WARPS + w;
-    if (g >= ngroup) return;  // warp-uniform
-    SearchSmem &S = smem[w];
+__device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A, int g, bool act,
+                                             int i, const double4 &pi, double ri) {
+    const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const int s0 = gstart[g], gc = gcount[g];
-    bool act = lane < gc;
-    const int i = s0 + (act ? lane : 0);
-    if (need) act = act && need[i];
-    if (!__any_sync(FULL, act)) return;
-    const double4 pi = p0[i];
-    const double ri = MODE == 0 ? 2.0 * hc[i] : pi.w;
     const double gx0 = wmin(act ? pi.x : INFINITY), gy0 = wmin(act ? pi.y : INFINITY),
                  gz0 = wmin(act ? pi.z : INFINITY);
     const double gx1 = wmax(act ? pi.x : -INFINITY), gy1 = wmax(act ? pi.y : -INFINITY),
                  gz1 = wmax(act ? pi.z : -INFINITY);
     const double rmax = wmax(act ? ri : 0.0);
     const double ri2 = ri * ri;
+    const int K = A.K;
     int count = 0;
     int sp = 1, nflat = 0;
     bool overflow = false;
-    if (lane == 0) S.stk[0] = croot[gcloud[g]];
+    if (lane == 0) S.stk[0] = A.croot[A.gcloud[g]];
     __syncwarp();
 
     auto process = [&](int m) {
         int j = 0;
         if (lane < m) {
             j = S.flat[lane];
-            S.stage[lane] = p0[j];
+            S.stage[lane] = A.p0[j];
         }
         __syncwarp();
         for (int k = 0; k < m; k++) {
@@ -95,7 +92,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
                 hit = ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w);
             }
             if (act && hit) {
-                if (count < K) rows[(size_t)i * K + count] = jj;
+                if (count < K) A.rows[(size_t)i * K + count] = jj;
                 count++;
             }
         }
@@ -110,9 +107,9 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
             bool open = false;
             if (lane < take) {
                 nd = S.stk[sp + lane];
-                const double4 a = sA[nd], b = sB[nd];
-                f = first[nd];
-                cn = last[nd] - f + 1;
+                const double4 a = A.sA[nd], b = A.sB[nd];
+                f = A.first[nd];
+                cn = A.last[nd] - f + 1;
                 double ex = fmax(fmax(a.x - gx1, gx0 - b.x), 0.0);
                 double ey = fmax(fmax(a.y - gy1, gy0 - b.y), 0.0);
                 double ez = fmax(fmax(a.z - gz1, gz0 - b.z), 0.0);
@@ -121,14 +118,14 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
                 open = d2 <= reach * reach * (1.0 + 1e-12);
             }
             __syncwarp();
-            const bool leafy = cn <= leaf_size;
+            const bool leafy = cn <= A.leaf_size;
             const unsigned pm = __ballot_sync(FULL, open && !leafy);
             const int npush = 2 * __popc(pm);
             if (sp + npush <= SSTK) {
                 if (open && !leafy) {
                     int pos = sp + 2 * __popc(pm & lt);
-                    S.stk[pos] = child[2 * nd + 1];
-                    S.stk[pos + 1] = child[2 * nd];
+                    S.stk[pos] = A.child[2 * nd + 1];
+                    S.stk[pos + 1] = A.child[2 * nd];
                 }
                 sp += npush;
             } else {
@@ -146,7 +143,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
                 __syncwarp();
                 while (nflat >= 32) {
                     process(32);
-                    int v0 = S.flat[32 + lane], v1 = lane + 64 < 96 ? S.flat[64 + lane] : 0;
+                    int v0 = S.flat[32 + lane], v1 = S.flat[64 + lane];
                     __syncwarp();
                     if (lane + 32 < nflat) S.flat[lane] = v0;
                     if (lane + 64 < nflat) S.flat[32 + lane] = v1;
@@ -161,10 +158,26 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         }
     }
     if (act) {
-        cnt[i] = min(count, K);
-        if (count > K) status_add(status, SPH_S_NGB_OVERFLOW, 1);
+        A.cnt[i] = min(count, K);
+        if (count > K) status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
     }
-    if (overflow && lane == 0) status_add(status, SPH_S_STACK_OVERFLOW, 1);
+    if (overflow && lane == 0) status_add(A.status, SPH_S_STACK_OVERFLOW, 1);
+    __syncwarp();
+}
+
+// exact lists for every particle
+__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+    k_lists(const int *__restrict__ ngroup_p, SearchArgs A) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+        const int s0 = A.gstart[g], gc = A.gcount[g];
+        const bool act = lane < gc;
+        const int i = s0 + (act ? lane : 0);
+        const double4 pi = A.p0[i];
+        group_search<1>(smem[w], A, g, act, i, pi, pi.w);
+    }
 }
 
 __global__ void k_h_init(int n, const double *__restrict__ h, double *__restrict__ hc,
@@ -175,40 +188,42 @@ __global__ void k_h_init(int n, const double *__restrict__ h, double *__restrict
     retry[i] = 1;
 }
 
-// one warp per particle; SLOTS candidates per lane
+struct NewtonArgs {
+    const void *p1;  // Real4 (v, m)
+    double *h_out, *hc;
+    int *retry;
+    double n_ngb, tol, grow;
+    int max_iter, last_round;
+};
+
+// Newton iteration of particle i by the whole warp (candidate row of i).
 template <class R, int SLOTS>
-__global__ void __launch_bounds__(128)
-    k_newton(int n, double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
-             const int *__restrict__ rows, const int *__restrict__ cnt, int K,
-             double *__restrict__ h_out, double *__restrict__ hc, int *__restrict__ retry,
-             double n_ngb, double tol, int max_iter, double grow, int last_round,
-             long long *status) {
+__device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs &B, int i) {
+    typedef typename R4<R>::T V4;
+    const V4 *p1 = (const V4 *)B.p1;
     const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    bool act = i < n && retry[i];
-    if (!__any_sync(FULL, act)) return;  // warp-uniform (one particle per warp)
-    const double4 pi = p0[i];
-    const int c = cnt[i];
+    const double4 pi = A.p0[i];
+    const int c = A.cnt[i];
     const double mi = (double)p1[i].w;
     R rj[SLOTS], mj[SLOTS];
 #pragma unroll
     for (int s = 0; s < SLOTS; s++) {
-        int k = lane + 32 * s;
+        const int k = lane + 32 * s;
         rj[s] = R(1e30);
         mj[s] = R(0);
         if (k < c) {
-            int j = rows[(size_t)i * K + k];
-            double4 pj = p0[j];
-            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const int j = A.rows[(size_t)i * A.K + k];
+            const double4 pj = A.p0[j];
+            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             rj[s] = (R)sqrt(dx * dx + dy * dy + dz * dz);
             mj[s] = (R)p1[j].w;
         }
     }
-    const double cap = hc[i];
+    const double cap = B.hc[i];
     const double cfac = 4.0 * SPH_PI / 3.0 * 8.0;
     double h = pi.w, lo = 0.0, hi = INFINITY;
     bool ok = false, need = false;
-    for (int it = 1; it <= max_iter; it++) {
+    for (int it = 1; it <= B.max_iter; it++) {
         if (h > cap) {  // 2h would pass the candidate radius 2*cap
             need = true;
             break;
@@ -217,14 +232,14 @@ __global__ void __launch_bounds__(128)
         KSum<R> S, D;
 #pragma unroll
         for (int s = 0; s < SLOTS; s++) {
-            R q = rj[s] * inv_h;
+            const R q = rj[s] * inv_h;
             if (q < R(2)) {
                 R w, dw;
                 if (q <= R(1)) {
                     w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
                     dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
                 } else {
-                    R t = R(2) - q;
+                    const R t = R(2) - q;
                     w = R(0.25) * t * t * t;
                     dw = R(1.5) * t * t * (R(1) - q);
                 }
@@ -236,10 +251,17 @@ __global__ void __launch_bounds__(128)
         const double h3 = h * h * h;
         const double rho = SPH_SIG / h3 * Ssum;
         const double drho = -SPH_SIG / (h3 * h) * Dsum;
-        const double f = cfac * h3 * rho - n_ngb * mi;
+        const double f = cfac * h3 * rho - B.n_ngb * mi;
         const double fp = cfac * h * h * (3.0 * rho + h * drho);
         if (f < 0.0) lo = h; else hi = h;
         double hn = fp > 0.0 ? h - f / fp : -1.0;
+        // a Newton step below the tolerance is accepted before any bracket
+        // test: in FP64 it can round to exactly h (= a bracket end)
+        if (fp > 0.0 && fabs(f / fp) < B.tol * h) {
+            h = hn;
+            ok = true;
+            break;
+        }
         // at most a factor 1.25 per iteration (keeps retries inside the rows)
         if (hn > 1.25 * h) hn = 1.25 * h;
         if (hn > 0.0 && hn < h / 1.25) hn = h / 1.25;
@@ -250,28 +272,49 @@ __global__ void __launch_bounds__(128)
         }
         const double dh = hn - h;
         h = hn;
-        if (fabs(dh) < tol * fabs(h - dh)) {
+        if (fabs(dh) < B.tol * fabs(h - dh)) {
             ok = true;
             break;
         }
     }
     if (lane == 0) {
-        if (need && !last_round) {
-            hc[i] = h * grow;
-            retry[i] = 1;
+        if (need && !B.last_round) {
+            B.hc[i] = h * B.grow;
+            B.retry[i] = 1;
         } else {
-            retry[i] = 0;
-            if (!ok) status_add(status, SPH_S_H_NOCONV, 1);
+            B.retry[i] = 0;
+            if (!ok) status_add(A.status, SPH_S_H_NOCONV, 1);
         }
-        if (need) status_add(status, SPH_S_H_RETRY, 1);
-        if (!need) {
-            h_out[i] = h;
-            p0[i].w = h;
-        } else {
-            // keep the last evaluated h (inside the candidate radius) for the restart
-            double hk = fmin(h, cap);
-            h_out[i] = hk;
-            p0[i].w = hk;
+        if (need) status_add(A.status, SPH_S_H_RETRY, 1);
+        B.h_out[i] = h;
+        A.p0[i].w = h;  // p0 is written only by the warp owning particle i
+    }
+    __syncwarp();
+}
+
+// candidate search + Newton iteration for the flagged particles of each group
+template <class R, int SLOTS>
+__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+    k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+        const int s0 = A.gstart[g], gc = A.gcount[g];
+        bool act = lane < gc;
+        const int i = s0 + (act ? lane : 0);
+        act = act && B.retry[i];
+        const unsigned todo = __ballot_sync(FULL, act);
+        if (!todo) continue;
+        const double4 pi = A.p0[i];
+        group_search<0>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
+        __threadfence_block();
+        __syncwarp();
+        unsigned t = todo;
+        while (t) {
+            const int l = __ffs(t) - 1;
+            t &= t - 1;
+            newton_one<R, SLOTS>(A, B, s0 + l);
         }
     }
 }
@@ -294,6 +337,26 @@ __global__ void k_export(int n, const int *__restrict__ rows, const int *__restr
     }
 }
 
+SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
+    SearchArgs A;
+    A.gstart = ctx->gstart;
+    A.gcount = ctx->gcount;
+    A.gcloud = ctx->groot_g;
+    A.croot = ctx->croot;
+    A.p0 = ctx->p0;
+    A.sA = (const double4 *)ctx->node_box;
+    A.sB = A.sA + 2 * (size_t)ctx->cfg.n_max;
+    A.first = ctx->first;
+    A.last = ctx->last;
+    A.child = ctx->child;
+    A.leaf_size = ctx->cfg.leaf_size;
+    A.K = ctx->cfg.max_ngb;
+    A.rows = rows;
+    A.cnt = cnt;
+    A.status = ctx->status;
+    return A;
+}
+
 }  // namespace
 
 static const double H_GROW = 1.15;
@@ -303,40 +366,28 @@ int launch_smoothing_h(sph_ctx *ctx) {
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
-    const int K = ctx->cfg.max_ngb;
-    const double4 *boxA = (const double4 *)ctx->node_box;
-    const double4 *boxB = boxA + 2 * (size_t)ctx->cfg.n_max;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->hcand, ctx->retry, H_GROW);
     const int rounds = ctx->prologue_done ? 3 : 8;
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    SearchArgs A = search_args(ctx, ctx->cand, ctx->cand_cnt);
+    NewtonArgs B;
+    B.p1 = ctx->p1;
+    B.h_out = ctx->st[c][ST_H];
+    B.hc = ctx->hcand;
+    B.retry = ctx->retry;
+    B.n_ngb = ctx->cfg.n_ngb;
+    B.tol = ctx->cfg.h_tol;
+    B.grow = H_GROW;
+    B.max_iter = ctx->cfg.h_max_iter;
+    const bool wide = (ctx->cfg.max_ngb + 31) / 32 > 8;
     for (int r = 0; r < rounds; r++) {
-        k_search<0><<<div_up(ctx->ngroup, SEARCH_WARPS), SEARCH_WARPS * 32, 0, s>>>(
-            ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot, ctx->p0, ctx->hcand, ctx->retry,
-            boxA, boxB, ctx->first, ctx->last, ctx->child, ctx->cfg.leaf_size, K, ctx->cand,
-            ctx->cand_cnt, ctx->status);
-        const int last = r == rounds - 1;
-        const int slots = (K + 31) / 32;
+        B.last_round = r == rounds - 1;
         if (ctx->cfg.precision == SPH_PREC_MIXED) {
-            if (slots <= 8)
-                k_newton<float, 8><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
-                    n, ctx->p0, (const float4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
-                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
-                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
-            else
-                k_newton<float, 16><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
-                    n, ctx->p0, (const float4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
-                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
-                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+            if (!wide) k_cand_newton<float, 8><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+            else k_cand_newton<float, 16><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
         } else {
-            if (slots <= 8)
-                k_newton<double, 8><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
-                    n, ctx->p0, (const double4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
-                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
-                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
-            else
-                k_newton<double, 16><<<div_up((long long)n * 32, 128), 128, 0, s>>>(
-                    n, ctx->p0, (const double4 *)ctx->p1, ctx->cand, ctx->cand_cnt, K,
-                    ctx->st[c][ST_H], ctx->hcand, ctx->retry, ctx->cfg.n_ngb, ctx->cfg.h_tol,
-                    ctx->cfg.h_max_iter, H_GROW, last, ctx->status);
+            if (!wide) k_cand_newton<double, 8><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+            else k_cand_newton<double, 16><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
         }
     }
     ctx->lists_ok = false;
@@ -348,13 +399,9 @@ int launch_neighbours(sph_ctx *ctx) {
     if (n <= 0) return SPH_OK;
     int rc = launch_refit_hmax(ctx);
     if (rc) return rc;
-    cudaStream_t s = ctx->stream;
-    const double4 *boxA = (const double4 *)ctx->node_box;
-    const double4 *boxB = boxA + 2 * (size_t)ctx->cfg.n_max;
-    k_search<1><<<div_up(ctx->ngroup, SEARCH_WARPS), SEARCH_WARPS * 32, 0, s>>>(
-        ctx->ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot, ctx->p0, nullptr, nullptr, boxA, boxB,
-        ctx->first, ctx->last, ctx->child, ctx->cfg.leaf_size, ctx->cfg.max_ngb, ctx->ngb,
-        ctx->ngb_cnt, ctx->status);
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    k_lists<<<grid, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup,
+                                                         search_args(ctx, ctx->ngb, ctx->ngb_cnt));
     ctx->lists_ok = true;
     ctx->rho_ok = ctx->divcurl_ok = false;
     return ctx_check_launch(ctx, "neighbours");

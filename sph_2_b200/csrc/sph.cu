@@ -109,6 +109,76 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// density, EOS, div v, |curl v| and the Balsara factor in one pass: the
+// div/curl sums need only the particle's own density (sum m_j/rho_i ...), so
+// they are accumulated unnormalised beside the density sum and divided by
+// rho_i at the end
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_density_divcurl(int n, const double4 *__restrict__ p0,
+                      const typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ p2,
+                      const int *__restrict__ rows, const int *__restrict__ cnt, int K,
+                      const double *__restrict__ u, double gamma, int balsara,
+                      double *__restrict__ rho_out, double *__restrict__ P_out,
+                      double *__restrict__ c_out, double *__restrict__ divV,
+                      double *__restrict__ curlV) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    const bool valid = i < n;
+    KSum<R> S, s, cx, cy, cz;
+    double hi = 1.0;
+    if (valid) {
+        const double4 pi = p0[i];
+        hi = pi.w;
+        const typename R4<R>::T vi = p1[i];
+        const int c = cnt[i];
+        const int *row = rows + (size_t)i * K;
+        for (int k = sl; k < c; k += LANES) {
+            const int j = row[k];
+            const double4 pj = p0[j];
+            const typename R4<R>::T vj = p1[j];
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R hij = (R)(0.5 * (pi.w + pj.w));
+            const R inv = R(1) / hij;
+            const R i2 = inv * inv;
+            const R q = rr * inv;
+            const R mj = vj.w;
+            S.add(mj * kern_w<R>(q, i2 * inv));
+            const R nW = kern_nw<R>(q, i2 * i2 * inv);
+            const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+            const R ux = vi.x - vj.x, uy = vi.y - vj.y, uz = vi.z - vj.z;
+            s.add(-mj * (ux * gx + uy * gy + uz * gz));
+            cx.add(mj * (uy * gz - uz * gy));
+            cy.add(mj * (uz * gx - ux * gz));
+            cz.add(mj * (ux * gy - uy * gx));
+        }
+    }
+    const double rho = seg_sum<LANES>(S.value());
+    const double Sd = seg_sum<LANES>(s.value());
+    const double X = seg_sum<LANES>(cx.value()), Y = seg_sum<LANES>(cy.value()),
+                 Z = seg_sum<LANES>(cz.value());
+    if (valid && sl == 0) {
+        const double ui = u[i];
+        const double P = (gamma - 1.0) * rho * ui;
+        const double cs = sqrt(gamma * (gamma - 1.0) * ui);
+        const double inv_rho = 1.0 / rho;
+        const double d = fabs(Sd * inv_rho);
+        const double cv = sqrt(X * X + Y * Y + Z * Z) * inv_rho;
+        rho_out[i] = rho;
+        P_out[i] = P;
+        c_out[i] = cs;
+        divV[i] = d;
+        curlV[i] = cv;
+        typename R4<R>::T q;
+        q.x = (R)rho;
+        q.y = (R)(P / (rho * rho));
+        q.z = (R)cs;
+        q.w = balsara ? (R)(d / (d + cv + 0.0001 * cs / hi)) : R(0);
+        p2[i] = q;
+    }
+}
+
 // acc_i = -sum m_j (P_i/rho_i^2 + P_j/rho_j^2 + PI_ij) gradW_ij,
 // du_i  =  sum m_j (P_i/rho_i^2 + PI_ij/2) v_ij . gradW_ij,
 // vsig_i = max_j (c_i + c_j - 3 w_ij), w_ij = v_ij.r_ij/(r_ij + 1e-5).
@@ -229,6 +299,16 @@ int run_density(sph_ctx *ctx) {
     return SPH_OK;
 }
 template <class R, int L>
+int run_density_divcurl(sph_ctx *ctx) {
+    const int n = ctx->n, c = ctx->cur;
+    const int bs = ctx->cfg.block_size;
+    k_density_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb,
+        ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara,
+        ctx->rho, ctx->P, ctx->c, ctx->divV, ctx->curlV);
+    return SPH_OK;
+}
+template <class R, int L>
 int run_divcurl(sph_ctx *ctx) {
     const int n = ctx->n;
     const int bs = ctx->cfg.block_size;
@@ -249,9 +329,6 @@ int run_force(sph_ctx *ctx, bool acc, bool du) {
     return SPH_OK;
 }
 
-template <template <class, int> class F, class R>
-struct Dispatch;
-
 #define SPH_DISPATCH_LANES(FN, R, ctx, ...)                 \
     switch ((ctx)->cfg.ngb_lanes) {                         \
         case 4: rc = FN<R, 4>(ctx, ##__VA_ARGS__); break;   \
@@ -270,6 +347,17 @@ int launch_density(sph_ctx *ctx) {
     if (rc) return rc;
     ctx->rho_ok = true;
     return ctx_check_launch(ctx, "density");
+}
+
+int launch_density_divcurl(sph_ctx *ctx) {
+    if (ctx->n <= 0) return SPH_OK;
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_density_divcurl, float, ctx); }
+    else { SPH_DISPATCH_LANES(run_density_divcurl, double, ctx); }
+    if (rc) return rc;
+    ctx->rho_ok = ctx->divcurl_ok = true;
+    ctx->p2_dirty = false;
+    return ctx_check_launch(ctx, "density_divcurl");
 }
 
 int launch_divcurl(sph_ctx *ctx) {

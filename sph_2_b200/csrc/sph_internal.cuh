@@ -81,7 +81,10 @@ struct sph_ctx {
     void *wA = nullptr, *wB = nullptr, *wC = nullptr;  // Real4 walk records
     int *croot = nullptr;                              // per cloud root node
     int *gstart = nullptr, *gcount = nullptr, *groot_g = nullptr;  // groups: start, size, cloud id
-    int ngroup = 0;
+    int *gnode = nullptr;                       // group -> tree node
+    int *gmark = nullptr, *gpos = nullptr, *gnode_at = nullptr, *scan_tmp = nullptr;
+    int *d_ngroup = nullptr;                    // number of groups (device)
+    int ngroup = 0;                             // capacity of the group table
     bool tree_ok = false;
 
     // neighbours
@@ -223,12 +226,16 @@ __device__ __forceinline__ void status_add(long long *status, int which, long lo
 
 // ---- host-side launch helpers implemented per translation unit ----
 int launch_sort(sph_ctx *ctx);
+int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
+int launch_groups(sph_ctx *ctx);
+int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 int launch_tree(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx);
 int launch_smoothing_h(sph_ctx *ctx);
 int launch_neighbours(sph_ctx *ctx);
 int launch_density(sph_ctx *ctx);
 int launch_divcurl(sph_ctx *ctx);
+int launch_density_divcurl(sph_ctx *ctx);
 int launch_forces(sph_ctx *ctx, bool want_acc, bool want_du, bool update_u);
 int launch_repack_p2(sph_ctx *ctx);
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot);

@@ -231,6 +231,8 @@ int launch_tree(sph_ctx *ctx) {
             n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
             ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
     }
+    int rc = launch_groups(ctx);
+    if (rc) return rc;
     ctx->tree_ok = true;
     return ctx_check_launch(ctx, "tree");
 }
