@@ -42,7 +42,7 @@ class SphConfig(C.Structure):
         ("n_max", C.c_int32), ("n_cloud_max", C.c_int32), ("precision", C.c_int32),
         ("av_mode", C.c_int32), ("balsara", C.c_int32), ("leaf_size", C.c_int32),
         ("ngb_lanes", C.c_int32), ("block_size", C.c_int32), ("max_ngb", C.c_int32),
-        ("h_max_iter", C.c_int32), ("flags", C.c_int32), ("walk_warps", C.c_int32),
+        ("h_max_iter", C.c_int32), ("flags", C.c_int32), ("walk_blocks", C.c_int32),
         ("n_ngb", C.c_double), ("h_tol", C.c_double), ("gamma", C.c_double),
         ("alpha", C.c_double), ("beta", C.c_double), ("eta", C.c_double), ("G", C.c_double),
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),

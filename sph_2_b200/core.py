@@ -33,7 +33,7 @@ class Config:
     max_ngb: int = 256
     h_max_iter: int = 64
     flags: int = 0
-    walk_warps: int = 4
+    walk_blocks: int = 0
     n_ngb: float = 64.0
     h_tol: float = 1e-3
     gamma: float = 5.0 / 3.0

@@ -80,6 +80,7 @@ int check_cfg(const sph_config *c) {
     if (!valid_lanes(c->ngb_lanes)) return SPH_ERR_ARG;
     if (c->block_size < 64 || c->block_size > 1024 || c->block_size % 32) return SPH_ERR_ARG;
     if (c->max_ngb < 32 || c->max_ngb > 512) return SPH_ERR_ARG;
+    if (c->walk_blocks < 0 || c->walk_blocks > 64) return SPH_ERR_ARG;
     if (c->h_max_iter < 1 || c->h_max_iter > 1000) return SPH_ERR_ARG;
     if (!(c->theta > 0.0 && c->theta <= 1.0)) return SPH_ERR_ARG;
     if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
@@ -227,7 +228,7 @@ int sph_default_config(sph_config *c) {
     c->max_ngb = 256;
     c->h_max_iter = 64;
     c->flags = 0;
-    c->walk_warps = 4;
+    c->walk_blocks = 0;
     c->n_ngb = 64.0;
     c->h_tol = 1e-3;
     c->gamma = 5.0 / 3.0;
@@ -385,6 +386,7 @@ int sph_set_params(sph_ctx *ctx, const sph_config *c) {
     t.G = c->G; t.eps = c->eps; t.theta = c->theta; t.courant = c->courant;
     t.dt_max = c->dt_max; t.dt_fixed = c->dt_fixed;
     t.ngb_lanes = c->ngb_lanes; t.block_size = c->block_size; t.leaf_size = c->leaf_size;
+    t.walk_blocks = c->walk_blocks;
     int rc = check_cfg(&t);
     if (rc) return rc;
     if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size) ctx->tree_ok = false;

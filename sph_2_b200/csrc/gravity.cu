@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                 const R qy = c.x * dx + b.y * dy + c.z * dz;
                 const R qz = c.y * dx + c.z * dy + b.z * dz;
                 const R dqd = dx * qx + dy * qy + dz * qz;
-                const R tr = b.x + b.y + b.z;
+                const R tr = c.w;
                 const R s = -a.w * g3 + R(1.5) * tr * g5 - R(7.5) * dqd * g7;
                 const R t5 = R(3) * g5;
                 sx += s * dx + t5 * qx;
@@ -348,6 +348,7 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
     // groups hold 1..32 particles (about 20 on average); size the grid for
     // one group per warp at 16 particles per group, the rest by grid stride
     int grid = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
+    if (ctx->cfg.walk_blocks > 0) grid = min(grid, ctx->num_sms * ctx->cfg.walk_blocks);
     const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
     k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
         ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,

@@ -214,8 +214,8 @@ __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs
         if (k < c) {
             const int j = A.rows[(size_t)i * A.K + k];
             const double4 pj = A.p0[j];
-            const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            rj[s] = (R)sqrt(dx * dx + dy * dy + dz * dz);
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            rj[s] = sqrt(dx * dx + dy * dy + dz * dz);
             mj[s] = (R)p1[j].w;
         }
     }

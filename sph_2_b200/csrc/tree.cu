@@ -69,7 +69,9 @@ __device__ __forceinline__ void write_walk(int nd, const double *o, double r2, d
     typename R4<R>::T a, b, c;
     a.x = (R)o[0]; a.y = (R)o[1]; a.z = (R)o[2]; a.w = (R)o[3];
     b.x = (R)o[4]; b.y = (R)o[5]; b.z = (R)o[6]; b.w = (R)r2;
-    c.x = (R)o[7]; c.y = (R)o[8]; c.z = (R)o[9]; c.w = (R)hm;
+    c.x = (R)o[7]; c.y = (R)o[8]; c.z = (R)o[9];
+    c.w = (R)(o[4] + o[5] + o[6]);  // trace of the second moments
+    (void)hm;
     wA[nd] = a;
     wB[nd] = b;
     wC[nd] = c;
