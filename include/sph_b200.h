@@ -299,6 +299,25 @@ int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
  * TFLOP/s (2 flops per FMA), the denominator for FP32-bound kernels */
 int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
 
+/* ---- allocation-free Morton order ---- */
+/* No counterpart in the reference.  For callers that must not allocate device
+ * memory when they need the particle order -- e.g. code whose device memory is
+ * all held by another framework's caching allocator, or that cannot afford the
+ * implicit synchronisation of cudaMalloc: 63-bit Morton keys of one cloud
+ * (keys[i], input order) and the stable sort permutation (perm[s] = input
+ * index of sorted slot s), the same definitions as sph_sort / sph_get_sort.
+ * x, y, z, keys and perm are caller-owned device arrays; nothing is allocated.
+ * Scratch is a fixed array compiled into the library (6.4 MB, held on
+ * every GPU that loads the library until the process exits), so
+ * n <= SPH_NOALLOC_MAX_N (SPH_ERR_CAPACITY above it).  All calls share that
+ * array: calls that overlap on the GPU race.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Work is queued on cuda_stream (NULL: the legacy
+ * default stream) of the current device. */
+#define SPH_NOALLOC_MAX_N 262144
+int sph_morton_sort_noalloc(const double *x, const double *y, const double *z, int32_t n,
+                            uint64_t *keys, int32_t *perm, void *cuda_stream);
+
 /* The same entry points a single GPU runs, for a rank of a multi-GPU job
  * that owns a slice of the ensemble: nothing here talks to other ranks. */
 

@@ -35,6 +35,7 @@ FLAG_TIMING = 32
 PHASES = ["kick_drift", "sort", "tree", "smoothing_h", "neighbours", "density", "divcurl",
           "forces", "wait_kick", "dudt", "update_dt", "gravity"]
 MLP_NPARAM = 3 * 64 + 64 + 64 * 64 + 64 + 64 + 1
+NOALLOC_MAX_N = 262144
 
 
 class SphConfig(C.Structure):
@@ -117,6 +118,7 @@ SIGNATURES = [
     ("sph_get_phase_times", C.c_int, [_P, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),
+    ("sph_morton_sort_noalloc", C.c_int, [_P, _P, _P, _I, _P, _P, _P]),
     ("sph_prologue", C.c_int, [_P]),
     ("sph_step", C.c_int, [_P, _I]),
 ]
