@@ -266,11 +266,16 @@ int sph_mlp_forward(sph_ctx *ctx, int32_t n, const float *X, float *y, int32_t h
  * the loss; forward+backward on tensor cores */
 int sph_mlp_grad(sph_ctx *ctx, int32_t n, const float *X, const float *t, float *grad,
                  float *loss, int32_t host);
-/* nsteps of Adam (lr, b1, b2, eps) on minibatches of size batch drawn in
- * order from device arrays X[n*3], t[n]; writes the mean loss of the last
- * epoch to loss */
+/* nsteps of Adam (lr; beta1 0.9, beta2 0.999, eps 1e-8) on consecutive
+ * minibatches of size batch of the device arrays X[n*3], t[n] (wrapping);
+ * writes the loss of the last minibatch to *loss (host) */
 int sph_mlp_train(sph_ctx *ctx, int32_t n, const float *X, const float *t, int32_t batch,
                   int32_t nsteps, float lr, float *loss);
+/* surrogate cooling on device arrays (cgs): u_new from the MLP where its
+ * estimated relative error is within mlp_err_tol, else from the exact solve;
+ * fell_back[i] = 1 where the exact solve ran (may be NULL) */
+int sph_cool_solve_mlp(sph_ctx *ctx, int32_t n, const double *rho, const double *u_old,
+                       const double *dt, double *u_new, int32_t *fell_back);
 
 /* ---- full step ---- */
 /* The prologue of the reference loop (sph_mpi4_v4.py:106-265): h, rho, forces,

@@ -466,3 +466,41 @@ def mlp_backward(cache, dy, W2, W3):
     gW1 = X.T @ dz1
     gb1 = dz1.sum(0)
     return gW1, gb1, gW2, gb2, gW3, gb3
+
+
+def bf16(x):
+    """Round float32 to bfloat16 (nearest even), returned as float32."""
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b >> 16) & 1) + 0x7FFF
+    return ((b + r) & 0xFFFF0000).astype(np.uint32).view(np.float32)
+
+
+def mlp_forward_bf16(X, W1, b1, W2, b2, W3, b3):
+    """Forward with the rounding points of the tensor-core kernels: matmul
+    operands in BF16, accumulation, bias, GELU and the last layer in FP32."""
+    z1 = bf16(X) @ bf16(W1) + b1
+    a1 = gelu_tanh(z1).astype(np.float32)
+    z2 = bf16(a1) @ bf16(W2) + b2
+    a2 = gelu_tanh(z2).astype(np.float32)
+    y = a2 @ W3 + b3
+    return y[:, 0], (X, z1, a1, z2, a2)
+
+
+def mlp_grad_bf16(X, t, W1, b1, W2, b2, W3, b3):
+    """Gradient of 0.5*mean((y-t)^2) with the kernels' rounding points."""
+    y, (X, z1, a1, z2, a2) = mlp_forward_bf16(X, W1, b1, W2, b2, W3, b3)
+    n = len(t)
+    dy = ((y - t) / n).astype(np.float32)[:, None]
+    loss = 0.5 * np.mean((y - t) ** 2)
+    gW3 = a2.T @ dy
+    gb3 = dy.sum(0)
+    dz2 = (dy @ W3.T) * gelu_tanh_grad(z2)
+    gb2 = dz2.sum(0)
+    gW2 = bf16(a1).T @ bf16(dz2)
+    da1 = bf16(dz2) @ bf16(W2).T
+    dz1 = da1 * gelu_tanh_grad(z1)
+    gb1 = dz1.sum(0)
+    gW1 = bf16(X).T @ bf16(dz1)
+    g = np.concatenate([gW1.ravel(), gb1, gW2.ravel(), gb2, gW3.ravel(), gb3]).astype(np.float32)
+    return g, float(loss)
+

@@ -114,6 +114,7 @@ SIGNATURES = [
     ("sph_mlp_forward", C.c_int, [_P, _I, _P, _P, _I]),
     ("sph_mlp_grad", C.c_int, [_P, _I, _P, _P, _P, _P, _I]),
     ("sph_mlp_train", C.c_int, [_P, _I, _P, _P, _I, _I, _F, _P]),
+    ("sph_cool_solve_mlp", C.c_int, [_P, _I, _P, _P, _P, _P, _P]),
     ("sph_debug_copy", C.c_int, [_P, _I, _P, _I]),
     ("sph_get_phase_times", C.c_int, [_P, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),

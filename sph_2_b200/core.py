@@ -334,6 +334,49 @@ class Context:
     def cooling_mlp(self):
         self._chk(self._L.sph_cooling_mlp(self._h), "cooling_mlp")
 
+    # -- cooling surrogate ----------------------------------------------------
+    def mlp_set(self, params, norm):
+        p = np.ascontiguousarray(params, np.float32)
+        nm = np.ascontiguousarray(norm, np.float32)
+        self._chk(self._L.sph_mlp_set(self._h, _ptr(p), _ptr(nm), 1), "mlp_set")
+
+    def mlp_get(self):
+        p = np.zeros(L.MLP_NPARAM, np.float32)
+        nm = np.zeros(8, np.float32)
+        self._chk(self._L.sph_mlp_get(self._h, _ptr(p), _ptr(nm), 1), "mlp_get")
+        return p, nm
+
+    def mlp_forward(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(len(X), np.float32)
+        self._chk(self._L.sph_mlp_forward(self._h, len(X), _ptr(X), _ptr(y), 1), "mlp_forward")
+        return y
+
+    def mlp_grad(self, X, t):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(L.MLP_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._chk(self._L.sph_mlp_grad(self._h, len(t), _ptr(X), _ptr(t), _ptr(g), _ptr(loss), 1),
+                  "mlp_grad")
+        return g, float(loss[0])
+
+    def cool_solve_mlp(self, rho, u_old, dt):
+        """Surrogate + Newton polish + exact fallback on device copies of the
+        arrays (cgs); returns (u_new, fell_back)."""
+        import torch
+        d = {k: torch.as_tensor(np.array(v, np.float64), device="cuda")
+             for k, v in (("rho", rho), ("u", u_old), ("dt", np.broadcast_to(dt, np.shape(rho))))}
+        out = torch.empty_like(d["u"])
+        fb = torch.empty(len(out), dtype=torch.int32, device="cuda")
+        self._chk(self._L.sph_cool_solve_mlp(self._h, len(out), C.c_void_p(d["rho"].data_ptr()),
+                                             C.c_void_p(d["u"].data_ptr()),
+                                             C.c_void_p(d["dt"].data_ptr()),
+                                             C.c_void_p(out.data_ptr()),
+                                             C.c_void_p(fb.data_ptr())), "cool_solve_mlp")
+        self.sync()
+        return out.cpu().numpy(), fb.cpu().numpy()
+
     def cool_solve(self, rho, u_old, dt):
         rho, u_old = _f64(rho), _f64(u_old)
         dt = _f64(np.broadcast_to(dt, rho.shape))

@@ -1,0 +1,165 @@
+// cooling.cuh -- device functions of the implicit cooling solve, shared by
+// the exact solver (cooling.cu) and the surrogate's fallback (mlp.cu).
+//
+// Same structure as DoCooling (GPU_sph/With_cooling/Model_C/
+// myPhotoLibsGPU.h:615-686): solve  u - u_old - ratefact * Lambda_net(u) * dt = 0
+// with ratefact = nH^2/rho, by bracketing (factors of 1.1) and bisection to
+// |du/u| <= tol, in FP64 and with every loop bounded.  Lambda_net is the
+// synthetic cooling function of the cooling-cloud workload: a log-log table of
+// Lambda(T) (n_bins power-law pieces between T0 and T1) and a constant heating
+// per H atom; T = (gamma-1) mu m_H u / k_B.
+#pragma once
+#include "sph_internal.cuh"
+
+#define KB_CGS 1.380649e-16
+#define MH_CGS 1.6726e-24
+
+struct CoolDev {
+    const double *logL;
+    int nb;
+    double logT0, logT1, mu, gamma, XH, gheat, tol;
+    int max_iter;
+};
+
+__device__ __forceinline__ double cool_lambda(const CoolDev &c, double T, double *slope) {
+    const double lt = log10(T);
+    const double dl = (c.logT1 - c.logT0) / c.nb;
+    int k = (int)floor((lt - c.logT0) / dl);
+    k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
+    const double s = (c.logL[k + 1] - c.logL[k]) / dl;
+    const double ll = c.logL[k] + s * (lt - (c.logT0 + k * dl));
+    if (slope) *slope = s;
+    return exp10(ll);
+}
+
+__device__ __forceinline__ double cool_net(const CoolDev &c, double u, double nH) {
+    const double T = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS * u;
+    return c.gheat / nH - cool_lambda(c, T, nullptr);
+}
+
+// returns the bisection count, -1 if the tolerance was not reached
+__device__ __forceinline__ int cool_solve(const CoolDev &c, double rho, double u_old, double dt, double *u_new) {
+    const double nH = c.XH * rho / MH_CGS;
+    const double ratefact = nH * nH / rho;
+    double u = u_old, up = u, lo = u;
+    const double r0 = u - u_old - ratefact * cool_net(c, u, nH) * dt;
+    int guard = 0;
+    if (r0 > 0.0) {
+        while (up - u_old - ratefact * cool_net(c, up, nH) * dt > 0.0 && guard++ < 2000) up /= 1.1;
+        lo = up;
+        up = lo * 1.1;
+    } else if (r0 < 0.0) {
+        while (up - u_old - ratefact * cool_net(c, up, nH) * dt < 0.0 && guard++ < 2000) up *= 1.1;
+        lo = up / 1.1;
+    } else {
+        *u_new = u;
+        return 0;
+    }
+    double du = u;
+    int it = 1;
+    while (fabs(du / u) > c.tol && it < c.max_iter) {
+        u = 0.5 * (lo + up);
+        const double r = u - u_old - ratefact * cool_net(c, u, nH) * dt;
+        if (r > 0.0) up = u; else lo = u;
+        du = fabs(up - lo);
+        it++;
+    }
+    *u_new = u;
+    return fabs(du / u) > c.tol ? -1 : it;
+}
+
+
+// Newton-step estimate of the error of an approximate solution u of
+// u - u_old - ratefact * net(u) * dt = 0:  delta = r(u) / r'(u), with
+// r'(u) = 1 + ratefact * dt * s * Lambda(T) / u (Lambda ~ T^s inside a bin,
+// T ~ u).  Returns |delta|/u, or +inf where r' <= 0 (the estimate is void).
+__device__ __forceinline__ double cool_error_estimate(const CoolDev &c, double rho, double u_old,
+                                                      double dt, double u) {
+    const double nH = c.XH * rho / MH_CGS;
+    const double ratefact = nH * nH / rho;
+    const double T = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS * u;
+    double s;
+    const double lam = cool_lambda(c, T, &s);
+    const double r = u - u_old - ratefact * (c.gheat / nH - lam) * dt;
+    const double rp = 1.0 + ratefact * dt * s * lam / u;
+    if (!(rp > 0.0) || !(u > 0.0)) return INFINITY;
+    return fabs(r / rp) / u;
+}
+
+// One Newton step of the implicit equation from an approximate solution *u
+// (the surrogate's prediction), then the error estimate of the result:
+// *u <- u - r(u)/r'(u) when r' > 0 and the step keeps u positive, *est <- the
+// relative error estimate of the new *u (+inf when it is void).
+__device__ __forceinline__ void cool_newton_polish(const CoolDev &c, double rho, double u_old,
+                                                   double dt, double *u, double *est) {
+    const double nH = c.XH * rho / MH_CGS;
+    const double ratefact = nH * nH / rho;
+    const double u0 = *u;
+    const double T = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS * u0;
+    double s;
+    const double lam = cool_lambda(c, T, &s);
+    const double r = u0 - u_old - ratefact * (c.gheat / nH - lam) * dt;
+    const double rp = 1.0 + ratefact * dt * s * lam / u0;
+    if (rp > 0.0 && u0 > 0.0) {
+        const double u1 = u0 - r / rp;
+        if (u1 > 0.0) *u = u1;
+    }
+    *est = cool_error_estimate(c, rho, u_old, dt, *u);
+}
+
+// True when r(u) = u - u_old - ratefact*net(u)*dt is strictly increasing on
+// [u_lo, u_hi]: r'(u) = 1 + ratefact*dt*s*Lambda(T)/u with Lambda/u a power
+// law inside each table bin, so checking r' > 0 at the interval's ends and at
+// every bin edge inside it checks the whole interval.  A monotone r has one
+// root there, the one the bracket-and-bisect solve reaches from u_old.
+__device__ __forceinline__ bool cool_monotone(const CoolDev &c, double rho, double dt, double u_lo,
+                                              double u_hi) {
+    const double nH = c.XH * rho / MH_CGS;
+    const double ratefact = nH * nH / rho;
+    const double kT = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS;
+    const double dl = (c.logT1 - c.logT0) / c.nb;
+    auto rp_at = [&](double T, int side) {
+        // slope of the bin on the given side of an edge (side -1 below, +1 above)
+        const double lt = log10(T);
+        int k = (int)floor((lt - c.logT0) / dl + (side < 0 ? -1e-9 : 1e-9));
+        k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
+        const double s = (c.logL[k + 1] - c.logL[k]) / dl;
+        const double lam = exp10(c.logL[k] + s * (lt - (c.logT0 + k * dl)));
+        return 1.0 + ratefact * dt * s * lam / (T / kT);
+    };
+    const double T0 = kT * u_lo, T1 = kT * u_hi;
+    if (!(rp_at(T0, +1) > 0.0) || !(rp_at(T1, -1) > 0.0)) return false;
+    const double l0 = log10(T0), l1 = log10(T1);
+    int k0 = (int)ceil((l0 - c.logT0) / dl), k1 = (int)floor((l1 - c.logT0) / dl);
+    k0 = k0 < 1 ? 1 : k0;
+    k1 = k1 > c.nb - 1 ? c.nb - 1 : k1;
+    for (int k = k0; k <= k1 && k - k0 < 4 * c.nb; k++) {
+        const double T = exp10(c.logT0 + k * dl);
+        if (!(rp_at(T, -1) > 0.0) || !(rp_at(T, +1) > 0.0)) return false;
+    }
+    return true;
+}
+
+// accept a surrogate solution un (after cool_newton_polish, estimate est)?
+__device__ __forceinline__ bool cool_accept(const CoolDev &c, double rho, double u_old, double dt,
+                                            double un, double est, double tol) {
+    if (!(est <= tol) || !(un > 0.0)) return false;
+    const double lo = fmin(u_old, un / 1.1), hi = fmax(u_old, un * 1.1);
+    return cool_monotone(c, rho, dt, lo, hi);
+}
+
+static inline CoolDev cool_dev_of(const sph_ctx *ctx) {
+    const sph_cooling_params &p = ctx->cool;
+    CoolDev c;
+    c.logL = ctx->cool_table;
+    c.nb = p.n_bins;
+    c.logT0 = p.logT0;
+    c.logT1 = p.logT1;
+    c.mu = p.mu;
+    c.gamma = p.gamma;
+    c.XH = p.XH;
+    c.gheat = p.gamma_heat;
+    c.tol = p.tol;
+    c.max_iter = p.max_iter;
+    return c;
+}

@@ -1,12 +1,672 @@
-// mlp.cu -- cooling-surrogate MLP (placeholder until the tensor-core kernels land)
-#include "sph_internal.cuh"
+// mlp.cu -- the cooling surrogate: a 3 -> 64 -> 64 -> 1 MLP (tanh-GELU),
+// BF16 operands with FP32 accumulation on the tensor cores
+// (mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32), forward, backward and
+// Adam kernels written here, and the in-step use: predict
+// dlog10(u) = log10(u_new/u_old) from (log10 rho, log10 u, log10 dt) [cgs],
+// estimate the error of the prediction with one Newton residual of the
+// implicit equation after one Newton step from the prediction, and fall back
+// to the exact solver where it exceeds the tolerance or where the implicit
+// equation is not monotone between u_old and the prediction (there it can have
+// several roots and the surrogate may have found another one).  No reference counterpart: the reference always runs the
+// bisection (myPhotoLibsGPU.h:615-686) or a table lookup (hcoolingx,
+// hfvCLibs_v7_hfv_v2.h:1240-1418).
+//
+// Parameters (FP32 masters, SPH_MLP_NPARAM): W1[3][64] b1[64] W2[64][64]
+// b2[64] W3[64] b3 -- layer k computes z = a W + b with a the row vector of
+// the previous layer -- followed by norm[8] = (mean[3], scale[3], y_mean,
+// y_scale).  Packed BF16 operand tables: W1t[64][16] (out x in, K padded to
+// 16), W2t[64][64] (out x in) for the forward pass, W2[64][64] (in x out) for
+// the backward pass.
+//
+// MMA fragment layout (per lane, gid = lane/4, tig = lane%4): A 16x16 holds
+// rows gid, gid+8 at columns 2tig..2tig+1 and 2tig+8..+9; B 16x8 holds
+// k = 2tig..+1 and 2tig+8..+9 at column gid; C 16x8 holds rows gid, gid+8 at
+// columns 2tig..+1.  Two adjacent C tiles of one layer are exactly the A
+// fragment of the next layer's K step, so activations stay in registers.
+#include <cuda_bf16.h>
 
-int launch_cooling_mlp(sph_ctx *ctx) { (void)ctx; return SPH_ERR_STATE; }
+#include "cooling.cuh"
+
+namespace {
+
+constexpr int H = 64;
+constexpr int NP = SPH_MLP_NPARAM;
+constexpr int OFF_W1 = 0, OFF_B1 = 192, OFF_W2 = 256, OFF_B2 = 4352, OFF_W3 = 4416, OFF_B3 = 4480;
+constexpr int PK_W1T = 0, PK_W2T = 1024, PK_W2 = 1024 + 4096, PK_N = 1024 + 2 * 4096;
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ void mma16816(float *d, const unsigned *a, const unsigned *b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ unsigned pack2(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<unsigned *>(&v);
+}
+__device__ __forceinline__ unsigned ld32(const __nv_bfloat16 *p) {
+    return *reinterpret_cast<const unsigned *>(p);
+}
+
+// tanh form of GELU and its derivative
+__device__ __forceinline__ float gelu(float z) {
+    const float k = 0.7978845608028654f;
+    return 0.5f * z * (1.0f + tanhf(k * (z + 0.044715f * z * z * z)));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float k = 0.7978845608028654f;
+    const float t = tanhf(k * (z + 0.044715f * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * k * (1.0f + 3.0f * 0.044715f * z * z);
+}
+
+struct MlpSmem {
+    __nv_bfloat16 w[PK_N];     // W1t, W2t, W2
+    float b1[H], b2[H], w3[H], b3;
+};
+
+__device__ __forceinline__ void load_weights(MlpSmem &S, const __nv_bfloat16 *pk, const float *P) {
+    for (int k = threadIdx.x; k < PK_N / 2; k += blockDim.x)
+        reinterpret_cast<unsigned *>(S.w)[k] = reinterpret_cast<const unsigned *>(pk)[k];
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        S.b1[k] = P[OFF_B1 + k];
+        S.b2[k] = P[OFF_B2 + k];
+        S.w3[k] = P[OFF_W3 + k];
+    }
+    if (threadIdx.x == 0) S.b3 = P[OFF_B3];
+    __syncthreads();
+}
+
+// forward of one 16-row tile: ax = A fragment of X (16 x 16, 3 real columns);
+// z1, z2 pre-activations (C fragments), y for rows gid and gid+8
+__device__ __forceinline__ void tile_forward(const MlpSmem &S, const unsigned *ax, float z1[8][4],
+                                             float z2[8][4], float &y0, float &y1) {
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const __nv_bfloat16 *W1t = S.w + PK_W1T, *W2t = S.w + PK_W2T;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int col = nt * 8 + 2 * tig;
+        z1[nt][0] = S.b1[col]; z1[nt][1] = S.b1[col + 1];
+        z1[nt][2] = S.b1[col]; z1[nt][3] = S.b1[col + 1];
+        const __nv_bfloat16 *wb = W1t + (nt * 8 + gid) * 16 + 2 * tig;
+        const unsigned b[2] = {ld32(wb), ld32(wb + 8)};
+        mma16816(z1[nt], ax, b);
+    }
+    unsigned a2[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        a2[kk][0] = pack2(gelu(z1[2 * kk][0]), gelu(z1[2 * kk][1]));
+        a2[kk][1] = pack2(gelu(z1[2 * kk][2]), gelu(z1[2 * kk][3]));
+        a2[kk][2] = pack2(gelu(z1[2 * kk + 1][0]), gelu(z1[2 * kk + 1][1]));
+        a2[kk][3] = pack2(gelu(z1[2 * kk + 1][2]), gelu(z1[2 * kk + 1][3]));
+    }
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int col = nt * 8 + 2 * tig;
+        z2[nt][0] = S.b2[col]; z2[nt][1] = S.b2[col + 1];
+        z2[nt][2] = S.b2[col]; z2[nt][3] = S.b2[col + 1];
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            const __nv_bfloat16 *wb = W2t + (nt * 8 + gid) * 64 + kk * 16 + 2 * tig;
+            const unsigned b[2] = {ld32(wb), ld32(wb + 8)};
+            mma16816(z2[nt], a2[kk], b);
+        }
+        s0 += gelu(z2[nt][0]) * S.w3[col] + gelu(z2[nt][1]) * S.w3[col + 1];
+        s1 += gelu(z2[nt][2]) * S.w3[col] + gelu(z2[nt][3]) * S.w3[col + 1];
+    }
+    s0 += __shfl_xor_sync(FULL, s0, 1);
+    s0 += __shfl_xor_sync(FULL, s0, 2);
+    s1 += __shfl_xor_sync(FULL, s1, 1);
+    s1 += __shfl_xor_sync(FULL, s1, 2);
+    y0 = s0 + S.b3;
+    y1 = s1 + S.b3;
+}
+
+// A fragment of a 16-row tile of X staged row-major as bf16 [16][16]
+__device__ __forceinline__ void x_fragment(const __nv_bfloat16 *X16, unsigned *ax) {
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    ax[0] = ld32(X16 + gid * 16 + 2 * tig);
+    ax[1] = ld32(X16 + (gid + 8) * 16 + 2 * tig);
+    ax[2] = ld32(X16 + gid * 16 + 2 * tig + 8);
+    ax[3] = ld32(X16 + (gid + 8) * 16 + 2 * tig + 8);
+}
+
+__global__ void k_mlp_pack(const float *__restrict__ P, __nv_bfloat16 *__restrict__ pk) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 1024) {  // W1t[j][c]
+        const int j = t / 16, c = t % 16;
+        pk[PK_W1T + t] = __float2bfloat16_rn(c < 3 ? P[OFF_W1 + c * H + j] : 0.f);
+    } else if (t < 1024 + 4096) {  // W2t[j][i] = W2[i][j]
+        const int u = t - 1024, j = u / 64, i = u % 64;
+        pk[PK_W2T + u] = __float2bfloat16_rn(P[OFF_W2 + i * H + j]);
+    } else if (t < PK_N) {  // W2[i][j]
+        const int u = t - 1024 - 4096;
+        pk[PK_W2 + u] = __float2bfloat16_rn(P[OFF_W2 + u]);
+    }
+}
+
+// forward on n rows of normalised X[n][3] -> y[n]; one warp per 16-row tile
+__global__ void __launch_bounds__(128)
+    k_mlp_forward(int n, const float *__restrict__ X, float *__restrict__ y,
+                  const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P) {
+    __shared__ MlpSmem S;
+    __shared__ __align__(16) __nv_bfloat16 xs[4][16 * 16];
+    load_weights(S, pk, P);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntile = (n + 15) / 16;
+    for (int tile = blockIdx.x * 4 + w; tile < ntile; tile += gridDim.x * 4) {
+        const int r0 = tile * 16;
+        for (int e = lane; e < 256; e += 32) {
+            const int r = e / 16, c = e % 16;
+            const int row = r0 + r;
+            xs[w][e] = __float2bfloat16_rn((c < 3 && row < n) ? X[3 * row + c] : 0.f);
+        }
+        __syncwarp();
+        unsigned ax[4];
+        x_fragment(xs[w], ax);
+        float z1[8][4], z2[8][4], y0, y1;
+        tile_forward(S, ax, z1, z2, y0, y1);
+        const int gid = lane >> 2, tig = lane & 3;
+        if (tig == 0) {
+            if (r0 + gid < n) y[r0 + gid] = y0;
+            if (r0 + gid + 8 < n) y[r0 + gid + 8] = y1;
+        }
+        __syncwarp();
+    }
+}
+
+// gradient of L = 0.5/n_total * sum (y - t)^2 over this launch's rows, added
+// into grad (FP32, pre-zeroed); loss added into *loss
+constexpr int GR = 256;        // rows per block
+constexpr int LD = GR + 8;     // padded row stride of the transposed tiles
+struct GradSmem {
+    MlpSmem W;
+    __nv_bfloat16 X[GR * 16];  // row-major [r][c]
+    __nv_bfloat16 Xt[16 * LD]; // [c][r]
+    __nv_bfloat16 At1[H * LD]; // gelu(z1) transposed [i][r]
+    __nv_bfloat16 dZ2t[H * LD];
+    __nv_bfloat16 dZ1t[H * LD];
+    float gb1[H], gb2[H], gw3[H], gb3, loss;
+};
+
+__global__ void __launch_bounds__(128)
+    k_mlp_grad(int n, const float *__restrict__ X, const float *__restrict__ T, float inv_n,
+               const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
+               float *__restrict__ grad, float *__restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GradSmem &S = *reinterpret_cast<GradSmem *>(smem_raw);
+    load_weights(S.W, pk, P);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int rb = blockIdx.x * GR;
+    for (int e = threadIdx.x; e < GR * 16; e += blockDim.x) {
+        const int r = e / 16, c = e % 16;
+        const float v = (c < 3 && rb + r < n) ? X[3 * (rb + r) + c] : 0.f;
+        const __nv_bfloat16 bv = __float2bfloat16_rn(v);
+        S.X[e] = bv;
+        S.Xt[c * LD + r] = bv;
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) S.gb1[k] = S.gb2[k] = S.gw3[k] = 0.f;
+    if (threadIdx.x == 0) S.gb3 = S.loss = 0.f;
+    __syncthreads();
+    const __nv_bfloat16 *W2 = S.W.w + PK_W2;
+    float pb3 = 0.f, pl = 0.f;
+    for (int tile = w; tile < GR / 16; tile += 4) {
+        const int r0 = tile * 16;
+        unsigned ax[4];
+        x_fragment(S.X + r0 * 16, ax);
+        float z1[8][4], z2[8][4], y0, y1;
+        tile_forward(S.W, ax, z1, z2, y0, y1);
+        const bool ok0 = rb + r0 + gid < n, ok1 = rb + r0 + gid + 8 < n;
+        const float e0 = ok0 ? y0 - T[rb + r0 + gid] : 0.f;
+        const float e1 = ok1 ? y1 - T[rb + r0 + gid + 8] : 0.f;
+        const float dy0 = e0 * inv_n, dy1 = e1 * inv_n;
+        if (tig == 0) {
+            pl += 0.5f * inv_n * (e0 * e0 + e1 * e1);
+            pb3 += dy0 + dy1;
+        }
+        // dZ2, bias/W3 partials, transposed tiles for the weight GEMMs
+        float dz2[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int col = nt * 8 + 2 * tig;
+            const float w30 = S.W.w3[col], w31 = S.W.w3[col + 1];
+            dz2[nt][0] = dy0 * w30 * gelu_grad(z2[nt][0]);
+            dz2[nt][1] = dy0 * w31 * gelu_grad(z2[nt][1]);
+            dz2[nt][2] = dy1 * w30 * gelu_grad(z2[nt][2]);
+            dz2[nt][3] = dy1 * w31 * gelu_grad(z2[nt][3]);
+            atomicAdd(&S.gw3[col], gelu(z2[nt][0]) * dy0 + gelu(z2[nt][2]) * dy1);
+            atomicAdd(&S.gw3[col + 1], gelu(z2[nt][1]) * dy0 + gelu(z2[nt][3]) * dy1);
+            atomicAdd(&S.gb2[col], dz2[nt][0] + dz2[nt][2]);
+            atomicAdd(&S.gb2[col + 1], dz2[nt][1] + dz2[nt][3]);
+            const int ra = r0 + gid, rc = r0 + gid + 8;
+            S.At1[col * LD + ra] = __float2bfloat16_rn(gelu(z1[nt][0]));
+            S.At1[(col + 1) * LD + ra] = __float2bfloat16_rn(gelu(z1[nt][1]));
+            S.At1[col * LD + rc] = __float2bfloat16_rn(gelu(z1[nt][2]));
+            S.At1[(col + 1) * LD + rc] = __float2bfloat16_rn(gelu(z1[nt][3]));
+            S.dZ2t[col * LD + ra] = __float2bfloat16_rn(dz2[nt][0]);
+            S.dZ2t[(col + 1) * LD + ra] = __float2bfloat16_rn(dz2[nt][1]);
+            S.dZ2t[col * LD + rc] = __float2bfloat16_rn(dz2[nt][2]);
+            S.dZ2t[(col + 1) * LD + rc] = __float2bfloat16_rn(dz2[nt][3]);
+        }
+        // dA1 = dZ2 W2^T  (B[k=j][n=i] = W2[i][j], stored [i][j])
+        unsigned ad[4][4];
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            ad[kk][0] = pack2(dz2[2 * kk][0], dz2[2 * kk][1]);
+            ad[kk][1] = pack2(dz2[2 * kk][2], dz2[2 * kk][3]);
+            ad[kk][2] = pack2(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
+            ad[kk][3] = pack2(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            float da[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                const __nv_bfloat16 *wb = W2 + (nt * 8 + gid) * 64 + kk * 16 + 2 * tig;
+                const unsigned b[2] = {ld32(wb), ld32(wb + 8)};
+                mma16816(da, ad[kk], b);
+            }
+            const int col = nt * 8 + 2 * tig;
+            const float d0 = da[0] * gelu_grad(z1[nt][0]), d1 = da[1] * gelu_grad(z1[nt][1]);
+            const float d2 = da[2] * gelu_grad(z1[nt][2]), d3 = da[3] * gelu_grad(z1[nt][3]);
+            atomicAdd(&S.gb1[col], d0 + d2);
+            atomicAdd(&S.gb1[col + 1], d1 + d3);
+            const int ra = r0 + gid, rc = r0 + gid + 8;
+            S.dZ1t[col * LD + ra] = __float2bfloat16_rn(d0);
+            S.dZ1t[(col + 1) * LD + ra] = __float2bfloat16_rn(d1);
+            S.dZ1t[col * LD + rc] = __float2bfloat16_rn(d2);
+            S.dZ1t[(col + 1) * LD + rc] = __float2bfloat16_rn(d3);
+        }
+    }
+    if (tig == 0) {
+        atomicAdd(&S.gb3, pb3);
+        atomicAdd(&S.loss, pl);
+    }
+    __syncthreads();
+    // dW2[i][j] = sum_r A1[r][i] dZ2[r][j]: warp w owns rows i = 16w..16w+15
+    {
+        float acc[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        const int i0 = 16 * w;
+        for (int kk = 0; kk < GR / 16; kk++) {
+            const __nv_bfloat16 *ap = S.At1 + (i0 + gid) * LD + kk * 16 + 2 * tig;
+            const unsigned a[4] = {ld32(ap), ld32(ap + 8 * LD), ld32(ap + 8), ld32(ap + 8 * LD + 8)};
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const __nv_bfloat16 *bp = S.dZ2t + (nt * 8 + gid) * LD + kk * 16 + 2 * tig;
+                const unsigned b[2] = {ld32(bp), ld32(bp + 8)};
+                mma16816(acc[nt], a, b);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int j = nt * 8 + 2 * tig;
+            atomicAdd(&grad[OFF_W2 + (i0 + gid) * H + j], acc[nt][0]);
+            atomicAdd(&grad[OFF_W2 + (i0 + gid) * H + j + 1], acc[nt][1]);
+            atomicAdd(&grad[OFF_W2 + (i0 + gid + 8) * H + j], acc[nt][2]);
+            atomicAdd(&grad[OFF_W2 + (i0 + gid + 8) * H + j + 1], acc[nt][3]);
+        }
+    }
+    // dW1[c][j] = sum_r X[r][c] dZ1[r][j]: warp w owns columns j = 16w..16w+15
+    {
+        float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+        for (int kk = 0; kk < GR / 16; kk++) {
+            const __nv_bfloat16 *ap = S.Xt + gid * LD + kk * 16 + 2 * tig;
+            const unsigned a[4] = {ld32(ap), ld32(ap + 8 * LD), ld32(ap + 8), ld32(ap + 8 * LD + 8)};
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const __nv_bfloat16 *bp = S.dZ1t + ((2 * w + q) * 8 + gid) * LD + kk * 16 + 2 * tig;
+                const unsigned b[2] = {ld32(bp), ld32(bp + 8)};
+                mma16816(acc[q], a, b);
+            }
+        }
+        if (gid < 3)
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int j = (2 * w + q) * 8 + 2 * tig;
+                atomicAdd(&grad[OFF_W1 + gid * H + j], acc[q][0]);
+                atomicAdd(&grad[OFF_W1 + gid * H + j + 1], acc[q][1]);
+            }
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        atomicAdd(&grad[OFF_B1 + k], S.gb1[k]);
+        atomicAdd(&grad[OFF_B2 + k], S.gb2[k]);
+        atomicAdd(&grad[OFF_W3 + k], S.gw3[k]);
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&grad[OFF_B3], S.gb3);
+        atomicAdd(loss, S.loss);
+    }
+}
+
+__global__ void k_adam(float *__restrict__ P, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, float lr, float b1, float b2, float eps, float c1,
+                       float c2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= NP) return;
+    const float gk = g[k];
+    const float mk = b1 * m[k] + (1.f - b1) * gk;
+    const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    P[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+}
+
+// In-step cooling with the surrogate: one warp per 16 particles.  Features are
+// staged through shared memory; rows whose estimated error exceeds err_tol
+// (or whose estimate is void) are solved exactly.
+__global__ void __launch_bounds__(128)
+    k_cool_mlp(CoolDev c, int n, const double *__restrict__ rho, double *__restrict__ u,
+               const int *__restrict__ cloud, const double *__restrict__ dt, double ur, double uu,
+               double ut, const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
+               double err_tol, long long *status) {
+    __shared__ MlpSmem S;
+    __shared__ __align__(16) __nv_bfloat16 xs[4][16 * 16];
+    __shared__ float ys[4][16];
+    load_weights(S, pk, P);
+    const float *norm = P + NP;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int ntile = (n + 15) / 16;
+    for (int tile = blockIdx.x * 4 + w; tile < ntile; tile += gridDim.x * 4) {
+        const int r0 = tile * 16;
+        const int i = r0 + (lane & 15);
+        const bool own = lane < 16 && i < n;
+        double rho_c = 0.0, u0 = 0.0, dt_c = 0.0;
+        if (own) {
+            rho_c = rho[i] * ur;
+            u0 = u[i] * uu;
+            dt_c = dt[cloud[i]] * ut;
+        }
+        for (int e = lane; e < 256; e += 32) xs[w][e] = __float2bfloat16_rn(0.f);
+        __syncwarp();
+        if (own) {
+            const float f0 = ((float)log10(rho_c) - norm[0]) / norm[3];
+            const float f1 = ((float)log10(u0) - norm[1]) / norm[4];
+            const float f2 = ((float)log10(dt_c) - norm[2]) / norm[5];
+            xs[w][(lane & 15) * 16 + 0] = __float2bfloat16_rn(f0);
+            xs[w][(lane & 15) * 16 + 1] = __float2bfloat16_rn(f1);
+            xs[w][(lane & 15) * 16 + 2] = __float2bfloat16_rn(f2);
+        }
+        __syncwarp();
+        unsigned ax[4];
+        x_fragment(xs[w], ax);
+        float z1[8][4], z2[8][4], y0, y1;
+        tile_forward(S, ax, z1, z2, y0, y1);
+        if (tig == 0) {
+            ys[w][gid] = y0;
+            ys[w][gid + 8] = y1;
+        }
+        __syncwarp();
+        if (own) {
+            const double dl = (double)ys[w][lane & 15] * norm[7] + norm[6];
+            double un = u0 * exp10(dl), est;
+            cool_newton_polish(c, rho_c, u0, dt_c, &un, &est);
+            if (!cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+                status_add(status, SPH_S_MLP_FALLBACK, 1);
+                if (cool_solve(c, rho_c, u0, dt_c, &un) < 0) status_add(status, SPH_S_COOL_NOCONV, 1);
+            }
+            u[i] = un / uu;
+        }
+        __syncwarp();
+    }
+}
+
+// the same for standalone arrays (cgs), with the per-row fallback flag
+__global__ void __launch_bounds__(128)
+    k_cool_mlp_arrays(CoolDev c, int n, const double *__restrict__ rho,
+                      const double *__restrict__ u_old, const double *__restrict__ dtv,
+                      double *__restrict__ u_new, int *__restrict__ fell_back,
+                      const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
+                      double err_tol) {
+    __shared__ MlpSmem S;
+    __shared__ __align__(16) __nv_bfloat16 xs[4][16 * 16];
+    __shared__ float ys[4][16];
+    load_weights(S, pk, P);
+    const float *norm = P + NP;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int ntile = (n + 15) / 16;
+    for (int tile = blockIdx.x * 4 + w; tile < ntile; tile += gridDim.x * 4) {
+        const int r0 = tile * 16;
+        const int i = r0 + (lane & 15);
+        const bool own = lane < 16 && i < n;
+        for (int e = lane; e < 256; e += 32) xs[w][e] = __float2bfloat16_rn(0.f);
+        __syncwarp();
+        if (own) {
+            xs[w][(lane & 15) * 16 + 0] = __float2bfloat16_rn(((float)log10(rho[i]) - norm[0]) / norm[3]);
+            xs[w][(lane & 15) * 16 + 1] = __float2bfloat16_rn(((float)log10(u_old[i]) - norm[1]) / norm[4]);
+            xs[w][(lane & 15) * 16 + 2] = __float2bfloat16_rn(((float)log10(dtv[i]) - norm[2]) / norm[5]);
+        }
+        __syncwarp();
+        unsigned ax[4];
+        x_fragment(xs[w], ax);
+        float z1[8][4], z2[8][4], y0, y1;
+        tile_forward(S, ax, z1, z2, y0, y1);
+        if (tig == 0) {
+            ys[w][gid] = y0;
+            ys[w][gid + 8] = y1;
+        }
+        __syncwarp();
+        if (own) {
+            const double dl = (double)ys[w][lane & 15] * norm[7] + norm[6];
+            double un = u_old[i] * exp10(dl), est;
+            cool_newton_polish(c, rho[i], u_old[i], dtv[i], &un, &est);
+            int fb = 0;
+            if (!cool_accept(c, rho[i], u_old[i], dtv[i], un, est, err_tol)) {
+                fb = 1;
+                cool_solve(c, rho[i], u_old[i], dtv[i], &un);
+            }
+            u_new[i] = un;
+            if (fell_back) fell_back[i] = fb;
+        }
+        __syncwarp();
+    }
+}
+
+int grid_for(sph_ctx *ctx, int n) { return max(1, min(div_up(div_up(n, 16), 4), ctx->num_sms * 8)); }
+
+int ensure_mlp(sph_ctx *ctx) {
+    if (ctx->mlp) return SPH_OK;
+    void *q = nullptr;
+    const size_t bytes = sizeof(float) * (NP + 8) + sizeof(float) * NP * 3 + sizeof(float) * 8 +
+                         sizeof(__nv_bfloat16) * PK_N;
+    CK(cudaMalloc(&q, bytes));
+    CK(cudaMemset(q, 0, bytes));
+    ctx->allocs.push_back(q);
+    ctx->dev_bytes += bytes;
+    float *f = (float *)q;
+    ctx->mlp = f;                    // params + norm
+    ctx->mlp_grad = f + NP + 8;      // grad
+    ctx->mlp_m = ctx->mlp_grad + NP;
+    ctx->mlp_v = ctx->mlp_m + NP;
+    ctx->mlp_scratch = ctx->mlp_v + NP;  // loss (+7 spare)
+    ctx->mlp_bf16 = (void *)(ctx->mlp_scratch + 8);
+    return SPH_OK;
+}
+
+}  // namespace
+
+int mlp_pack(sph_ctx *ctx) {
+    k_mlp_pack<<<div_up(PK_N, 256), 256, 0, ctx->stream>>>(ctx->mlp,
+                                                            (__nv_bfloat16 *)ctx->mlp_bf16);
+    return ctx_check_launch(ctx, "mlp_pack");
+}
+
+int mlp_forward_dev(sph_ctx *ctx, int n, const float *X, float *y) {
+    if (n <= 0) return SPH_OK;
+    k_mlp_forward<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+        n, X, y, (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp);
+    return ctx_check_launch(ctx, "mlp_forward");
+}
+
+static int grad_launch(sph_ctx *ctx, int n, const float *X, const float *t, float inv_n) {
+    const size_t sm = sizeof(GradSmem);
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        attr = true;
+    }
+    k_mlp_grad<<<div_up(n, GR), 128, sm, ctx->stream>>>(
+        n, X, t, inv_n, (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->mlp_grad,
+        ctx->mlp_scratch);
+    return ctx_check_launch(ctx, "mlp_grad");
+}
+
+int mlp_grad_dev(sph_ctx *ctx, int n, const float *X, const float *t, float *grad, float *loss) {
+    if (n <= 0) return SPH_ERR_ARG;
+    CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * NP, ctx->stream));
+    CK(cudaMemsetAsync(ctx->mlp_scratch, 0, sizeof(float), ctx->stream));
+    int rc = grad_launch(ctx, n, X, t, 1.0f / n);
+    if (rc) return rc;
+    if (grad) CK(cudaMemcpyAsync(grad, ctx->mlp_grad, sizeof(float) * NP, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+    if (loss) CK(cudaMemcpyAsync(loss, ctx->mlp_scratch, sizeof(float), cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+    return SPH_OK;
+}
+
+int mlp_train_dev(sph_ctx *ctx, int n, const float *X, const float *t, int batch, int nsteps,
+                  float lr, float *loss_out) {
+    if (n <= 0 || batch <= 0 || nsteps < 0) return SPH_ERR_ARG;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const int nb = max(1, n / batch);
+    for (int s = 0; s < nsteps; s++) {
+        const int b = s % nb;
+        const int rows = min(batch, n - b * batch);
+        CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * NP, ctx->stream));
+        CK(cudaMemsetAsync(ctx->mlp_scratch, 0, sizeof(float), ctx->stream));
+        int rc = grad_launch(ctx, rows, X + 3 * (size_t)b * batch, t + (size_t)b * batch, 1.0f / rows);
+        if (rc) return rc;
+        ctx->mlp_step++;
+        const float c1 = 1.f - powf(b1, (float)ctx->mlp_step), c2 = 1.f - powf(b2, (float)ctx->mlp_step);
+        k_adam<<<div_up(NP, 256), 256, 0, ctx->stream>>>(ctx->mlp, ctx->mlp_grad, ctx->mlp_m,
+                                                         ctx->mlp_v, lr, b1, b2, eps, c1, c2);
+        rc = mlp_pack(ctx);
+        if (rc) return rc;
+    }
+    if (loss_out)
+        CK(cudaMemcpyAsync(loss_out, ctx->mlp_scratch, sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
+}
+
+int launch_cooling_mlp(sph_ctx *ctx) {
+    if (!ctx->cool_ok || !ctx->mlp_ok) return SPH_ERR_STATE;
+    const int n = ctx->n, c = ctx->cur;
+    if (n <= 0) return SPH_OK;
+    k_cool_mlp<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+        cool_dev_of(ctx), n, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
+        ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t,
+        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->status);
+    return ctx_check_launch(ctx, "cooling_mlp");
+}
 
 extern "C" {
-int sph_mlp_set(sph_ctx *, const float *, const float *, int32_t) { return SPH_ERR_STATE; }
-int sph_mlp_get(sph_ctx *, float *, float *, int32_t) { return SPH_ERR_STATE; }
-int sph_mlp_forward(sph_ctx *, int32_t, const float *, float *, int32_t) { return SPH_ERR_STATE; }
-int sph_mlp_grad(sph_ctx *, int32_t, const float *, const float *, float *, float *, int32_t) { return SPH_ERR_STATE; }
-int sph_mlp_train(sph_ctx *, int32_t, const float *, const float *, int32_t, int32_t, float, float *) { return SPH_ERR_STATE; }
+
+int sph_mlp_set(sph_ctx *ctx, const float *params, const float *norm, int32_t host) {
+    if (!ctx || !params || !norm) return SPH_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = ensure_mlp(ctx);
+    if (rc) return rc;
+    cudaMemcpyKind k = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    CK(cudaMemcpyAsync(ctx->mlp, params, sizeof(float) * NP, k, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->mlp + NP, norm, sizeof(float) * 8, k, ctx->stream));
+    CK(cudaMemsetAsync(ctx->mlp_m, 0, sizeof(float) * NP * 2, ctx->stream));
+    ctx->mlp_step = 0;
+    rc = mlp_pack(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->mlp_ok = true;
+    return SPH_OK;
 }
+
+int sph_mlp_get(sph_ctx *ctx, float *params, float *norm, int32_t host) {
+    if (!ctx || !ctx->mlp_ok) return SPH_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (params) CK(cudaMemcpy(params, ctx->mlp, sizeof(float) * NP, k));
+    if (norm) CK(cudaMemcpy(norm, ctx->mlp + NP, sizeof(float) * 8, k));
+    return SPH_OK;
+}
+
+static int to_device(sph_ctx *ctx, const void *src, size_t bytes, int host, void **dst) {
+    *dst = nullptr;
+    if (!host) {
+        *dst = (void *)src;
+        return SPH_OK;
+    }
+    CK(cudaMalloc(dst, bytes));
+    CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return SPH_OK;
+}
+
+int sph_mlp_forward(sph_ctx *ctx, int32_t n, const float *X, float *y, int32_t host) {
+    if (!ctx || n < 0 || (n && (!X || !y))) return SPH_ERR_ARG;
+    if (!ctx->mlp_ok) return SPH_ERR_STATE;
+    if (n == 0) return SPH_OK;
+    cudaSetDevice(ctx->device);
+    void *dX = nullptr, *dy = nullptr;
+    int rc = to_device(ctx, X, sizeof(float) * 3 * n, host, &dX);
+    if (rc) return rc;
+    if (host) CK(cudaMalloc(&dy, sizeof(float) * n));
+    else dy = y;
+    rc = mlp_forward_dev(ctx, n, (const float *)dX, (float *)dy);
+    if (!rc && host) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaMemcpy(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
+    if (host) {
+        cudaFree(dX);
+        cudaFree(dy);
+    }
+    return rc;
+}
+
+int sph_mlp_grad(sph_ctx *ctx, int32_t n, const float *X, const float *t, float *grad, float *loss,
+                 int32_t host) {
+    if (!ctx || n <= 0 || !X || !t) return SPH_ERR_ARG;
+    if (!ctx->mlp_ok) return SPH_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    void *dX = nullptr, *dt = nullptr;
+    int rc = to_device(ctx, X, sizeof(float) * 3 * n, host, &dX);
+    if (!rc) rc = to_device(ctx, t, sizeof(float) * n, host, &dt);
+    if (!rc) rc = mlp_grad_dev(ctx, n, (const float *)dX, (const float *)dt, nullptr, nullptr);
+    if (!rc) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        if (grad) CK(cudaMemcpy(grad, ctx->mlp_grad, sizeof(float) * NP, k));
+        if (loss) CK(cudaMemcpy(loss, ctx->mlp_scratch, sizeof(float), k));
+    }
+    if (host) {
+        cudaFree(dX);
+        cudaFree(dt);
+    }
+    return rc;
+}
+
+int sph_mlp_train(sph_ctx *ctx, int32_t n, const float *X, const float *t, int32_t batch,
+                  int32_t nsteps, float lr, float *loss) {
+    if (!ctx || !X || !t) return SPH_ERR_ARG;
+    if (!ctx->mlp_ok) return SPH_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    return mlp_train_dev(ctx, n, X, t, batch, nsteps, lr, loss);
+}
+
+int sph_cool_solve_mlp(sph_ctx *ctx, int32_t n, const double *rho, const double *u_old,
+                       const double *dt, double *u_new, int32_t *fell_back) {
+    if (!ctx || n < 0) return SPH_ERR_ARG;
+    if (!ctx->cool_ok || !ctx->mlp_ok) return SPH_ERR_STATE;
+    if (n == 0) return SPH_OK;
+    cudaSetDevice(ctx->device);
+    k_cool_mlp_arrays<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+        cool_dev_of(ctx), n, rho, u_old, dt, u_new, fell_back,
+        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol);
+    return ctx_check_launch(ctx, "cool_solve_mlp");
+}
+
+}  // extern "C"
