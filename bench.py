@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-subset", type=int, default=10_000)
+    ap.add_argument("--workload", default="evrard", choices=["evrard", "ensemble", "cooling"],
+                    help="evrard: the headline line; ensemble / cooling: extra workloads")
+    ap.add_argument("--clouds", type=int, default=64)
+    ap.add_argument("--tune", action="store_true", help="run the autotuner before timing")
     return ap.parse_args()
 
 
@@ -188,6 +192,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         reference_arm(a, rank)
+        return
+    if a.workload != "evrard":
+        extra_workload(a, world, rank, local)
         return
 
     import torch
@@ -388,6 +395,99 @@ def main():
     ctx.close()
     if rank == 0:
         print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def extra_workload(a, world, rank, local):
+    """The batched 64-cloud ensemble (clouds sharded over the ranks) or the
+    2M-particle turbulent cooling cloud (exact implicit cooling vs the MLP
+    surrogate path).  Same timing rules as the headline line."""
+    import torch
+    import torch.distributed as dist
+    from sph_2_b200 import Config, Context, cooling, ic
+    from sph_2_b200 import _lib as L
+    from sph_2_b200.distributed import local_ensemble, shard_clouds
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    stream = torch.cuda.Stream(priority=-10)
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(ctx, steps, warmup):
+        ctx.step(warmup)
+        ctx.sync()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+            ctx.step(steps)
+            e1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32+fp64 (mixed)", "data": "synthetic"}
+    if a.workload == "ensemble":
+        e = ic.ensemble(n_clouds=a.clouds, seed=42)
+        owner = shard_clouds(e["counts"], world)
+        mine = local_ensemble(e, owner, rank)
+        n = len(mine["m"])
+        ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
+                             theta=a.theta, leaf_size=a.leaf, ngb_lanes=a.lanes))
+        ctx.set_stream(stream.cuda_stream)
+        ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
+        ctx.prologue()
+        if a.tune:
+            from sph_2_b200.autotune import tune
+            out["tuned"] = tune(ctx)[0]
+        ms = timed(ctx, a.steps, a.warmup)
+        total = int(e["counts"].sum())
+        out.update(value=total * a.steps / (ms * 1e-3), ms_per_step=ms / a.steps,
+                   config={"workload": f"ensemble_{a.clouds}_clouds", "particles": total,
+                           "clouds": a.clouds, "theta": a.theta,
+                           "parallelism": f"clouds sharded over {world} ranks (LPT)",
+                           "per_rank_particles": n},
+                   status=ctx.status())
+    else:
+        n = a.n if a.n != 1_000_000 else 2_000_000
+        d = ic.cooling_cloud(n, seed=42)
+        res = {}
+        for mode in ("exact", "mlp"):
+            flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0)
+            ctx = Context(Config(n_max=n, precision="mixed", theta=a.theta, leaf_size=a.leaf,
+                                 flags=flags))
+            ctx.set_stream(stream.cuda_stream)
+            cooling.setup(ctx, d["units"])
+            if mode == "mlp":
+                Xn, yn, norm, _ = cooling.training_set(ctx, n=1_000_000, seed=7)
+                ctx.mlp_set(cooling.init_params(seed=0), norm)
+                cooling.train(ctx, Xn, yn, steps=3000, batch=4096, lr=2e-3)
+            ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+            ctx.prologue()
+            ms = timed(ctx, a.steps, a.warmup)
+            res[mode] = {"value": n * a.steps / (ms * 1e-3), "ms_per_step": ms / a.steps,
+                         "status": ctx.status()}
+            ctx.close()
+        out.update(value=res["mlp"]["value"], ms_per_step=res["mlp"]["ms_per_step"],
+                   config={"workload": f"cooling_cloud_{n}", "n": n, "theta": a.theta,
+                           "mach": 2, "n_cgs": 100, "T": 1e4},
+                   exact=res["exact"], mlp=res["mlp"])
+    if rank == 0:
+        print(json.dumps(out))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
