@@ -16,8 +16,13 @@
 // list.  Accepted nodes and bucket particles are staged 32 at a time in shared
 // memory and every lane evaluates all 32 against its own particle, so the
 // interaction loop is branch-free FP32 (mixed) or FP64 (plain) FMA work with
-// one reciprocal square root per interaction.  Each 32-term chunk is summed
-// plainly and folded into a Kahan accumulator (mixed).
+// one reciprocal square root per interaction.  In FP32 every instruction
+// evaluates two staged entries at once with the packed f32x2 arithmetic of
+// sm_100 (__ffma2_rn / __fmul2_rn), which halves the issued instructions of
+// this issue-bound loop.  Each 32-term chunk is summed plainly and folded into
+// a Kahan accumulator (mixed).
+#include <type_traits>
+
 #include "sph_internal.cuh"
 
 namespace {
@@ -36,6 +41,19 @@ template <class R> struct WalkSmem {
     int plist[96];
     typename R4<R>::T sa[32], sb[32], sc[32];
 };
+
+// FP32 staging as one array per field, so that a 64-bit shared load gives the
+// field of two consecutive entries for the packed f32x2 arithmetic
+struct WalkSmemF {
+    int stk[WSTK];
+    int clist[64];
+    int plist[96];
+    // cells: com x y z, -mass, Qxx Qyy Qzz Qxy Qxz Qyz, trace
+    __align__(8) float f[11][32];
+};
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 
 template <class R> __device__ __forceinline__ R wmin(R v) {
     for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
@@ -75,9 +93,11 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
            double *__restrict__ agrav, double *__restrict__ pot, unsigned *work,
            unsigned long long *counters, long long *status) {
     typedef typename R4<R>::T V4;
-    __shared__ WalkSmem<R> smem[WALK_WARPS];
+    constexpr bool PACKED = std::is_same<R, float>::value;
+    typedef typename std::conditional<PACKED, WalkSmemF, WalkSmem<R>>::type SM;
+    __shared__ SM smem[WALK_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WalkSmem<R> &S = smem[w];
+    SM &S = smem[w];
     const unsigned lt = (1u << lane) - 1u;
     int maxsp = 0;
     const int ngroup = *ngroup_p;
@@ -101,6 +121,65 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         __syncwarp();
 
         auto flush_cells = [&](int m) {
+          if constexpr (PACKED) {
+            // two cells per lane per instruction (f32x2); odd chunks are padded
+            // with a massless, moment-free entry that contributes zero
+            const int m2 = (m + 1) & ~1;
+            if (lane < m2) {
+                float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, c = a;
+                if (lane < m) {
+                    const int nd = S.clist[lane];
+                    a = wA[nd];
+                    b = wB[nd];
+                    c = wC[nd];
+                }
+                S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -a.w;
+                S.f[4][lane] = b.x; S.f[5][lane] = b.y; S.f[6][lane] = b.z;
+                S.f[7][lane] = c.x; S.f[8][lane] = c.y; S.f[9][lane] = c.z; S.f[10][lane] = c.w;
+            }
+            __syncwarp();
+            const float2 px = f2(pi.x), py = f2(pi.y), pz = f2(pi.z), e2 = f2(eps2);
+            const float2 m1 = f2(-1.f), c15 = f2(1.5f), cm75 = f2(-7.5f), c3 = f2(3.f);
+            float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), spp = f2(0.f);
+#pragma unroll 2
+            for (int k = 0; k < m2; k += 2) {
+                const float2 dx = __ffma2_rn(ld2(&S.f[0][k]), m1, px);
+                const float2 dy = __ffma2_rn(ld2(&S.f[1][k]), m1, py);
+                const float2 dz = __ffma2_rn(ld2(&S.f[2][k]), m1, pz);
+                float2 r2 = __ffma2_rn(dx, dx, e2);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                const float2 ri2 = __fmul2_rn(rinv, rinv);
+                const float2 g3 = __fmul2_rn(rinv, ri2), g5 = __fmul2_rn(g3, ri2),
+                             g7 = __fmul2_rn(g5, ri2);
+                const float2 qxx = ld2(&S.f[4][k]), qyy = ld2(&S.f[5][k]), qzz = ld2(&S.f[6][k]);
+                const float2 qxy = ld2(&S.f[7][k]), qxz = ld2(&S.f[8][k]), qyz = ld2(&S.f[9][k]);
+                const float2 qx = __ffma2_rn(qxx, dx, __ffma2_rn(qxy, dy, __fmul2_rn(qxz, dz)));
+                const float2 qy = __ffma2_rn(qxy, dx, __ffma2_rn(qyy, dy, __fmul2_rn(qyz, dz)));
+                const float2 qz = __ffma2_rn(qxz, dx, __ffma2_rn(qyz, dy, __fmul2_rn(qzz, dz)));
+                const float2 dqd = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+                const float2 tr = ld2(&S.f[10][k]), nm = ld2(&S.f[3][k]);
+                const float2 a7 = __fmul2_rn(dqd, g7), b5 = __fmul2_rn(tr, g5);
+                // s = -M g3 + 1.5 tr g5 - 7.5 dqd g7
+                const float2 sc = __ffma2_rn(b5, c15, __ffma2_rn(a7, cm75, __fmul2_rn(nm, g3)));
+                const float2 t5 = __fmul2_rn(g5, c3);
+                sx = __ffma2_rn(t5, qx, __ffma2_rn(sc, dx, sx));
+                sy = __ffma2_rn(t5, qy, __ffma2_rn(sc, dy, sy));
+                sz = __ffma2_rn(t5, qz, __ffma2_rn(sc, dz, sz));
+                if (POT) {
+                    // -(M rinv + 0.5 (3 dqd g5 - tr g3))
+                    const float2 hq = __ffma2_rn(__fmul2_rn(dqd, g5), f2(1.5f),
+                                                 __fmul2_rn(__fmul2_rn(tr, g3), f2(-0.5f)));
+                    spp = __ffma2_rn(nm, rinv, spp);
+                    spp = __ffma2_rn(hq, m1, spp);
+                }
+            }
+            ax.add(sx.x + sx.y); ay.add(sy.x + sy.y); az.add(sz.x + sz.y);
+            if (POT) ph.add(spp.x + spp.y);
+            nC += m;
+            __syncwarp();
+          } else {
             if (lane < m) {
                 int nd = S.clist[lane];
                 S.sa[lane] = wA[nd];
@@ -133,8 +212,42 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
             if (POT) ph.add(sp_);
             nC += m;
             __syncwarp();
+          }
         };
         auto flush_parts = [&](int m) {
+          if constexpr (PACKED) {
+            const int m2 = (m + 1) & ~1;
+            if (lane < m2) {
+                float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (lane < m) a = pw[S.plist[lane]];
+                S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -a.w;
+            }
+            __syncwarp();
+            const float2 px = f2(pi.x), py = f2(pi.y), pz = f2(pi.z), e2 = f2(eps2);
+            const float2 m1 = f2(-1.f);
+            float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), spp = f2(0.f);
+#pragma unroll 4
+            for (int k = 0; k < m2; k += 2) {
+                const float2 dx = __ffma2_rn(ld2(&S.f[0][k]), m1, px);
+                const float2 dy = __ffma2_rn(ld2(&S.f[1][k]), m1, py);
+                const float2 dz = __ffma2_rn(ld2(&S.f[2][k]), m1, pz);
+                float2 r2 = __ffma2_rn(dx, dx, e2);
+                r2 = __ffma2_rn(dy, dy, r2);
+                r2 = __ffma2_rn(dz, dz, r2);
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                const float2 nm = ld2(&S.f[3][k]);  // -m
+                const float2 nmr = __fmul2_rn(nm, rinv);
+                const float2 g = __fmul2_rn(nmr, __fmul2_rn(rinv, rinv));  // -m / r^3
+                sx = __ffma2_rn(g, dx, sx);
+                sy = __ffma2_rn(g, dy, sy);
+                sz = __ffma2_rn(g, dz, sz);
+                if (POT) spp = __fadd2_rn(spp, nmr);
+            }
+            ax.add(sx.x + sx.y); ay.add(sy.x + sy.y); az.add(sz.x + sz.y);
+            if (POT) ph.add(spp.x + spp.y);
+            nP += m;
+            __syncwarp();
+          } else {
             if (lane < m) S.sa[lane] = pw[S.plist[lane]];
             __syncwarp();
             R sx = 0, sy = 0, sz = 0, sp_ = 0;
@@ -154,6 +267,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
             if (POT) ph.add(sp_);
             nP += m;
             __syncwarp();
+          }
         };
 
         while (sp > 0 || nc > 0 || np > 0) {
