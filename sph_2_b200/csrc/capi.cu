@@ -305,6 +305,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(tmpb, rs * NN); ctx->wA = tmpb;
     DAF(tmpb, rs * NN); ctx->wB = tmpb;
     DAF(tmpb, rs * NN); ctx->wC = tmpb;
+    DAF(ctx->wL, NN);
     DAF(ctx->croot, C);
     const size_t G = N + C + 1;
     DAF(ctx->gstart, G); DAF(ctx->gcount, G); DAF(ctx->groot_g, G); DAF(ctx->gnode, G);

@@ -88,8 +88,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
            const int *__restrict__ gcloud, const int *__restrict__ croot,
            const typename R4<R>::T *__restrict__ pw, const typename R4<R>::T *__restrict__ wA,
            const typename R4<R>::T *__restrict__ wB, const typename R4<R>::T *__restrict__ wC,
-           const int *__restrict__ first, const int *__restrict__ last,
-           const int *__restrict__ child, int leaf_size, R eps2, double G, int n,
+           const int4 *__restrict__ wL, int leaf_size, R eps2, double G, int n,
            double *__restrict__ agrav, double *__restrict__ pot, unsigned *work,
            unsigned long long *counters, long long *status) {
     typedef typename R4<R>::T V4;
@@ -133,7 +132,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                     b = wB[nd];
                     c = wC[nd];
                 }
-                S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -a.w;
+                S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -b.w;
                 S.f[4][lane] = b.x; S.f[5][lane] = b.y; S.f[6][lane] = b.z;
                 S.f[7][lane] = c.x; S.f[8][lane] = c.y; S.f[9][lane] = c.z; S.f[10][lane] = c.w;
             }
@@ -201,12 +200,12 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                 const R qz = c.y * dx + c.z * dy + b.z * dz;
                 const R dqd = dx * qx + dy * qy + dz * qz;
                 const R tr = c.w;
-                const R s = -a.w * g3 + R(1.5) * tr * g5 - R(7.5) * dqd * g7;
+                const R s = -b.w * g3 + R(1.5) * tr * g5 - R(7.5) * dqd * g7;
                 const R t5 = R(3) * g5;
                 sx += s * dx + t5 * qx;
                 sy += s * dy + t5 * qy;
                 sz += s * dz + t5 * qz;
-                if (POT) sp_ -= a.w * rinv + R(0.5) * (R(3) * dqd * g5 - tr * g3);
+                if (POT) sp_ -= b.w * rinv + R(0.5) * (R(3) * dqd * g5 - tr * g3);
             }
             ax.add(sx); ay.add(sy); az.add(sz);
             if (POT) ph.add(sp_);
@@ -276,14 +275,18 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                 sp -= take;
                 int nd = 0, f = 0, cn = 0;
                 bool accept = false, open = false;
+                int cl = 0, cr = 0;
                 if (lane < take) {
                     nd = S.stk[sp + lane];
+                    // the two 16-byte records a node visit needs, issued together
                     const V4 a = wA[nd];
-                    const R r2o = wB[nd].w;
-                    f = first[nd];
-                    cn = last[nd] - f + 1;
+                    const int4 L = wL[nd];
+                    f = L.x;
+                    cn = L.y;
+                    cl = L.z;
+                    cr = L.w;
                     const R d2 = box_d2(bx0, by0, bz0, bx1, by1, bz1, a.x, a.y, a.z);
-                    accept = d2 >= r2o && cn > 1;
+                    accept = d2 >= a.w && cn > 1;
                     open = !accept;
                 }
                 __syncwarp();
@@ -299,8 +302,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                 if (sp + npush <= WSTK) {
                     if (inner) {
                         const int pos = sp + 2 * __popc(im & lt);
-                        S.stk[pos] = child[2 * nd + 1];
-                        S.stk[pos + 1] = child[2 * nd];
+                        S.stk[pos] = cr;
+                        S.stk[pos + 1] = cl;
                     }
                     sp += npush;
                     maxsp = max(maxsp, sp);
@@ -467,8 +470,8 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
     k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
         ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
         (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
-        (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->first,
-        ctx->last, ctx->child, ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
+        (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->wL,
+        ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
         ctx->work, ctx->counters, ctx->status);
     return SPH_OK;
 }

@@ -78,7 +78,10 @@ struct sph_ctx {
     int *child = nullptr, *parent = nullptr, *first = nullptr, *last = nullptr, *flag = nullptr;
     double *node = nullptr, *hmax = nullptr, *ropen2 = nullptr;
     void *node_box = nullptr;  // double4 [2][2*n_max]: (box min, h_max), (box max, 0)
-    void *wA = nullptr, *wB = nullptr, *wC = nullptr;  // Real4 walk records
+    // Real4 walk records per node: wA (com, r_open^2), wB (Qxx, Qyy, Qzz, M),
+    // wC (Qxy, Qxz, Qyz, trace); wL (first, count, left, right child)
+    void *wA = nullptr, *wB = nullptr, *wC = nullptr;
+    int4 *wL = nullptr;
     int *croot = nullptr;                              // per cloud root node
     int *gstart = nullptr, *gcount = nullptr, *groot_g = nullptr;  // groups: start, size, cloud id
     int *gnode = nullptr;                       // group -> tree node

@@ -23,7 +23,8 @@ __device__ __forceinline__ int delta_pref(const unsigned long long *__restrict__
 
 __global__ void k_karras(const unsigned long long *__restrict__ key, const int *__restrict__ cloud,
                          int n, int *__restrict__ child, int *__restrict__ parent,
-                         int *__restrict__ first, int *__restrict__ last, int *__restrict__ croot) {
+                         int *__restrict__ first, int *__restrict__ last, int *__restrict__ croot,
+                         int4 *__restrict__ wL) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int d = (delta_pref(key, n, i, i + 1) - delta_pref(key, n, i, i - 1)) > 0 ? 1 : -1;
@@ -50,6 +51,7 @@ __global__ void k_karras(const unsigned long long *__restrict__ key, const int *
     parent[R] = i;
     first[i] = lo;
     last[i] = hi;
+    wL[i] = make_int4(lo, hi - lo + 1, L, R);
     int c = cloud[lo];
     if (cloud[hi] == c && (lo == 0 || cloud[lo - 1] != c) && (hi == n - 1 || cloud[hi + 1] != c))
         croot[c] = i;
@@ -67,8 +69,8 @@ __device__ __forceinline__ void write_walk(int nd, const double *o, double r2, d
                                            typename R4<R>::T *wA, typename R4<R>::T *wB,
                                            typename R4<R>::T *wC) {
     typename R4<R>::T a, b, c;
-    a.x = (R)o[0]; a.y = (R)o[1]; a.z = (R)o[2]; a.w = (R)o[3];
-    b.x = (R)o[4]; b.y = (R)o[5]; b.z = (R)o[6]; b.w = (R)r2;
+    a.x = (R)o[0]; a.y = (R)o[1]; a.z = (R)o[2]; a.w = (R)r2;
+    b.x = (R)o[4]; b.y = (R)o[5]; b.z = (R)o[6]; b.w = (R)o[3];
     c.x = (R)o[7]; c.y = (R)o[8]; c.z = (R)o[9];
     c.w = (R)(o[4] + o[5] + o[6]);  // trace of the second moments
     (void)hm;
@@ -96,7 +98,8 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
                          double *__restrict__ hmax, double *__restrict__ ropen2,
                          double4 *__restrict__ sA, double4 *__restrict__ sB, int *__restrict__ flag,
                          int *__restrict__ first, int *__restrict__ last, int *__restrict__ child,
-                         typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC) {
+                         typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC,
+                         int4 *__restrict__ wL) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     int nd = n - 1 + p;
@@ -114,6 +117,7 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
     last[nd] = p;
     child[2 * nd] = -1;
     child[2 * nd + 1] = -1;
+    wL[nd] = make_int4(p, 1, -1, -1);
     write_walk<R>(nd, o, 0.0, h[p], wA, wB, wC);
     if (p < n - 1) flag[p] = 0;
 }
@@ -209,7 +213,7 @@ int launch_tree(sph_ctx *ctx) {
     const bool mixed = ctx->cfg.precision == SPH_PREC_MIXED;
     if (n > 1)
         k_karras<<<div_up(n - 1, 256), 256, 0, s>>>(key, ctx->cloud[c], n, ctx->child, ctx->parent,
-                                                    ctx->first, ctx->last, ctx->croot);
+                                                    ctx->first, ctx->last, ctx->croot, ctx->wL);
     k_single_roots<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->cloud_start, ctx->ncloud, n,
                                                             ctx->croot);
     // leaf records; the root has no parent
@@ -220,7 +224,7 @@ int launch_tree(sph_ctx *ctx) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
-            ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
+            ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->wL);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
             ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
@@ -228,7 +232,7 @@ int launch_tree(sph_ctx *ctx) {
         k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
-            ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
+            ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->wL);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
             ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
