@@ -42,6 +42,8 @@ extern "C" {
 #define SPH_ERR_NONFINITE (-6)  /* NaN/Inf found in positions or results               */
 #define SPH_ERR_STATE (-7)      /* call order violated (e.g. forces before density)    */
 #define SPH_ERR_NOMEM (-8)      /* device allocation failed                            */
+#define SPH_ERR_IO (-9)         /* file cannot be opened/read/written, or its size
+                                   does not match the format                         */
 
 /* ---- enums ---- */
 #define SPH_PREC_FP64 0   /* every sum and the gravity walk in FP64                  */
@@ -322,6 +324,27 @@ int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
 #define SPH_NOALLOC_MAX_N 262144
 int sph_morton_sort_noalloc(const double *x, const double *y, const double *z, int32_t n,
                             uint64_t *keys, int32_t *perm, void *cuda_stream);
+
+/* ---- the reference's binary files (host I/O) ---- */
+/* IC file of IC_evrard4.cu:245-260 / readVectorsFromFile
+ * (hfvCLibs_v7_hfv_v2.h:59-101): int32 N, int32 Typ[N], then float32 x, y, z,
+ * vx, vy, vz, u, h, eps, mass, N values each.  sph_ic_count reads and checks
+ * the header (file size must equal 4 + 44 N) and needs no GPU.  sph_load_ic
+ * replaces the context's particles with the file's (widened to FP64; Typ must
+ * be 0, gas, else SPH_ERR_ARG); eps_out (host, n, may be NULL) receives the
+ * per-particle softening column.  sph_write_ic writes the context's particles
+ * in original order (Typ 0; eps = the given host array, or h as
+ * IC_evrard4.cu:224-229 does when eps is NULL). */
+int sph_ic_count(const char *path, int32_t *n);
+int sph_load_ic(sph_ctx *ctx, const char *path, double *eps_out);
+int sph_write_ic(sph_ctx *ctx, const char *path, const double *eps);
+/* Snapshot of saveArraysToBinary (hfvCLibs_v7_hfv_v2.h:107-143), as read by
+ * Evrard_test/singlex_gpu_data.py:55-72: int32 N, int32 N_ionFrac, int32
+ * Typ[N], float32 x, y, z, vx, vy, vz, rho, h, u, mass (N each), float32
+ * ionFrac[N_ionFrac], int32 per-particle debug slot[N] (written here as the
+ * neighbour count, -1 before the first list build).  Original particle order.
+ * ion_frac is host memory and may be NULL when n_ion_frac is 0. */
+int sph_write_snapshot(sph_ctx *ctx, const char *path, const float *ion_frac, int32_t n_ion_frac);
 
 /* The same entry points a single GPU runs, for a rank of a multi-GPU job
  * that owns a slice of the ensemble: nothing here talks to other ranks. */

@@ -17,6 +17,7 @@ SPH_OK = 0
 ERRORS = {
     -1: "SPH_ERR_ARG", -2: "SPH_ERR_CUDA", -3: "SPH_ERR_CAPACITY", -4: "SPH_ERR_NOCONV",
     -5: "SPH_ERR_OVERFLOW", -6: "SPH_ERR_NONFINITE", -7: "SPH_ERR_STATE", -8: "SPH_ERR_NOMEM",
+    -9: "SPH_ERR_IO",
 }
 PREC = {"fp64": 0, "mixed": 1}
 AV = {"mg83": 0, "gadget": 1}
@@ -120,6 +121,10 @@ SIGNATURES = [
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),
     ("sph_morton_sort_noalloc", C.c_int, [_P, _P, _P, _I, _P, _P, _P]),
+    ("sph_ic_count", C.c_int, [C.c_char_p, _P]),
+    ("sph_load_ic", C.c_int, [_P, C.c_char_p, _P]),
+    ("sph_write_ic", C.c_int, [_P, C.c_char_p, _P]),
+    ("sph_write_snapshot", C.c_int, [_P, C.c_char_p, _P, _I]),
     ("sph_prologue", C.c_int, [_P]),
     ("sph_step", C.c_int, [_P, _I]),
 ]

@@ -69,6 +69,13 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def ic_count(path) -> int:
+    """Particle count of a reference IC file, its size checked (no GPU)."""
+    n = C.c_int32(0)
+    L.check(L.load().sph_ic_count(str(path).encode(), C.byref(n)), "sph_ic_count")
+    return int(n.value)
+
+
 class Context:
     """One device context (capacity n_max particles, n_cloud_max clouds)."""
 
@@ -136,8 +143,34 @@ class Context:
         self._chk(self._L.sph_load(self._h, n, _ptr(cl), _ptr(x), _ptr(y), _ptr(z), _ptr(vx),
                                    _ptr(vy), _ptr(vz), _ptr(m), _ptr(h), _ptr(u), 1), "sph_load")
 
-    def get(self, name: str, storage_order=False) -> np.ndarray:
-        out = np.zeros(self.n)
+    def load_ic(self, path, want_eps=False):
+        """Replace the particles with those of a reference IC file
+        (IC_evrard4.cu:245-260 layout); returns the file's eps column if asked."""
+        n = ic_count(path)
+        eps = np.zeros(max(n, 1)) if want_eps else None
+        self._chk(self._L.sph_load_ic(self._h, str(path).encode(), _ptr(eps)), "sph_load_ic")
+        return eps[:n] if want_eps else None
+
+    def write_ic(self, path, eps=None):
+        """Write the particles as a reference IC file (eps defaults to h)."""
+        e = None if eps is None else _f64(eps)
+        self._chk(self._L.sph_write_ic(self._h, str(path).encode(), _ptr(e)), "sph_write_ic")
+
+    def write_snapshot(self, path, ion_frac=None):
+        """Write a snapshot in the reference's saveArraysToBinary layout
+        (hfvCLibs_v7_hfv_v2.h:107-143)."""
+        ion = None if ion_frac is None else np.ascontiguousarray(ion_frac, dtype=np.float32)
+        nion = 0 if ion is None else int(ion.size)
+        self._chk(self._L.sph_write_snapshot(self._h, str(path).encode(), _ptr(ion), nion),
+                  "sph_write_snapshot")
+
+    def get(self, name: str, storage_order=False, out=None) -> np.ndarray:
+        """Field in original (or storage) order.  `out`: an existing C-contiguous
+        float64 array of n values (e.g. pinned host memory) to copy into."""
+        if out is None:
+            out = np.zeros(self.n)
+        elif out.dtype != np.float64 or out.shape != (self.n,) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of n values")
         self._chk(self._L.sph_get_field(self._h, L.FIELD[name], _ptr(out), 1, int(storage_order)),
                   f"get {name}")
         return out

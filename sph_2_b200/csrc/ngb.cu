@@ -32,7 +32,12 @@ struct SearchSmem {
     int stk[SSTK];
     int flat[96];
     double4 stage[32];
+    double smass[32];
 };
+
+template <class R> struct R2;
+template <> struct R2<float> { typedef float2 T; };
+template <> struct R2<double> { typedef double2 T; };
 
 __device__ __forceinline__ double wmin(double v) {
     for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
@@ -50,15 +55,22 @@ struct SearchArgs {
     const int *first, *last, *child;
     int leaf_size, K;
     int *rows, *cnt;
+    // candidate rows of the h iteration: (r_ij, m_j) pairs in the walk's real
+    // type, so that the Newton loop reads one contiguous row per particle
+    // instead of gathering positions and masses through the index row
+    void *cdat;
+    const void *p1;  // Real4 (v, m)
     long long *status;
 };
 
 // Walk the tree for group g and write the rows of the active lanes.
 // MODE 0: candidates r^2 <= ri^2 (ri = 2 hc_i, the h iteration's gather radius)
 // MODE 1: exact lists |r|^2 <= (h_i + h_j)^2
-template <int MODE>
+template <int MODE, class R = double>
 __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A, int g, bool act,
                                              int i, const double4 &pi, double ri) {
+    typedef typename R4<R>::T V4;
+    typedef typename R2<R>::T P2;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const double gx0 = wmin(act ? pi.x : INFINITY), gy0 = wmin(act ? pi.y : INFINITY),
@@ -79,21 +91,29 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         if (lane < m) {
             j = S.flat[lane];
             S.stage[lane] = A.p0[j];
+            if (MODE == 0) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
         }
         __syncwarp();
         for (int k = 0; k < m; k++) {
             const double4 pj = S.stage[k];
-            const int jj = __shfl_sync(FULL, j, k);
-            bool hit;
             if (MODE == 0) {
-                double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                hit = dx * dx + dy * dy + dz * dz <= ri2;
+                const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                if (act && dx * dx + dy * dy + dz * dz <= ri2) {
+                    if (count < K) {
+                        const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
+                        P2 v;
+                        v.x = sqrt(rx * rx + ry * ry + rz * rz);
+                        v.y = (R)S.smass[k];
+                        ((P2 *)A.cdat)[(size_t)i * K + count] = v;
+                    }
+                    count++;
+                }
             } else {
-                hit = ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w);
-            }
-            if (act && hit) {
-                if (count < K) A.rows[(size_t)i * K + count] = jj;
-                count++;
+                const int jj = __shfl_sync(FULL, j, k);
+                if (act && ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w)) {
+                    if (count < K) A.rows[(size_t)i * K + count] = jj;
+                    count++;
+                }
             }
         }
         __syncwarp();
@@ -158,8 +178,14 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         }
     }
     if (act) {
-        A.cnt[i] = min(count, K);
-        if (count > K) status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+        if (MODE == 0) {
+            // the full count: the Newton step shrinks the gather radius of a
+            // row that did not fit instead of iterating on a truncated one
+            A.cnt[i] = count;
+        } else {
+            A.cnt[i] = min(count, K);
+            if (count > K) status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+        }
     }
     if (overflow && lane == 0) status_add(A.status, SPH_S_STACK_OVERFLOW, 1);
     __syncwarp();
@@ -200,11 +226,35 @@ struct NewtonArgs {
 template <class R, int SLOTS>
 __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs &B, int i) {
     typedef typename R4<R>::T V4;
+    typedef typename R2<R>::T P2;
     const V4 *p1 = (const V4 *)B.p1;
     const int lane = threadIdx.x & 31;
     const double4 pi = A.p0[i];
-    const int c = A.cnt[i];
+    const int craw = A.cnt[i];
+    if (craw > A.K) {
+        // more candidates inside 2 hc than the row holds: the sums would miss
+        // some, so shrink hc towards a half-full row and search again; h
+        // restarts just below the new radius
+        if (lane == 0) {
+            if (!B.last_round) {
+                const double hc = B.hc[i] * fmax(0.5, cbrt(0.5 * A.K / (double)craw));
+                B.hc[i] = hc;
+                B.retry[i] = 1;
+                B.h_out[i] = hc / B.grow;
+                A.p0[i].w = hc / B.grow;
+                status_add(A.status, SPH_S_H_RETRY, 1);
+            } else {
+                B.retry[i] = 0;
+                status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+                status_add(A.status, SPH_S_H_NOCONV, 1);
+            }
+        }
+        __syncwarp();
+        return;
+    }
+    const int c = craw;
     const double mi = (double)p1[i].w;
+    const P2 *row = (const P2 *)A.cdat + (size_t)i * A.K;
     R rj[SLOTS], mj[SLOTS];
 #pragma unroll
     for (int s = 0; s < SLOTS; s++) {
@@ -212,11 +262,9 @@ __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs
         rj[s] = R(1e30);
         mj[s] = R(0);
         if (k < c) {
-            const int j = A.rows[(size_t)i * A.K + k];
-            const double4 pj = A.p0[j];
-            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
-            rj[s] = sqrt(dx * dx + dy * dy + dz * dz);
-            mj[s] = (R)p1[j].w;
+            const P2 v = row[k];
+            rj[s] = v.x;
+            mj[s] = v.y;
         }
     }
     const double cap = B.hc[i];
@@ -307,7 +355,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         const unsigned todo = __ballot_sync(FULL, act);
         if (!todo) continue;
         const double4 pi = A.p0[i];
-        group_search<0>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
+        group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
         __threadfence_block();
         __syncwarp();
         unsigned t = todo;
@@ -353,6 +401,8 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.K = ctx->cfg.max_ngb;
     A.rows = rows;
     A.cnt = cnt;
+    A.cdat = ctx->cand;
+    A.p1 = ctx->p1;
     A.status = ctx->status;
     return A;
 }
@@ -369,7 +419,7 @@ int launch_smoothing_h(sph_ctx *ctx) {
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->hcand, ctx->retry, H_GROW);
     const int rounds = ctx->prologue_done ? 3 : 8;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
-    SearchArgs A = search_args(ctx, ctx->cand, ctx->cand_cnt);
+    SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
     NewtonArgs B;
     B.p1 = ctx->p1;
     B.h_out = ctx->st[c][ST_H];

@@ -92,7 +92,8 @@ struct sph_ctx {
 
     // neighbours
     int *ngb = nullptr, *ngb_cnt = nullptr;
-    int *cand = nullptr, *cand_cnt = nullptr;
+    void *cand = nullptr;  // (r_ij, m_j) Real pairs, max_ngb per particle
+    int *cand_cnt = nullptr;
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
     double *hcand = nullptr;     // candidate radius / 2 used per particle
     bool lists_ok = false, rho_ok = false, divcurl_ok = false;
