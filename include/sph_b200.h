@@ -291,7 +291,10 @@ int sph_step(sph_ctx *ctx, int32_t nsteps);
 /* internal per-particle arrays for diagnostics, storage order:
  * 0 candidate count (int32), 1 list count (int32), 2 retry flag (int32),
  * 3 candidate radius / 2 (double), 4 h of the packed position record,
- * 5 mass of the packed velocity record (both as double) */
+ * 5 mass of the packed velocity record (both as double),
+ * 6 tree-search flags of the last list build (int32, n + 1: per particle 1 =
+ *   its list came from the tree search, not from its candidate row; the last
+ *   entry 1 = every list did) */
 int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host);
 
 /* ---- measurement ---- */

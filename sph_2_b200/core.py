@@ -323,8 +323,9 @@ class Context:
         self._chk(self._L.sph_step(self._h, nsteps), "sph_step")
 
     def debug_array(self, which: str) -> np.ndarray:
-        k = {"cand_cnt": 0, "ngb_cnt": 1, "retry": 2, "hcand": 3, "p0_h": 4, "p1_m": 5}[which]
-        out = np.zeros(self.n, np.float64 if k >= 3 else np.int32)
+        k = {"cand_cnt": 0, "ngb_cnt": 1, "retry": 2, "hcand": 3, "p0_h": 4, "p1_m": 5,
+             "tree_search": 6}[which]
+        out = np.zeros(self.n + (k == 6), np.float64 if 3 <= k <= 5 else np.int32)
         self._chk(self._L.sph_debug_copy(self._h, k, _ptr(out), 1), "debug_copy")
         return out
 

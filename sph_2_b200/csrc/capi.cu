@@ -314,7 +314,9 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->d_ngroup, 1);
     DAF(ctx->ngb, K * N); DAF(ctx->ngb_cnt, N);
     DAF(tmpb, (rs / 2) * K * N); ctx->cand = tmpb;  // Real2 per slot
+    DAF(ctx->cand_idx, K * N);
     DAF(ctx->cand_cnt, N);
+    DAF(ctx->lflag, N + 1);
     DAF(ctx->retry, N); DAF(ctx->hcand, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
     DAF(ctx->status, SPH_NSTATUS);
@@ -458,7 +460,7 @@ int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, con
         if (rc) return rc;
     }
     CK(cudaStreamSynchronize(s));
-    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = false;
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = ctx->cand_ok = false;
     ctx->p2_dirty = true;
     ctx->prologue_done = false;
     ctx->step_count = 0;
@@ -508,6 +510,7 @@ int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host,
         rc = launch_pack_p1(ctx);
         if (rc) return rc;
         if (field <= SPH_F_Z || field == SPH_F_M) ctx->tree_ok = false;
+        ctx->cand_ok = false;
     }
     if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
     CK(cudaStreamSynchronize(s));
@@ -562,7 +565,7 @@ int sph_sort(sph_ctx *ctx) {
     if (rc) return rc;
     drop_graphs(ctx);
     rc = launch_sort(ctx);
-    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = false;
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = ctx->cand_ok = false;
     ctx->p2_dirty = true;
     return rc;
 }
@@ -744,7 +747,7 @@ int sph_kick(sph_ctx *ctx, double fac) {
 int sph_drift(sph_ctx *ctx) {
     int rc = enter(ctx);
     if (rc) return rc;
-    ctx->tree_ok = ctx->lists_ok = false;
+    ctx->tree_ok = ctx->lists_ok = ctx->cand_ok = false;
     return launch_drift(ctx);
 }
 
@@ -877,7 +880,13 @@ __global__ void k_dbg_w(int n, const double4 *p0, const void *p1, int mixed, dou
 int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host) {
     int rc = enter(ctx);
     if (rc) return rc;
-    if (!out || which < 0 || which > 5) return SPH_ERR_ARG;
+    if (!out || which < 0 || which > 6) return SPH_ERR_ARG;
+    if (which == 6) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaMemcpy(out, ctx->lflag, sizeof(int) * (ctx->n + 1),
+                      host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+        return SPH_OK;
+    }
     if (which >= 4) {
         const int n = ctx->n;
         k_dbg_w<<<div_up(n, 256), 256, 0, ctx->stream>>>(n, ctx->p0, ctx->p1,

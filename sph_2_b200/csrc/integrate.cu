@@ -11,6 +11,36 @@
 
 namespace {
 
+// Courant estimate of particle i: C min(h / v_sig, sqrt(h / |a|)), or 0 if
+// it is not a finite positive number
+__device__ __forceinline__ double courant_dt(double hi, double vs, double ax, double ay, double az,
+                                             double courant) {
+    const double amag = sqrt(ax * ax + ay * ay + az * az);
+    double t = hi / fmax(vs, 1e-300);
+    if (amag > 0.0) t = fmin(t, sqrt(hi / amag));
+    t *= courant;
+    return (t > 0.0 && isfinite(t)) ? t : 0.0;
+}
+
+// per-cloud minimum of t over the warp: one atomic per warp when the warp
+// holds one cloud (clouds are contiguous in storage order), else one per
+// lane.  Every lane of the warp calls; t = 0 marks a lane with no estimate.
+__device__ __forceinline__ void cloud_min(unsigned long long *dt_bits, bool valid, int c, double t) {
+    unsigned long long v = (valid && t > 0.0) ? dbl_to_ord(t) : ~0ULL;
+    const int cc = valid ? c : -1;
+    const int c0 = __shfl_sync(0xffffffffu, cc, 0);
+    if (__all_sync(0xffffffffu, !valid || cc == c0)) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w < v ? w : v;
+        }
+        if ((threadIdx.x & 31) == 0 && v != ~0ULL) atomicMin(&dt_bits[c0], v);
+    } else if (v != ~0ULL) {
+        atomicMin(&dt_bits[cc], v);
+    }
+}
+
 template <class R>
 __global__ void k_kick(int n, double *__restrict__ vx, double *__restrict__ vy,
                        double *__restrict__ vz, const double *__restrict__ asph,
@@ -18,27 +48,25 @@ __global__ void k_kick(int n, double *__restrict__ vx, double *__restrict__ vy,
                        const double *__restrict__ dt, double fac, typename R4<R>::T *__restrict__ p1,
                        int cfl, const double *__restrict__ h, const double *__restrict__ vsig,
                        double courant, unsigned long long *__restrict__ dt_bits) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int c = cloud[i];
-    const double d = dt[c] * fac;
-    const double ax = asph[i] + agrav[i], ay = asph[(size_t)n + i] + agrav[(size_t)n + i],
-                 az = asph[2 * (size_t)n + i] + agrav[2 * (size_t)n + i];
-    const double nx = vx[i] + ax * d, ny = vy[i] + ay * d, nz = vz[i] + az * d;
-    vx[i] = nx;
-    vy[i] = ny;
-    vz[i] = nz;
-    typename R4<R>::T q = p1[i];
-    q.x = (R)nx; q.y = (R)ny; q.z = (R)nz;
-    p1[i] = q;
-    if (cfl) {
-        const double hi = h[i];
-        const double amag = sqrt(ax * ax + ay * ay + az * az);
-        double t = hi / fmax(vsig[i], 1e-300);
-        if (amag > 0.0) t = fmin(t, sqrt(hi / amag));
-        t *= courant;
-        if (t > 0.0 && isfinite(t)) atomicMin(&dt_bits[c], dbl_to_ord(t));
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    int c = 0;
+    double t = 0.0;
+    if (valid) {
+        c = cloud[i];
+        const double d = dt[c] * fac;
+        const double ax = asph[i] + agrav[i], ay = asph[(size_t)n + i] + agrav[(size_t)n + i],
+                     az = asph[2 * (size_t)n + i] + agrav[2 * (size_t)n + i];
+        const double nx = vx[i] + ax * d, ny = vy[i] + ay * d, nz = vz[i] + az * d;
+        vx[i] = nx;
+        vy[i] = ny;
+        vz[i] = nz;
+        typename R4<R>::T q = p1[i];
+        q.x = (R)nx; q.y = (R)ny; q.z = (R)nz;
+        p1[i] = q;
+        if (cfl) t = courant_dt(h[i], vsig[i], ax, ay, az, courant);
     }
+    if (cfl) cloud_min(dt_bits, valid, c, t);
 }
 
 // the Courant estimate alone (prologue), from a = a_sph + a_grav
@@ -46,16 +74,17 @@ __global__ void k_cfl(int n, const double *__restrict__ asph, const double *__re
                       const int *__restrict__ cloud, const double *__restrict__ h,
                       const double *__restrict__ vsig, double courant,
                       unsigned long long *__restrict__ dt_bits) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double ax = asph[i] + agrav[i], ay = asph[(size_t)n + i] + agrav[(size_t)n + i],
-                 az = asph[2 * (size_t)n + i] + agrav[2 * (size_t)n + i];
-    const double hi = h[i];
-    const double amag = sqrt(ax * ax + ay * ay + az * az);
-    double t = hi / fmax(vsig[i], 1e-300);
-    if (amag > 0.0) t = fmin(t, sqrt(hi / amag));
-    t *= courant;
-    if (t > 0.0 && isfinite(t)) atomicMin(&dt_bits[cloud[i]], dbl_to_ord(t));
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    int c = 0;
+    double t = 0.0;
+    if (valid) {
+        const double ax = asph[i] + agrav[i], ay = asph[(size_t)n + i] + agrav[(size_t)n + i],
+                     az = asph[2 * (size_t)n + i] + agrav[2 * (size_t)n + i];
+        c = cloud[i];
+        t = courant_dt(h[i], vsig[i], ax, ay, az, courant);
+    }
+    cloud_min(dt_bits, valid, c, t);
 }
 
 // dt[c] <- min(Courant estimate, dt_max) (or the fixed step); reset the bits

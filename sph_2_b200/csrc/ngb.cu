@@ -14,12 +14,13 @@
 // particle.  Rows are written in traversal order (deterministic);
 // sph_get_neighbours exports them sorted.
 //
-// h iteration (fused with the candidate search): after a group's candidate rows
-// are written, the same warp takes the group's particles one at a time, keeps
-// that particle's candidate distances and masses in registers (a few per lane)
-// and runs a bracketed Newton iteration on (4pi/3)(2h)^3 rho(h) = n_ngb m with
-// FP64 updates and convergence test.  Particles whose h outgrows the candidate
-// radius are flagged and searched again in the next round.
+// h iteration (fused with the candidate search): the search writes each
+// lane's candidates as (r_ij, m_j) pairs into rows laid out k-major over the
+// group's slots, then every lane runs a bracketed Newton iteration on
+// (4pi/3)(2h)^3 rho(h) = n_ngb m over its own row (coalesced across the warp)
+// with FP64 updates and convergence test.  Particles whose h outgrows the
+// candidate radius are flagged and searched again in the next round; a row
+// that overflows shrinks the radius instead.
 #include "sph_internal.cuh"
 
 namespace {
@@ -33,7 +34,16 @@ struct SearchSmem {
     int flat[96];
     double4 stage[32];
     double smass[32];
+    // FP32 copies of the staged positions relative to the group's centre and
+    // of their h, one array per field (two entries per 64-bit load)
+    __align__(8) float fx[32];
+    __align__(8) float fy[32];
+    __align__(8) float fz[32];
+    __align__(8) float fh[32];
 };
+
+__device__ __forceinline__ float2 ldf2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
 
 template <class R> struct R2;
 template <> struct R2<float> { typedef float2 T; };
@@ -55,11 +65,17 @@ struct SearchArgs {
     const int *first, *last, *child;
     int leaf_size, K;
     int *rows, *cnt;
+    int *ngb_cnt;  // list counts written by k_lists_cand (cnt holds candidate counts)
+    double *hnb;   // per particle: the largest h_j of its list (written by the list builds)
     // candidate rows of the h iteration: (r_ij, m_j) pairs in the walk's real
     // type, so that the Newton loop reads one contiguous row per particle
     // instead of gathering positions and masses through the index row
     void *cdat;
+    int *cidx;       // candidate particle slots, same layout as cdat
     const void *p1;  // Real4 (v, m)
+    // exact search restricted to the particles with only[i] != 0, or to all
+    // of them when *only_all != 0 (null: every particle)
+    const int *only, *only_all;
     long long *status;
 };
 
@@ -80,39 +96,83 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const double rmax = wmax(act ? ri : 0.0);
     const double ri2 = ri * ri;
     const int K = A.K;
+    // candidate rows of the group's slots [s0, s0 + gc) occupy entries
+    // [s0 K, (s0 + gc) K) k-major: entry k of lane l at s0 K + k gc + l, so
+    // the lanes of the Newton loop read entry k of their rows coalesced
+    const size_t cbase = MODE == 0 ? (size_t)A.gstart[g] * K + lane : 0;
+    const int cstride = MODE == 0 ? A.gcount[g] : 0;
     int count = 0;
+    double hnb = 0.0;
     int sp = 1, nflat = 0;
     bool overflow = false;
     if (lane == 0) S.stk[0] = A.croot[A.gcloud[g]];
     __syncwarp();
 
+    // FP32 prefilter: distances relative to the group's centre, compared
+    // with the threshold widened by 1e-4 (FP32 rounding of the relative
+    // coordinates is below 1e-6 of the threshold); the candidates it passes
+    // get the exact FP64 test, so the rows are the same as an FP64-only scan
+    const double cx = 0.5 * (gx0 + gx1), cy = 0.5 * (gy0 + gy1), cz = 0.5 * (gz0 + gz1);
+    const float2 pfx = bc2((float)(pi.x - cx)), pfy = bc2((float)(pi.y - cy)),
+                 pfz = bc2((float)(pi.z - cz));
+    const float2 ri2f = bc2((float)ri2 * 1.0001f), hif = bc2((float)pi.w);
+    const float2 m1 = bc2(-1.f), widen = bc2(1.0001f);
+
     auto process = [&](int m) {
-        int j = 0;
         if (lane < m) {
-            j = S.flat[lane];
-            S.stage[lane] = A.p0[j];
+            const int j = S.flat[lane];
+            const double4 q = A.p0[j];
+            S.stage[lane] = q;
+            S.fx[lane] = (float)(q.x - cx);
+            S.fy[lane] = (float)(q.y - cy);
+            S.fz[lane] = (float)(q.z - cz);
+            S.fh[lane] = (float)q.w;
             if (MODE == 0) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
+        } else if (lane < ((m + 1) & ~1)) {
+            // the odd tail of a chunk: an entry that never passes
+            S.fx[lane] = S.fy[lane] = S.fz[lane] = INFINITY;
+            S.fh[lane] = 0.f;
         }
         __syncwarp();
-        for (int k = 0; k < m; k++) {
+        unsigned hit = 0;
+        if (act) {
+#pragma unroll 4
+            for (int k = 0; k < m; k += 2) {
+                const float2 dx = __ffma2_rn(ldf2(&S.fx[k]), m1, pfx);
+                const float2 dy = __ffma2_rn(ldf2(&S.fy[k]), m1, pfy);
+                const float2 dz = __ffma2_rn(ldf2(&S.fz[k]), m1, pfz);
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                float2 lim = ri2f;
+                if (MODE == 1) {
+                    const float2 sh = __fadd2_rn(hif, ldf2(&S.fh[k]));
+                    lim = __fmul2_rn(__fmul2_rn(sh, sh), widen);
+                }
+                hit |= (r2.x <= lim.x ? 1u : 0u) << k;
+                hit |= (r2.y <= lim.y ? 2u : 0u) << k;
+            }
+        }
+        while (hit) {
+            const int k = __ffs(hit) - 1;
+            hit &= hit - 1;
             const double4 pj = S.stage[k];
             if (MODE == 0) {
                 const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                if (act && dx * dx + dy * dy + dz * dz <= ri2) {
+                if (dx * dx + dy * dy + dz * dz <= ri2) {
                     if (count < K) {
                         const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
                         P2 v;
                         v.x = sqrt(rx * rx + ry * ry + rz * rz);
                         v.y = (R)S.smass[k];
-                        ((P2 *)A.cdat)[(size_t)i * K + count] = v;
+                        ((P2 *)A.cdat)[cbase + (size_t)count * cstride] = v;
+                        A.cidx[cbase + (size_t)count * cstride] = S.flat[k];
                     }
                     count++;
                 }
             } else {
-                const int jj = __shfl_sync(FULL, j, k);
-                if (act && ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w)) {
-                    if (count < K) A.rows[(size_t)i * K + count] = jj;
+                if (ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w)) {
+                    if (count < K) A.rows[(size_t)i * K + count] = S.flat[k];
                     count++;
+                    hnb = fmax(hnb, pj.w);
                 }
             }
         }
@@ -185,6 +245,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         } else {
             A.cnt[i] = min(count, K);
             if (count > K) status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+            A.hnb[i] = hnb;
         }
     }
     if (overflow && lane == 0) status_add(A.status, SPH_S_STACK_OVERFLOW, 1);
@@ -199,18 +260,88 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
     const int ngroup = *ngroup_p;
     for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
-        const bool act = lane < gc;
+        bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
+        if (A.only && !*A.only_all) {
+            act = act && A.only[i];
+            if (!__any_sync(FULL, act)) continue;
+        }
         const double4 pi = A.p0[i];
         group_search<1>(smem[w], A, g, act, i, pi, pi.w);
     }
 }
 
-__global__ void k_h_init(int n, const double *__restrict__ h, double *__restrict__ hc,
-                         int *__restrict__ retry, double grow) {
+// Exact lists from the candidate rows of the h iteration.  A pair with
+// |r| <= h_i + h_j lies inside 2 max(h_i, h_j), so it sits in the candidate
+// row of the particle with the larger h (2 h <= 2 hc, the radius of that
+// particle's last candidate search).  Each lane filters its own row with the
+// exact predicate (same rounding as the tree search); where a pair's partner
+// j did not hold i in its own row (|r| beyond 2 hc_j, with a margin for
+// rounding), j's list may miss i and j is marked for the tree search.  A row
+// that is not a complete candidate set (overflow, or h above the candidate
+// radius after the last round) sends every particle to the tree search.
+__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+    k_lists_cand(const int *__restrict__ ngroup_p, SearchArgs A, const double *__restrict__ hc,
+                 int *__restrict__ full, int *__restrict__ full_all) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    const int K = A.K;
+    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+        const int s0 = A.gstart[g], gc = A.gcount[g];
+        if (lane >= gc) continue;
+        const int i = s0 + lane;
+        const double4 pi = A.p0[i];
+        const int craw = A.cnt[i];
+        if (craw > K || !(pi.w <= hc[i])) {
+            *full_all = 1;
+            continue;
+        }
+        const int *crow = A.cidx + (size_t)s0 * K + lane;
+        const double4 *__restrict__ p0 = A.p0;
+        int count = 0;
+        double hnb = 0.0;
+        // four candidates per round: their index, position and radius loads
+        // are issued together (the loop is bound by gather latency)
+        constexpr int U = 4;
+        for (int k0 = 0; k0 < craw; k0 += U) {
+            int jj[U];
+            double4 pj[U];
+            double hj[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) jj[u] = k0 + u < craw ? __ldg(&crow[(size_t)(k0 + u) * gc]) : i;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                pj[u] = p0[jj[u]];
+                hj[u] = __ldg(&hc[jj[u]]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (k0 + u < craw && ngb_pred(pi.x, pi.y, pi.z, pi.w, pj[u].x, pj[u].y, pj[u].z, pj[u].w)) {
+                    if (count < K) A.rows[(size_t)i * K + count] = jj[u];
+                    count++;
+                    hnb = fmax(hnb, pj[u].w);
+                    const double dx = pi.x - pj[u].x, dy = pi.y - pj[u].y, dz = pi.z - pj[u].z;
+                    const double rj = 2.0 * hj[u];
+                    if (dx * dx + dy * dy + dz * dz > rj * rj * (1.0 - 1e-9)) full[jj[u]] = 1;
+                }
+            }
+        }
+        A.ngb_cnt[i] = min(count, K);
+        if (count > K) status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+        A.hnb[i] = hnb;
+    }
+}
+
+// candidate radius 2 hc: a margin `grow` over h for the iteration, widened
+// to reach h_i + 1.05 h_nb (the largest neighbour h of the last list build) so
+// that the next list is complete from the particle's own candidates, at most
+// to 2 (1.5 h)
+__global__ void k_h_init(int n, const double *__restrict__ h, const double *__restrict__ hnb,
+                         double *__restrict__ hc, int *__restrict__ retry, double grow) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    hc[i] = h[i] * grow;
+    const double hi = h[i];
+    hc[i] = fmax(hi * grow, fmin(0.5 * (hi + 1.05 * hnb[i]), 1.5 * hi));
     retry[i] = 1;
 }
 
@@ -222,51 +353,37 @@ struct NewtonArgs {
     int max_iter, last_round;
 };
 
-// Newton iteration of particle i by the whole warp (candidate row of i).
-template <class R, int SLOTS>
-__device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs &B, int i) {
+// Newton iteration of the particle of every active lane over its own
+// candidate row (entry k at row[k * gc], see group_search), FP32 or FP64
+// kernel sums with FP64 update and convergence test.  No warp collectives:
+// lanes run independent iteration counts.
+template <class R>
+__device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArgs &B, int i,
+                                            const double4 &pi, const void *rowp, int gc) {
     typedef typename R4<R>::T V4;
     typedef typename R2<R>::T P2;
-    const V4 *p1 = (const V4 *)B.p1;
-    const int lane = threadIdx.x & 31;
-    const double4 pi = A.p0[i];
+    const P2 *row = (const P2 *)rowp;
     const int craw = A.cnt[i];
     if (craw > A.K) {
         // more candidates inside 2 hc than the row holds: the sums would miss
         // some, so shrink hc towards a half-full row and search again; h
         // restarts just below the new radius
-        if (lane == 0) {
-            if (!B.last_round) {
-                const double hc = B.hc[i] * fmax(0.5, cbrt(0.5 * A.K / (double)craw));
-                B.hc[i] = hc;
-                B.retry[i] = 1;
-                B.h_out[i] = hc / B.grow;
-                A.p0[i].w = hc / B.grow;
-                status_add(A.status, SPH_S_H_RETRY, 1);
-            } else {
-                B.retry[i] = 0;
-                status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
-                status_add(A.status, SPH_S_H_NOCONV, 1);
-            }
+        if (!B.last_round) {
+            const double hc = B.hc[i] * fmax(0.5, cbrt(0.5 * A.K / (double)craw));
+            B.hc[i] = hc;
+            B.retry[i] = 1;
+            B.h_out[i] = hc / B.grow;
+            A.p0[i].w = hc / B.grow;
+            status_add(A.status, SPH_S_H_RETRY, 1);
+        } else {
+            B.retry[i] = 0;
+            status_add(A.status, SPH_S_NGB_OVERFLOW, 1);
+            status_add(A.status, SPH_S_H_NOCONV, 1);
         }
-        __syncwarp();
         return;
     }
     const int c = craw;
-    const double mi = (double)p1[i].w;
-    const P2 *row = (const P2 *)A.cdat + (size_t)i * A.K;
-    R rj[SLOTS], mj[SLOTS];
-#pragma unroll
-    for (int s = 0; s < SLOTS; s++) {
-        const int k = lane + 32 * s;
-        rj[s] = R(1e30);
-        mj[s] = R(0);
-        if (k < c) {
-            const P2 v = row[k];
-            rj[s] = v.x;
-            mj[s] = v.y;
-        }
-    }
+    const double mi = (double)((const V4 *)B.p1)[i].w;
     const double cap = B.hc[i];
     const double cfac = 4.0 * SPH_PI / 3.0 * 8.0;
     double h = pi.w, lo = 0.0, hi = INFINITY;
@@ -278,9 +395,9 @@ __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs
         }
         const R inv_h = R(1.0 / h);
         KSum<R> S, D;
-#pragma unroll
-        for (int s = 0; s < SLOTS; s++) {
-            const R q = rj[s] * inv_h;
+        for (int k = 0; k < c; k++) {
+            const P2 v = row[(size_t)k * gc];
+            const R q = v.x * inv_h;
             if (q < R(2)) {
                 R w, dw;
                 if (q <= R(1)) {
@@ -291,11 +408,11 @@ __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs
                     w = R(0.25) * t * t * t;
                     dw = R(1.5) * t * t * (R(1) - q);
                 }
-                S.add(mj[s] * w);
-                D.add(mj[s] * dw);
+                S.add(v.y * w);
+                D.add(v.y * dw);
             }
         }
-        const double Ssum = seg_sum<32>(S.value()), Dsum = seg_sum<32>(D.value());
+        const double Ssum = S.value(), Dsum = D.value();
         const double h3 = h * h * h;
         const double rho = SPH_SIG / h3 * Ssum;
         const double drho = -SPH_SIG / (h3 * h) * Dsum;
@@ -325,23 +442,20 @@ __device__ __forceinline__ void newton_one(const SearchArgs &A, const NewtonArgs
             break;
         }
     }
-    if (lane == 0) {
-        if (need && !B.last_round) {
-            B.hc[i] = h * B.grow;
-            B.retry[i] = 1;
-        } else {
-            B.retry[i] = 0;
-            if (!ok) status_add(A.status, SPH_S_H_NOCONV, 1);
-        }
-        if (need) status_add(A.status, SPH_S_H_RETRY, 1);
-        B.h_out[i] = h;
-        A.p0[i].w = h;  // p0 is written only by the warp owning particle i
+    if (need && !B.last_round) {
+        B.hc[i] = h * B.grow;
+        B.retry[i] = 1;
+    } else {
+        B.retry[i] = 0;
+        if (!ok) status_add(A.status, SPH_S_H_NOCONV, 1);
     }
-    __syncwarp();
+    if (need) status_add(A.status, SPH_S_H_RETRY, 1);
+    B.h_out[i] = h;
+    A.p0[i].w = h;  // p0 is written only by the lane owning particle i
 }
 
 // candidate search + Newton iteration for the flagged particles of each group
-template <class R, int SLOTS>
+template <class R>
 __global__ void __launch_bounds__(SEARCH_WARPS * 32)
     k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B) {
     __shared__ SearchSmem smem[SEARCH_WARPS];
@@ -356,14 +470,11 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         if (!todo) continue;
         const double4 pi = A.p0[i];
         group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
-        __threadfence_block();
+        // each lane reads back only the row entries it wrote itself
+        if (act)
+            newton_lane<R>(A, B, i, pi,
+                           (const typename R2<R>::T *)A.cdat + (size_t)s0 * A.K + lane, gc);
         __syncwarp();
-        unsigned t = todo;
-        while (t) {
-            const int l = __ffs(t) - 1;
-            t &= t - 1;
-            newton_one<R, SLOTS>(A, B, s0 + l);
-        }
     }
 }
 
@@ -402,6 +513,11 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.rows = rows;
     A.cnt = cnt;
     A.cdat = ctx->cand;
+    A.cidx = ctx->cand_idx;
+    A.ngb_cnt = ctx->ngb_cnt;
+    A.hnb = ctx->st[ctx->cur][ST_HNB];
+    A.only = nullptr;
+    A.only_all = nullptr;
     A.p1 = ctx->p1;
     A.status = ctx->status;
     return A;
@@ -416,7 +532,8 @@ int launch_smoothing_h(sph_ctx *ctx) {
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
-    k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->hcand, ctx->retry, H_GROW);
+    k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
+                                            ctx->retry, H_GROW);
     const int rounds = ctx->prologue_done ? 3 : 8;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
@@ -429,29 +546,37 @@ int launch_smoothing_h(sph_ctx *ctx) {
     B.tol = ctx->cfg.h_tol;
     B.grow = H_GROW;
     B.max_iter = ctx->cfg.h_max_iter;
-    const bool wide = (ctx->cfg.max_ngb + 31) / 32 > 8;
     for (int r = 0; r < rounds; r++) {
         B.last_round = r == rounds - 1;
-        if (ctx->cfg.precision == SPH_PREC_MIXED) {
-            if (!wide) k_cand_newton<float, 8><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
-            else k_cand_newton<float, 16><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
-        } else {
-            if (!wide) k_cand_newton<double, 8><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
-            else k_cand_newton<double, 16><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
-        }
+        if (ctx->cfg.precision == SPH_PREC_MIXED)
+            k_cand_newton<float><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+        else
+            k_cand_newton<double><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
     }
     ctx->lists_ok = false;
+    ctx->cand_ok = true;
     return ctx_check_launch(ctx, "smoothing_h");
 }
 
 int launch_neighbours(sph_ctx *ctx) {
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    SearchArgs A = search_args(ctx, ctx->ngb, ctx->ngb_cnt);
+    if (ctx->cand_ok) {
+        // lists from the candidate rows, then the tree search for the
+        // particles whose rows cannot show that their list is complete
+        CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 1), s));
+        SearchArgs C = search_args(ctx, ctx->ngb, ctx->cand_cnt);
+        k_lists_cand<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, C, ctx->hcand, ctx->lflag,
+                                                       ctx->lflag + n);
+        A.only = ctx->lflag;
+        A.only_all = ctx->lflag + n;
+    }
     int rc = launch_refit_hmax(ctx);
     if (rc) return rc;
-    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
-    k_lists<<<grid, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup,
-                                                         search_args(ctx, ctx->ngb, ctx->ngb_cnt));
+    k_lists<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A);
     ctx->lists_ok = true;
     ctx->rho_ok = ctx->divcurl_ok = false;
     return ctx_check_launch(ctx, "neighbours");

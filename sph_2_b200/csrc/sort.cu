@@ -251,6 +251,7 @@ static int morton_bits_for(int ncloud) {
 }
 
 int launch_sort(sph_ctx *ctx) {
+    ctx->cand_ok = false;
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;

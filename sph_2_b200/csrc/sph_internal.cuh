@@ -34,7 +34,10 @@
     } while (0)
 
 // ---- state field indices of the double-buffered persistent SoA ----
-enum { ST_X, ST_Y, ST_Z, ST_VX, ST_VY, ST_VZ, ST_M, ST_H, ST_U, ST_DUDT_PREV, ST_N };
+// ST_HNB: the largest h among the particle's list neighbours at the last list
+// build (widens its next candidate search so that its list is complete from
+// its own candidates)
+enum { ST_X, ST_Y, ST_Z, ST_VX, ST_VY, ST_VZ, ST_M, ST_H, ST_U, ST_DUDT_PREV, ST_HNB, ST_N };
 
 struct sph_ctx {
     sph_config cfg;
@@ -93,7 +96,10 @@ struct sph_ctx {
     // neighbours
     int *ngb = nullptr, *ngb_cnt = nullptr;
     void *cand = nullptr;  // (r_ij, m_j) Real pairs, max_ngb per particle
+    int *cand_idx = nullptr;  // candidate slots j, same layout as cand
     int *cand_cnt = nullptr;
+    int *lflag = nullptr;     // n+1: per particle "needs the tree search", then "all do"
+    bool cand_ok = false;     // candidate rows match the current order, positions and h
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
     double *hcand = nullptr;     // candidate radius / 2 used per particle
     bool lists_ok = false, rho_ok = false, divcurl_ok = false;

@@ -205,6 +205,7 @@ __global__ void k_refit_up(int n, const int *__restrict__ parent, const int *__r
 }  // namespace
 
 int launch_tree(sph_ctx *ctx) {
+    ctx->cand_ok = false;
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;

@@ -175,6 +175,31 @@ def test_neighbour_lists_with_coincident_particles():
     assert np.array_equal(off, oo) and np.array_equal(lst, ol)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lists_from_candidate_rows_with_steep_h_contrast(precision):
+    """A dense clump inside a sparse halo: at the clump's edge h jumps by far
+    more than the candidate radius margin, so some lists are missing pairs in
+    their own candidate rows and must come from the tree search.  Every list
+    is still the exact |r| <= h_i + h_j set."""
+    rng = np.random.default_rng(21)
+    n_in, n_out = 1000, 3000      # h ratios up to 2.6 between neighbours
+    a = rng.normal(size=(n_in, 3)); a *= (0.35 * rng.random(n_in) ** (1 / 3) / np.linalg.norm(a, axis=1))[:, None]
+    b = rng.normal(size=(n_out, 3)); b *= (rng.random(n_out) ** (1 / 3) / np.linalg.norm(b, axis=1))[:, None]
+    pos = np.concatenate([a, b])
+    n = n_in + n_out
+    ctx = make_ctx(n, precision)
+    ctx.load(pos, np.zeros((n, 3)), np.full(n, 1.0 / n), np.full(n, 0.05), np.full(n, 0.05))
+    ctx.sort(); ctx.build_tree(); ctx.smoothing_h(); ctx.neighbours()
+    st = ctx.status()
+    assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0
+    flags = ctx.debug_array("tree_search")
+    assert flags[-1] == 0 and 0 < flags[:-1].sum() < n // 2
+    off, lst = ctx.neighbour_lists()
+    x, y, z, m, h = storage_state(ctx)
+    oo, ol = O.neighbours(x, y, z, h)
+    assert np.array_equal(off, oo) and np.array_equal(lst, ol)
+
+
 # --------------------------------------------------------- SPH sums --------
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 2e-5)])
 @pytest.mark.parametrize("av,bal", [("mg83", False), ("gadget", True)])
