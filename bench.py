@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--theta", type=float, default=0.4)
+    ap.add_argument("--theta", type=float, default=0.38)
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
@@ -345,6 +345,35 @@ def main():
     else:
         fp64 = None
 
+    # ---- energy and momentum drift over 100 steps, N = 10,000 Evrard (the
+    # plain FP64 method's own configuration: theta 0.5, Courant 0.25) ----
+    conservation = {}
+    if not a.no_fp64:
+        n0 = 10_000
+        d0 = ic.evrard(n0, seed=42)
+        for prec in ("fp64", "mixed"):
+            c0 = Context(Config(n_max=n0, precision=prec, theta=0.5, leaf_size=a.leaf,
+                                ngb_lanes=a.lanes, flags=L.FLAG_POTENTIAL))
+            c0.set_stream(stream.cuda_stream)
+            c0.load(d0["pos"], d0["vel"], d0["m"], d0["h"], d0["u"])
+            c0.prologue()
+            e0 = c0.energies()
+            c0.step(100)
+            c0.sync()
+            e1 = c0.energies()
+            E0 = e0["KE"] + e0["U"] + e0["PE"]
+            E1 = e1["KE"] + e1["U"] + e1["PE"]
+            v = np.stack([c0.get("vx"), c0.get("vy"), c0.get("vz")], 1)
+            pscale = float(np.sum(d0["m"] * np.linalg.norm(v, axis=1)))
+            p1 = float(np.linalg.norm([e1["px"], e1["py"], e1["pz"]]))
+            conservation[prec] = {"E0": E0, "E100": E1, "rel_energy_drift": abs(E1 - E0) / abs(E0),
+                                  "momentum_100": p1, "momentum_rel": p1 / pscale if pscale > 0 else None,
+                                  "KE100": e1["KE"], "status": c0.status()}
+            c0.close()
+        conservation["definition"] = ("E = KE + U + PE (PE from the tree walk's potential), "
+                                      "drift |E100 - E0| / |E0|; momentum |sum m v| after 100 steps, "
+                                      "relative to sum m |v|")
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
     if not a.no_e2e:
@@ -397,6 +426,7 @@ def main():
         "fp64_plain": fp64,
         "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
         "accel_err": err,
+        "conservation_100_steps_n10k": conservation,
         "phases_ms": phases,
         "status": final_status,
         "device_gb": ctx.device_bytes() / 1e9,

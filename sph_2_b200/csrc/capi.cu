@@ -313,10 +313,9 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->scan_tmp, N / 1024 + 64);
     DAF(ctx->d_ngroup, 1);
     DAF(ctx->ngb, K * N); DAF(ctx->ngb_cnt, N);
-    DAF(tmpb, (rs / 2) * K * N); ctx->cand = tmpb;  // Real2 per slot
     DAF(ctx->cand_idx, K * N);
     DAF(ctx->cand_cnt, N);
-    DAF(ctx->lflag, N + 1);
+    DAF(ctx->lflag, N + 2);
     DAF(ctx->retry, N); DAF(ctx->hcand, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
     DAF(ctx->status, SPH_NSTATUS);

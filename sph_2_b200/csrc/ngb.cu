@@ -15,10 +15,11 @@
 // sph_get_neighbours exports them sorted.
 //
 // h iteration (fused with the candidate search): the search writes each
-// lane's candidates as (r_ij, m_j) pairs into rows laid out k-major over the
-// group's slots, then every lane runs a bracketed Newton iteration on
-// (4pi/3)(2h)^3 rho(h) = n_ngb m over its own row (coalesced across the warp)
-// with FP64 updates and convergence test.  Particles whose h outgrows the
+// lane's candidate slots into rows laid out k-major over the group's slots and
+// accumulates the kernel sums of the first Newton evaluation on the way; every
+// lane then runs a bracketed Newton iteration on (4pi/3)(2h)^3 rho(h) = n_ngb m
+// with FP64 updates and convergence test, gathering its row again only for
+// the rare second and later evaluations.  Particles whose h outgrows the
 // candidate radius are flagged and searched again in the next round; a row
 // that overflows shrinks the radius instead.
 #include "sph_internal.cuh"
@@ -49,6 +50,36 @@ template <class R> struct R2;
 template <> struct R2<float> { typedef float2 T; };
 template <> struct R2<double> { typedef double2 T; };
 
+// Sums of the h iteration at one trial h: S = sum m_j w(q), D = sum m_j
+// w'(q)-form (q = r_ij / h, M4 kernel without its 1/(pi h^3) factor)
+template <class R> struct HSums {
+    KSum<R> S, D;
+    R inv_h;
+    __device__ __forceinline__ void add(R r, R m) {
+        const R q = r * inv_h;
+        if (q < R(2)) {
+            R w, dw;
+            if (q <= R(1)) {
+                w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
+                dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
+            } else {
+                const R t = R(2) - q;
+                w = R(0.25) * t * t * t;
+                dw = R(1.5) * t * t * (R(1) - q);
+            }
+            S.add(m * w);
+            D.add(m * dw);
+        }
+    }
+};
+
+// |r_ij| in the sums' type: the difference taken in FP64, then rounded
+template <class R>
+__device__ __forceinline__ R pair_r(const double4 &pi, const double4 &pj) {
+    const R rx = (R)(pi.x - pj.x), ry = (R)(pi.y - pj.y), rz = (R)(pi.z - pj.z);
+    return sqrt(rx * rx + ry * ry + rz * rz);
+}
+
 __device__ __forceinline__ double wmin(double v) {
     for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
     return v;
@@ -67,11 +98,9 @@ struct SearchArgs {
     int *rows, *cnt;
     int *ngb_cnt;  // list counts written by k_lists_cand (cnt holds candidate counts)
     double *hnb;   // per particle: the largest h_j of its list (written by the list builds)
-    // candidate rows of the h iteration: (r_ij, m_j) pairs in the walk's real
-    // type, so that the Newton loop reads one contiguous row per particle
-    // instead of gathering positions and masses through the index row
-    void *cdat;
-    int *cidx;       // candidate particle slots, same layout as cdat
+    // candidate rows of the h iteration: the slots j inside the particle's
+    // candidate radius, laid out k-major over the group (see group_search)
+    int *cidx;
     const void *p1;  // Real4 (v, m)
     // exact search restricted to the particles with only[i] != 0, or to all
     // of them when *only_all != 0 (null: every particle)
@@ -84,9 +113,9 @@ struct SearchArgs {
 // MODE 1: exact lists |r|^2 <= (h_i + h_j)^2
 template <int MODE, class R = double>
 __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A, int g, bool act,
-                                             int i, const double4 &pi, double ri) {
+                                             int i, const double4 &pi, double ri,
+                                             HSums<R> *hs = nullptr) {
     typedef typename R4<R>::T V4;
-    typedef typename R2<R>::T P2;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const double gx0 = wmin(act ? pi.x : INFINITY), gy0 = wmin(act ? pi.y : INFINITY),
@@ -158,14 +187,10 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             if (MODE == 0) {
                 const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                 if (dx * dx + dy * dy + dz * dz <= ri2) {
-                    if (count < K) {
-                        const R rx = (R)dx, ry = (R)dy, rz = (R)dz;
-                        P2 v;
-                        v.x = sqrt(rx * rx + ry * ry + rz * rz);
-                        v.y = (R)S.smass[k];
-                        ((P2 *)A.cdat)[cbase + (size_t)count * cstride] = v;
-                        A.cidx[cbase + (size_t)count * cstride] = S.flat[k];
-                    }
+                    // the first Newton evaluation (at h = pi.w) rides on the
+                    // search: rows are only re-read by later iterations
+                    hs->add(pair_r<R>(pi, pj), (R)S.smass[k]);
+                    if (count < K) A.cidx[cbase + (size_t)count * cstride] = S.flat[k];
                     count++;
                 }
             } else {
@@ -282,7 +307,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
 // radius after the last round) sends every particle to the tree search.
 __global__ void __launch_bounds__(SEARCH_WARPS * 32)
     k_lists_cand(const int *__restrict__ ngroup_p, SearchArgs A, const double *__restrict__ hc,
-                 int *__restrict__ full, int *__restrict__ full_all) {
+                 int *__restrict__ full, int *__restrict__ full_all, int *__restrict__ full_any) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
     const int K = A.K;
@@ -294,6 +319,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         const int craw = A.cnt[i];
         if (craw > K || !(pi.w <= hc[i])) {
             *full_all = 1;
+            *full_any = 1;
             continue;
         }
         const int *crow = A.cidx + (size_t)s0 * K + lane;
@@ -322,7 +348,10 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
                     hnb = fmax(hnb, pj[u].w);
                     const double dx = pi.x - pj[u].x, dy = pi.y - pj[u].y, dz = pi.z - pj[u].z;
                     const double rj = 2.0 * hj[u];
-                    if (dx * dx + dy * dy + dz * dz > rj * rj * (1.0 - 1e-9)) full[jj[u]] = 1;
+                    if (dx * dx + dy * dy + dz * dz > rj * rj * (1.0 - 1e-9)) {
+                        full[jj[u]] = 1;
+                        *full_any = 1;
+                    }
                 }
             }
         }
@@ -353,16 +382,19 @@ struct NewtonArgs {
     int max_iter, last_round;
 };
 
-// Newton iteration of the particle of every active lane over its own
-// candidate row (entry k at row[k * gc], see group_search), FP32 or FP64
-// kernel sums with FP64 update and convergence test.  No warp collectives:
+// Newton iteration of the particle of every active lane, FP32 or FP64 kernel
+// sums with FP64 update and convergence test.  The first evaluation (at
+// h = pi.w) comes from the search (hs0); later ones, rare once h has settled
+// from step to step, gather the candidates again through the particle's slot
+// row (entry k at row[k * gc], see group_search) in the same order, so every
+// evaluation sums the same terms in the same order.  No warp collectives:
 // lanes run independent iteration counts.
 template <class R>
 __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArgs &B, int i,
-                                            const double4 &pi, const void *rowp, int gc) {
+                                            const double4 &pi, const int *row, int gc,
+                                            const HSums<R> &hs0) {
     typedef typename R4<R>::T V4;
-    typedef typename R2<R>::T P2;
-    const P2 *row = (const P2 *)rowp;
+    const V4 *p1 = (const V4 *)B.p1;
     const int craw = A.cnt[i];
     if (craw > A.K) {
         // more candidates inside 2 hc than the row holds: the sums would miss
@@ -383,7 +415,7 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
         return;
     }
     const int c = craw;
-    const double mi = (double)((const V4 *)B.p1)[i].w;
+    const double mi = (double)p1[i].w;
     const double cap = B.hc[i];
     const double cfac = 4.0 * SPH_PI / 3.0 * 8.0;
     double h = pi.w, lo = 0.0, hi = INFINITY;
@@ -393,26 +425,20 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
             need = true;
             break;
         }
-        const R inv_h = R(1.0 / h);
-        KSum<R> S, D;
-        for (int k = 0; k < c; k++) {
-            const P2 v = row[(size_t)k * gc];
-            const R q = v.x * inv_h;
-            if (q < R(2)) {
-                R w, dw;
-                if (q <= R(1)) {
-                    w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
-                    dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
-                } else {
-                    const R t = R(2) - q;
-                    w = R(0.25) * t * t * t;
-                    dw = R(1.5) * t * t * (R(1) - q);
-                }
-                S.add(v.y * w);
-                D.add(v.y * dw);
+        double Ssum, Dsum;
+        if (it == 1) {
+            Ssum = hs0.S.value();
+            Dsum = hs0.D.value();
+        } else {
+            HSums<R> hs;
+            hs.inv_h = R(1.0 / h);
+            for (int k = 0; k < c; k++) {
+                const int j = row[(size_t)k * gc];
+                hs.add(pair_r<R>(pi, A.p0[j]), (R)(double)p1[j].w);
             }
+            Ssum = hs.S.value();
+            Dsum = hs.D.value();
         }
-        const double Ssum = S.value(), Dsum = D.value();
         const double h3 = h * h * h;
         const double rho = SPH_SIG / h3 * Ssum;
         const double drho = -SPH_SIG / (h3 * h) * Dsum;
@@ -455,8 +481,9 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
 }
 
 // candidate search + Newton iteration for the flagged particles of each group
+// (latency-bound: 8 blocks per SM, 64 registers, measured faster than 95)
 template <class R>
-__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
     k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B) {
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -469,11 +496,11 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         const unsigned todo = __ballot_sync(FULL, act);
         if (!todo) continue;
         const double4 pi = A.p0[i];
-        group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
+        HSums<R> hs;
+        hs.inv_h = R(1.0 / pi.w);
+        group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i], &hs);
         // each lane reads back only the row entries it wrote itself
-        if (act)
-            newton_lane<R>(A, B, i, pi,
-                           (const typename R2<R>::T *)A.cdat + (size_t)s0 * A.K + lane, gc);
+        if (act) newton_lane<R>(A, B, i, pi, A.cidx + (size_t)s0 * A.K + lane, gc, hs);
         __syncwarp();
     }
 }
@@ -512,7 +539,6 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.K = ctx->cfg.max_ngb;
     A.rows = rows;
     A.cnt = cnt;
-    A.cdat = ctx->cand;
     A.cidx = ctx->cand_idx;
     A.ngb_cnt = ctx->ngb_cnt;
     A.hnb = ctx->st[ctx->cur][ST_HNB];
@@ -567,14 +593,15 @@ int launch_neighbours(sph_ctx *ctx) {
     if (ctx->cand_ok) {
         // lists from the candidate rows, then the tree search for the
         // particles whose rows cannot show that their list is complete
-        CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 1), s));
+        CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 2), s));
         SearchArgs C = search_args(ctx, ctx->ngb, ctx->cand_cnt);
         k_lists_cand<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, C, ctx->hcand, ctx->lflag,
-                                                       ctx->lflag + n);
+                                                       ctx->lflag + n, ctx->lflag + n + 1);
         A.only = ctx->lflag;
         A.only_all = ctx->lflag + n;
     }
-    int rc = launch_refit_hmax(ctx);
+    // node h_max only matters to the tree search: skipped when no list needs it
+    int rc = launch_refit_hmax(ctx, ctx->cand_ok ? ctx->lflag + n + 1 : nullptr);
     if (rc) return rc;
     k_lists<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A);
     ctx->lists_ok = true;

@@ -95,10 +95,9 @@ struct sph_ctx {
 
     // neighbours
     int *ngb = nullptr, *ngb_cnt = nullptr;
-    void *cand = nullptr;  // (r_ij, m_j) Real pairs, max_ngb per particle
-    int *cand_idx = nullptr;  // candidate slots j, same layout as cand
+    int *cand_idx = nullptr;  // candidate slots j of the h iteration, max_ngb per particle
     int *cand_cnt = nullptr;
-    int *lflag = nullptr;     // n+1: per particle "needs the tree search", then "all do"
+    int *lflag = nullptr;     // n+2: per particle "needs the tree search", "all do", "any does"
     bool cand_ok = false;     // candidate rows match the current order, positions and h
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
     double *hcand = nullptr;     // candidate radius / 2 used per particle
@@ -240,7 +239,7 @@ int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
 int launch_groups(sph_ctx *ctx);
 int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 int launch_tree(sph_ctx *ctx);
-int launch_refit_hmax(sph_ctx *ctx);
+int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);
 int launch_neighbours(sph_ctx *ctx);
 int launch_density(sph_ctx *ctx);

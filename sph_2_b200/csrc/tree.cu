@@ -177,19 +177,20 @@ __global__ void k_bottom_up(int n, const int *__restrict__ parent, const int *__
 }
 
 // h_max refit after the smoothing lengths changed
+// need (may be null): skip the refit when *need == 0 (no tree search follows)
 __global__ void k_refit_leaves(int n, const double *__restrict__ h, double *hmax, double4 *sA,
-                               int *flag) {
+                               int *flag, const int *__restrict__ need) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    if (p >= n || (need && !*need)) return;
     hmax[n - 1 + p] = h[p];
     sA[n - 1 + p].w = h[p];
     if (p < n - 1) flag[p] = 0;
 }
 
 __global__ void k_refit_up(int n, const int *__restrict__ parent, const int *__restrict__ child,
-                           double *hmax, double4 *sA, int *flag) {
+                           double *hmax, double4 *sA, int *flag, const int *__restrict__ need) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n || n < 2) return;
+    if (p >= n || n < 2 || (need && !*need)) return;
     int nd = parent[n - 1 + p];
     while (nd >= 0) {
         __threadfence();
@@ -244,14 +245,14 @@ int launch_tree(sph_ctx *ctx) {
     return ctx_check_launch(ctx, "tree");
 }
 
-int launch_refit_hmax(sph_ctx *ctx) {
+int launch_refit_hmax(sph_ctx *ctx, const int *need) {
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     double4 *boxA = (double4 *)ctx->node_box;
     k_refit_leaves<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[ctx->cur][ST_H], ctx->hmax, boxA,
-                                                  ctx->flag);
+                                                  ctx->flag, need);
     k_refit_up<<<div_up(n, 256), 256, 0, s>>>(n, ctx->parent, ctx->child, ctx->hmax, boxA,
-                                              ctx->flag);
+                                              ctx->flag, need);
     return ctx_check_launch(ctx, "refit");
 }
