@@ -506,7 +506,7 @@ def extra_workload(a, world, rank, local):
         d = ic.cooling_cloud(n, seed=42)
         res = {}
         for mode in ("exact", "mlp"):
-            flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0)
+            flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
             ctx = Context(Config(n_max=n, precision="mixed", theta=a.theta, leaf_size=a.leaf,
                                  flags=flags))
             ctx.set_stream(stream.cuda_stream)
@@ -518,7 +518,10 @@ def extra_workload(a, world, rank, local):
             ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
             ctx.prologue()
             ms = timed(ctx, a.steps, a.warmup)
+            ph = ctx.phase_times()
             res[mode] = {"value": n * a.steps / (ms * 1e-3), "ms_per_step": ms / a.steps,
+                         "cooling_phase_ms": ph["update_dt"],
+                         "cooling_phase": "u update + cooling solve + dt commit of the last step",
                          "status": ctx.status()}
             ctx.close()
         out.update(value=res["mlp"]["value"], ms_per_step=res["mlp"]["ms_per_step"],

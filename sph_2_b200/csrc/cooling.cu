@@ -2,6 +2,10 @@
 //
 // The solver itself is in cooling.cuh.  The reference's table path
 // (hcoolingx, hfvCLibs_v7_hfv_v2.h:1240-1418) is replaced by this solve.
+#include <math.h>
+
+#include <vector>
+
 #include "cooling.cuh"
 
 __global__ void k_cool_arrays(CoolDev c, int n, const double *__restrict__ rho,
@@ -60,13 +64,21 @@ int sph_cooling_setup(sph_ctx *ctx, const sph_cooling_params *p, const double *l
     cudaSetDevice(ctx->device);
     if (!ctx->cool_table) {
         void *q = nullptr;
-        CK(cudaMalloc(&q, sizeof(double) * 4097));
+        CK(cudaMalloc(&q, sizeof(double) * 2 * 4097));
         ctx->allocs.push_back(q);
-        ctx->dev_bytes += sizeof(double) * 4097;
+        ctx->dev_bytes += sizeof(double) * 2 * 4097;
         ctx->cool_table = (double *)q;
     }
     CK(cudaMemcpy(ctx->cool_table, log_lambda, sizeof(double) * (p->n_bins + 1),
                   cudaMemcpyHostToDevice));
+    {
+        // Lambda(T_e) / T_e at the bin edges, for the surrogate's monotonicity test
+        const double dl = (p->logT1 - p->logT0) / p->n_bins;
+        std::vector<double> lamT(p->n_bins + 1);
+        for (int e = 0; e <= p->n_bins; e++) lamT[e] = pow(10.0, log_lambda[e] - (p->logT0 + e * dl));
+        CK(cudaMemcpy(ctx->cool_table + 4097, lamT.data(), sizeof(double) * (p->n_bins + 1),
+                      cudaMemcpyHostToDevice));
+    }
     ctx->cool = *p;
     ctx->cool_ok = true;
     return SPH_OK;

@@ -16,6 +16,7 @@
 
 struct CoolDev {
     const double *logL;
+    const double *lamT;  // Lambda(T_e) / T_e at the bin edges T_e (host-computed)
     int nb;
     double logT0, logT1, mu, gamma, XH, gheat, tol;
     int max_iter;
@@ -108,34 +109,37 @@ __device__ __forceinline__ void cool_newton_polish(const CoolDev &c, double rho,
 }
 
 // True when r(u) = u - u_old - ratefact*net(u)*dt is strictly increasing on
-// [u_lo, u_hi]: r'(u) = 1 + ratefact*dt*s*Lambda(T)/u with Lambda/u a power
-// law inside each table bin, so checking r' > 0 at the interval's ends and at
-// every bin edge inside it checks the whole interval.  A monotone r has one
-// root there, the one the bracket-and-bisect solve reaches from u_old.
+// [u_lo, u_hi]: r'(u) = 1 + ratefact*dt*s*Lambda(T)/u.  Inside a table bin
+// Lambda ~ T^s, so Lambda/u ~ T^(s-1): r' > 1 where s >= 0, and where s < 0 r'
+// grows with T, so its smallest value in a bin is at the bin's lower end.  The
+// interval is monotone iff r' > 0 at T(u_lo) (when its bin has s < 0) and at
+// the lower edge of every bin with s < 0 that starts inside the interval;
+// Lambda/T at the edges is tabulated, so only T(u_lo) needs a transcendental.
 __device__ __forceinline__ bool cool_monotone(const CoolDev &c, double rho, double dt, double u_lo,
                                               double u_hi) {
     const double nH = c.XH * rho / MH_CGS;
-    const double ratefact = nH * nH / rho;
+    const double A = nH * nH / rho * dt;
     const double kT = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS;
     const double dl = (c.logT1 - c.logT0) / c.nb;
-    auto rp_at = [&](double T, int side) {
-        // slope of the bin on the given side of an edge (side -1 below, +1 above)
-        const double lt = log10(T);
-        int k = (int)floor((lt - c.logT0) / dl + (side < 0 ? -1e-9 : 1e-9));
-        k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
-        const double s = (c.logL[k + 1] - c.logL[k]) / dl;
-        const double lam = exp10(c.logL[k] + s * (lt - (c.logT0 + k * dl)));
-        return 1.0 + ratefact * dt * s * lam / (T / kT);
-    };
     const double T0 = kT * u_lo, T1 = kT * u_hi;
-    if (!(rp_at(T0, +1) > 0.0) || !(rp_at(T1, -1) > 0.0)) return false;
+    if (!(T0 > 0.0) || !(T1 >= T0)) return false;
     const double l0 = log10(T0), l1 = log10(T1);
-    int k0 = (int)ceil((l0 - c.logT0) / dl), k1 = (int)floor((l1 - c.logT0) / dl);
-    k0 = k0 < 1 ? 1 : k0;
-    k1 = k1 > c.nb - 1 ? c.nb - 1 : k1;
-    for (int k = k0; k <= k1 && k - k0 < 4 * c.nb; k++) {
-        const double T = exp10(c.logT0 + k * dl);
-        if (!(rp_at(T, -1) > 0.0) || !(rp_at(T, +1) > 0.0)) return false;
+    int k = (int)floor((l0 - c.logT0) / dl);
+    k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
+    double s = (c.logL[k + 1] - c.logL[k]) / dl;
+    if (s < 0.0) {
+        const double lam = exp10(c.logL[k] + s * (l0 - (c.logT0 + k * dl)));
+        if (!(1.0 + A * s * lam * kT / T0 > 0.0)) return false;
+    }
+    // lower edges of the bins after T0's bin, up to T1 (edge k at logT0 + k dl;
+    // below bin 0 and above bin nb-1 the end slopes continue, no edges)
+    int kend = (int)floor((l1 - c.logT0) / dl);
+    kend = kend > c.nb - 1 ? c.nb - 1 : kend;
+    for (int e = k + 1; e <= kend; e++) {
+        s = (c.logL[e + 1] - c.logL[e]) / dl;
+        if (s < 0.0) {
+            if (!(1.0 + A * s * c.lamT[e] * kT > 0.0)) return false;
+        }
     }
     return true;
 }
@@ -152,6 +156,7 @@ static inline CoolDev cool_dev_of(const sph_ctx *ctx) {
     const sph_cooling_params &p = ctx->cool;
     CoolDev c;
     c.logL = ctx->cool_table;
+    c.lamT = ctx->cool_table + 4097;
     c.nb = p.n_bins;
     c.logT0 = p.logT0;
     c.logT1 = p.logT1;

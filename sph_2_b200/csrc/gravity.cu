@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
             const float2 px = f2(pi.x), py = f2(pi.y), pz = f2(pi.z), e2 = f2(eps2);
             const float2 m1 = f2(-1.f), c15 = f2(1.5f), cm75 = f2(-7.5f), c3 = f2(3.f);
             float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), spp = f2(0.f);
-#pragma unroll 2
+#pragma unroll 4
             for (int k = 0; k < m2; k += 2) {
                 const float2 dx = __ffma2_rn(ld2(&S.f[0][k]), m1, px);
                 const float2 dy = __ffma2_rn(ld2(&S.f[1][k]), m1, py);

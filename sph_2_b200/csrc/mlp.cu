@@ -56,6 +56,17 @@ __device__ __forceinline__ float gelu(float z) {
     const float k = 0.7978845608028654f;
     return 0.5f * z * (1.0f + tanhf(k * (z + 0.044715f * z * z * z)));
 }
+// the same with the hardware tanh approximation (tanh.approx.f32, relative
+// error about 2^-11, below the BF16 rounding of the activations it feeds):
+// used by the in-step inference only; training and the reference forward
+// keep tanhf
+__device__ __forceinline__ float gelu_fast(float z) {
+    const float k = 0.7978845608028654f;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(k * (z + 0.044715f * z * z * z)));
+    return 0.5f * z * (1.0f + t);
+}
+template <bool FAST> __device__ __forceinline__ float act(float z) { return FAST ? gelu_fast(z) : gelu(z); }
 __device__ __forceinline__ float gelu_grad(float z) {
     const float k = 0.7978845608028654f;
     const float t = tanhf(k * (z + 0.044715f * z * z * z));
@@ -81,6 +92,7 @@ __device__ __forceinline__ void load_weights(MlpSmem &S, const __nv_bfloat16 *pk
 
 // forward of one 16-row tile: ax = A fragment of X (16 x 16, 3 real columns);
 // z1, z2 pre-activations (C fragments), y for rows gid and gid+8
+template <bool FAST = false>
 __device__ __forceinline__ void tile_forward(const MlpSmem &S, const unsigned *ax, float z1[8][4],
                                              float z2[8][4], float &y0, float &y1) {
     const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
@@ -97,10 +109,10 @@ __device__ __forceinline__ void tile_forward(const MlpSmem &S, const unsigned *a
     unsigned a2[4][4];
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
-        a2[kk][0] = pack2(gelu(z1[2 * kk][0]), gelu(z1[2 * kk][1]));
-        a2[kk][1] = pack2(gelu(z1[2 * kk][2]), gelu(z1[2 * kk][3]));
-        a2[kk][2] = pack2(gelu(z1[2 * kk + 1][0]), gelu(z1[2 * kk + 1][1]));
-        a2[kk][3] = pack2(gelu(z1[2 * kk + 1][2]), gelu(z1[2 * kk + 1][3]));
+        a2[kk][0] = pack2(act<FAST>(z1[2 * kk][0]), act<FAST>(z1[2 * kk][1]));
+        a2[kk][1] = pack2(act<FAST>(z1[2 * kk][2]), act<FAST>(z1[2 * kk][3]));
+        a2[kk][2] = pack2(act<FAST>(z1[2 * kk + 1][0]), act<FAST>(z1[2 * kk + 1][1]));
+        a2[kk][3] = pack2(act<FAST>(z1[2 * kk + 1][2]), act<FAST>(z1[2 * kk + 1][3]));
     }
     float s0 = 0.f, s1 = 0.f;
 #pragma unroll
@@ -114,8 +126,8 @@ __device__ __forceinline__ void tile_forward(const MlpSmem &S, const unsigned *a
             const unsigned b[2] = {ld32(wb), ld32(wb + 8)};
             mma16816(z2[nt], a2[kk], b);
         }
-        s0 += gelu(z2[nt][0]) * S.w3[col] + gelu(z2[nt][1]) * S.w3[col + 1];
-        s1 += gelu(z2[nt][2]) * S.w3[col] + gelu(z2[nt][3]) * S.w3[col + 1];
+        s0 += act<FAST>(z2[nt][0]) * S.w3[col] + act<FAST>(z2[nt][1]) * S.w3[col + 1];
+        s1 += act<FAST>(z2[nt][2]) * S.w3[col] + act<FAST>(z2[nt][3]) * S.w3[col + 1];
     }
     s0 += __shfl_xor_sync(FULL, s0, 1);
     s0 += __shfl_xor_sync(FULL, s0, 2);
@@ -356,62 +368,105 @@ __global__ void k_adam(float *__restrict__ P, const float *__restrict__ g, float
     P[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
 }
 
-// In-step cooling with the surrogate: one warp per 16 particles.  Features are
-// staged through shared memory; rows whose estimated error exceeds err_tol
-// (or whose estimate is void) are solved exactly.
+// Surrogate prediction for the 32 rows of one warp (two 16-row MMA tiles):
+// features (log10 rho, log10 u, log10 dt) staged through shared memory, the
+// network's dlog10(u) returned for the lane's own row.
+__device__ __forceinline__ float predict32(const MlpSmem &S, __nv_bfloat16 *xs, float *ys,
+                                           const float *norm, bool own, double rho_c, double u0,
+                                           double dt_c) {
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    for (int e = lane; e < 512; e += 32) xs[e] = __float2bfloat16_rn(0.f);
+    __syncwarp();
+    if (own) {
+        // FP32 logarithms: the features are rounded to BF16 next
+        xs[lane * 16 + 0] = __float2bfloat16_rn((log10f((float)rho_c) - norm[0]) / norm[3]);
+        xs[lane * 16 + 1] = __float2bfloat16_rn((log10f((float)u0) - norm[1]) / norm[4]);
+        xs[lane * 16 + 2] = __float2bfloat16_rn((log10f((float)dt_c) - norm[2]) / norm[5]);
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int t = 0; t < 2; t++) {
+        unsigned ax[4];
+        x_fragment(xs + t * 256, ax);
+        float z1[8][4], z2[8][4], y0, y1;
+        tile_forward<true>(S, ax, z1, z2, y0, y1);
+        if (tig == 0) {
+            ys[t * 16 + gid] = y0;
+            ys[t * 16 + gid + 8] = y1;
+        }
+    }
+    __syncwarp();
+    const float y = ys[lane];
+    __syncwarp();
+    return y;
+}
+
+// Rows the surrogate does not answer go to a list (list[cap] counts them) that
+// k_cool_list solves exactly with full warps; a row that finds the list full
+// is solved in place.
+__device__ __forceinline__ bool to_list(int *list, int cap, int i) {
+    const int k = atomicAdd(&list[cap], 1);
+    if (k < cap) {
+        list[k] = i;
+        return true;
+    }
+    return false;
+}
+
+// In-step cooling with the surrogate: one warp per 32 particles.  Rows whose
+// estimated error exceeds err_tol (or whose estimate is void) are solved
+// exactly by k_cool_list.
 __global__ void __launch_bounds__(128)
     k_cool_mlp(CoolDev c, int n, const double *__restrict__ rho, double *__restrict__ u,
                const int *__restrict__ cloud, const double *__restrict__ dt, double ur, double uu,
                double ut, const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
-               double err_tol, long long *status) {
+               double err_tol, int *__restrict__ list, int cap, long long *status) {
     __shared__ MlpSmem S;
-    __shared__ __align__(16) __nv_bfloat16 xs[4][16 * 16];
-    __shared__ float ys[4][16];
+    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * 16];
+    __shared__ float ys[4][32];
     load_weights(S, pk, P);
     const float *norm = P + NP;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const int ntile = (n + 15) / 16;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntile = (n + 31) / 32;
     for (int tile = blockIdx.x * 4 + w; tile < ntile; tile += gridDim.x * 4) {
-        const int r0 = tile * 16;
-        const int i = r0 + (lane & 15);
-        const bool own = lane < 16 && i < n;
-        double rho_c = 0.0, u0 = 0.0, dt_c = 0.0;
+        const int i = tile * 32 + lane;
+        const bool own = i < n;
+        double rho_c = 1.0, u0 = 1.0, dt_c = 1.0;
         if (own) {
             rho_c = rho[i] * ur;
             u0 = u[i] * uu;
             dt_c = dt[cloud[i]] * ut;
         }
-        for (int e = lane; e < 256; e += 32) xs[w][e] = __float2bfloat16_rn(0.f);
-        __syncwarp();
+        const float y = predict32(S, xs[w], ys[w], norm, own, rho_c, u0, dt_c);
         if (own) {
-            const float f0 = ((float)log10(rho_c) - norm[0]) / norm[3];
-            const float f1 = ((float)log10(u0) - norm[1]) / norm[4];
-            const float f2 = ((float)log10(dt_c) - norm[2]) / norm[5];
-            xs[w][(lane & 15) * 16 + 0] = __float2bfloat16_rn(f0);
-            xs[w][(lane & 15) * 16 + 1] = __float2bfloat16_rn(f1);
-            xs[w][(lane & 15) * 16 + 2] = __float2bfloat16_rn(f2);
-        }
-        __syncwarp();
-        unsigned ax[4];
-        x_fragment(xs[w], ax);
-        float z1[8][4], z2[8][4], y0, y1;
-        tile_forward(S, ax, z1, z2, y0, y1);
-        if (tig == 0) {
-            ys[w][gid] = y0;
-            ys[w][gid + 8] = y1;
-        }
-        __syncwarp();
-        if (own) {
-            const double dl = (double)ys[w][lane & 15] * norm[7] + norm[6];
+            const double dl = (double)y * norm[7] + norm[6];
             double un = u0 * exp10(dl), est;
             cool_newton_polish(c, rho_c, u0, dt_c, &un, &est);
-            if (!cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+            if (cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+                u[i] = un / uu;
+            } else {
                 status_add(status, SPH_S_MLP_FALLBACK, 1);
-                if (cool_solve(c, rho_c, u0, dt_c, &un) < 0) status_add(status, SPH_S_COOL_NOCONV, 1);
+                if (!to_list(list, cap, i)) {
+                    if (cool_solve(c, rho_c, u0, dt_c, &un) < 0) status_add(status, SPH_S_COOL_NOCONV, 1);
+                    u[i] = un / uu;
+                }
             }
-            u[i] = un / uu;
         }
-        __syncwarp();
+    }
+}
+
+// exact solves of the listed in-step rows (u still holds u_old there)
+__global__ void k_cool_list(CoolDev c, const int *__restrict__ list, int cap,
+                            const double *__restrict__ rho, double *__restrict__ u,
+                            const int *__restrict__ cloud, const double *__restrict__ dt, double ur,
+                            double uu, double ut, long long *status) {
+    const int cnt = min(list[cap], cap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const int i = list[k];
+        double un;
+        if (cool_solve(c, rho[i] * ur, u[i] * uu, dt[cloud[i]] * ut, &un) < 0)
+            status_add(status, SPH_S_COOL_NOCONV, 1);
+        u[i] = un / uu;
     }
 }
 
@@ -421,52 +476,52 @@ __global__ void __launch_bounds__(128)
                       const double *__restrict__ u_old, const double *__restrict__ dtv,
                       double *__restrict__ u_new, int *__restrict__ fell_back,
                       const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
-                      double err_tol) {
+                      double err_tol, int *__restrict__ list, int cap) {
     __shared__ MlpSmem S;
-    __shared__ __align__(16) __nv_bfloat16 xs[4][16 * 16];
-    __shared__ float ys[4][16];
+    __shared__ __align__(16) __nv_bfloat16 xs[4][32 * 16];
+    __shared__ float ys[4][32];
     load_weights(S, pk, P);
     const float *norm = P + NP;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const int ntile = (n + 15) / 16;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntile = (n + 31) / 32;
     for (int tile = blockIdx.x * 4 + w; tile < ntile; tile += gridDim.x * 4) {
-        const int r0 = tile * 16;
-        const int i = r0 + (lane & 15);
-        const bool own = lane < 16 && i < n;
-        for (int e = lane; e < 256; e += 32) xs[w][e] = __float2bfloat16_rn(0.f);
-        __syncwarp();
+        const int i = tile * 32 + lane;
+        const bool own = i < n;
+        const double r = own ? rho[i] : 1.0, u0 = own ? u_old[i] : 1.0, d = own ? dtv[i] : 1.0;
+        const float y = predict32(S, xs[w], ys[w], norm, own, r, u0, d);
         if (own) {
-            xs[w][(lane & 15) * 16 + 0] = __float2bfloat16_rn(((float)log10(rho[i]) - norm[0]) / norm[3]);
-            xs[w][(lane & 15) * 16 + 1] = __float2bfloat16_rn(((float)log10(u_old[i]) - norm[1]) / norm[4]);
-            xs[w][(lane & 15) * 16 + 2] = __float2bfloat16_rn(((float)log10(dtv[i]) - norm[2]) / norm[5]);
-        }
-        __syncwarp();
-        unsigned ax[4];
-        x_fragment(xs[w], ax);
-        float z1[8][4], z2[8][4], y0, y1;
-        tile_forward(S, ax, z1, z2, y0, y1);
-        if (tig == 0) {
-            ys[w][gid] = y0;
-            ys[w][gid + 8] = y1;
-        }
-        __syncwarp();
-        if (own) {
-            const double dl = (double)ys[w][lane & 15] * norm[7] + norm[6];
-            double un = u_old[i] * exp10(dl), est;
-            cool_newton_polish(c, rho[i], u_old[i], dtv[i], &un, &est);
+            const double dl = (double)y * norm[7] + norm[6];
+            double un = u0 * exp10(dl), est;
+            cool_newton_polish(c, r, u0, d, &un, &est);
             int fb = 0;
-            if (!cool_accept(c, rho[i], u_old[i], dtv[i], un, est, err_tol)) {
+            if (cool_accept(c, r, u0, d, un, est, err_tol)) {
+                u_new[i] = un;
+            } else {
                 fb = 1;
-                cool_solve(c, rho[i], u_old[i], dtv[i], &un);
+                if (!to_list(list, cap, i)) {
+                    cool_solve(c, r, u0, d, &un);
+                    u_new[i] = un;
+                }
             }
-            u_new[i] = un;
             if (fell_back) fell_back[i] = fb;
         }
-        __syncwarp();
+    }
+}
+
+__global__ void k_cool_list_arrays(CoolDev c, const int *__restrict__ list, int cap,
+                                   const double *__restrict__ rho, const double *__restrict__ u_old,
+                                   const double *__restrict__ dtv, double *__restrict__ u_new) {
+    const int cnt = min(list[cap], cap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const int i = list[k];
+        double un;
+        cool_solve(c, rho[i], u_old[i], dtv[i], &un);
+        u_new[i] = un;
     }
 }
 
 int grid_for(sph_ctx *ctx, int n) { return max(1, min(div_up(div_up(n, 16), 4), ctx->num_sms * 8)); }
+int grid32_for(sph_ctx *ctx, int n) { return max(1, min(div_up(div_up(n, 32), 4), ctx->num_sms * 8)); }
 
 int ensure_mlp(sph_ctx *ctx) {
     if (ctx->mlp) return SPH_OK;
@@ -474,6 +529,14 @@ int ensure_mlp(sph_ctx *ctx) {
     const size_t bytes = sizeof(float) * (NP + 8) + sizeof(float) * NP * 3 + sizeof(float) * 8 +
                          sizeof(__nv_bfloat16) * PK_N;
     CK(cudaMalloc(&q, bytes));
+    {
+        // fallback rows of the surrogate (n_max entries + a counter)
+        void *l = nullptr;
+        CK(cudaMalloc(&l, sizeof(int) * ((size_t)ctx->cfg.n_max + 1)));
+        ctx->allocs.push_back(l);
+        ctx->dev_bytes += sizeof(int) * ((size_t)ctx->cfg.n_max + 1);
+        ctx->cool_list = (int *)l;
+    }
     CK(cudaMemset(q, 0, bytes));
     ctx->allocs.push_back(q);
     ctx->dev_bytes += bytes;
@@ -558,10 +621,16 @@ int launch_cooling_mlp(sph_ctx *ctx) {
     if (!ctx->cool_ok || !ctx->mlp_ok) return SPH_ERR_STATE;
     const int n = ctx->n, c = ctx->cur;
     if (n <= 0) return SPH_OK;
-    k_cool_mlp<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+    const int cap = ctx->cfg.n_max;
+    CK(cudaMemsetAsync(ctx->cool_list + cap, 0, sizeof(int), ctx->stream));
+    k_cool_mlp<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
         cool_dev_of(ctx), n, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
         ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t,
-        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->status);
+        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list, cap,
+        ctx->status);
+    k_cool_list<<<ctx->num_sms * 4, 128, 0, ctx->stream>>>(
+        cool_dev_of(ctx), ctx->cool_list, cap, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
+        ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t, ctx->status);
     return ctx_check_launch(ctx, "cooling_mlp");
 }
 
@@ -663,9 +732,13 @@ int sph_cool_solve_mlp(sph_ctx *ctx, int32_t n, const double *rho, const double 
     if (!ctx->cool_ok || !ctx->mlp_ok) return SPH_ERR_STATE;
     if (n == 0) return SPH_OK;
     cudaSetDevice(ctx->device);
-    k_cool_mlp_arrays<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+    const int cap = ctx->cfg.n_max;
+    CK(cudaMemsetAsync(ctx->cool_list + cap, 0, sizeof(int), ctx->stream));
+    k_cool_mlp_arrays<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
         cool_dev_of(ctx), n, rho, u_old, dt, u_new, fell_back,
-        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol);
+        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list, cap);
+    k_cool_list_arrays<<<ctx->num_sms * 4, 128, 0, ctx->stream>>>(cool_dev_of(ctx), ctx->cool_list,
+                                                                 cap, rho, u_old, dt, u_new);
     return ctx_check_launch(ctx, "cool_solve_mlp");
 }
 

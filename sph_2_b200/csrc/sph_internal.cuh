@@ -119,6 +119,7 @@ struct sph_ctx {
     void *mlp_bf16 = nullptr;      // packed BF16 weights for the tensor-core kernels
     float *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr;
     float *mlp_scratch = nullptr;
+    int *cool_list = nullptr;      // surrogate fallback rows (n_max) + their count
     int mlp_step = 0;
     bool mlp_ok = false;
 

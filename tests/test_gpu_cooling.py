@@ -98,3 +98,62 @@ def test_training_and_surrogate_within_tolerance():
     assert err.max() < 10 * p["mlp_err_tol"]
     c.close()
     print(f"surrogate rows {acc.mean():.3f}, exact {t1 - t0:.3f}s, surrogate {t2 - t1:.3f}s")
+
+
+def test_surrogate_gain_over_exact_solve():
+    """What the trained network buys: the cooling solve of 2^20 unseen states
+    through the surrogate path (prediction, one Newton step, acceptance test,
+    exact fallback for the rows it does not answer) against the exact
+    bracket-and-bisect solve of the same states, both on the device, both
+    timed with CUDA events on the library's stream."""
+    import ctypes as C
+
+    import torch
+
+    from sph_2_b200 import _lib as L
+
+    n = 1 << 20
+    c = Context(Config(n_max=n, precision="mixed"))
+    p = cooling.setup(c)
+    Xn, yn, norm, _ = cooling.training_set(c, n=200_000, seed=11)
+    c.mlp_set(cooling.init_params(seed=0), norm)
+    cooling.train(c, Xn, yn, steps=3000, batch=4096, lr=2e-3)
+    rho, u, dt = cooling.sample_states(n, seed=99)
+    s = torch.cuda.Stream()
+    c.set_stream(s.cuda_stream)
+    dv = [torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda") for a in (rho, u, dt)]
+    ue, um = torch.empty_like(dv[1]), torch.empty_like(dv[1])
+    fb = torch.empty(n, dtype=torch.int32, device="cuda")
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    lib = L.load()
+    torch.cuda.synchronize()
+
+    def exact():
+        L.check(lib.sph_cool_solve(c.handle, n, ptr(dv[0]), ptr(dv[1]), ptr(dv[2]), ptr(ue), None, 0),
+                "sph_cool_solve", c.handle)
+
+    def surrogate():
+        L.check(lib.sph_cool_solve_mlp(c.handle, n, ptr(dv[0]), ptr(dv[1]), ptr(dv[2]), ptr(um),
+                                       ptr(fb)), "sph_cool_solve_mlp", c.handle)
+
+    def timed(fn, reps=3):
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_exact, t_mlp = timed(exact), timed(surrogate)
+    u_ex, u_ml, f = ue.cpu().numpy(), um.cpu().numpy(), fb.cpu().numpy()
+    err = np.abs(u_ml / u_ex - 1)
+    acc = f == 0
+    assert acc.mean() > 0.5
+    assert np.percentile(err[acc], 99.9) < p["mlp_err_tol"] + 2 * p["tol"]
+    assert err.max() < 10 * p["mlp_err_tol"]
+    print(f"cooling solve of {n} states: exact {t_exact:.3f} ms, surrogate {t_mlp:.3f} ms "
+          f"({t_exact / t_mlp:.2f}x), answered by the surrogate {acc.mean():.3f}")
+    assert t_mlp < t_exact
+    c.close()
