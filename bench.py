@@ -47,8 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--err-subset", type=int, default=10_000)
-    ap.add_argument("--workload", default="evrard", choices=["evrard", "ensemble", "cooling"],
-                    help="evrard: the headline line; ensemble / cooling: extra workloads")
+    ap.add_argument("--workload", default="evrard", choices=["evrard", "ensemble", "cooling", "large"],
+                    help="evrard: the headline line; ensemble / cooling / large: extra workloads")
     ap.add_argument("--clouds", type=int, default=64)
     ap.add_argument("--tune", action="store_true", help="run the autotuner before timing")
     return ap.parse_args()
@@ -179,6 +179,53 @@ def reference_arm(a, rank):
 
 
 # ------------------------------------------------------------------ ours ----
+# compulsory bytes per particle of each SPH-side phase (FP64 arrays; neighbour
+# j-data re-reads that hit L1/L2 are not counted), the figures the per-phase
+# roofline fractions use
+PHASE_BYTES = {"sort": 416, "smoothing_h": 312, "neighbours": 288, "density_divcurl": 344,
+               "forces": 392, "dudt": 392}
+
+
+def hbm_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def phase_roofline(ctx, n, stream, reps=3):
+    """Each phase run alone through the C ABI on the context's current state,
+    timed with CUDA events on its stream: ms per call, and for the SPH-side
+    phases the compulsory bytes per particle / time against the HBM peak (the
+    walk's FP32 figure is in the roofline object)."""
+    import torch
+    calls = [("sort", ctx.sort), ("tree", ctx.build_tree), ("smoothing_h", ctx.smoothing_h),
+             ("neighbours", ctx.neighbours), ("density_divcurl", lambda: (ctx.density(), ctx.divcurl())),
+             ("forces", ctx.forces), ("dudt", ctx.dudt), ("gravity", ctx.gravity)]
+    peak, src = hbm_peak_gbs()
+    out = {}
+    for name, fn in calls:
+        fn()
+        ctx.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        row = {"ms": ms}
+        if name in PHASE_BYTES:
+            gbs = PHASE_BYTES[name] * n / (ms * 1e-3) / 1e9
+            row.update(bytes_per_particle=PHASE_BYTES[name], achieved_gbs=gbs, frac_hbm=gbs / peak)
+        out[name] = row
+    out["peak_gbs"] = peak
+    out["peak_source"] = src
+    return out
+
+
 def rms_rel(a, b):
     num = np.sum((a - b) ** 2, axis=1)
     den = np.sum(b * b, axis=1) + 1e-300
@@ -301,6 +348,9 @@ def main():
         roofline["traffic_source"] = tr["source"]
     except (OSError, KeyError, ValueError):
         pass
+
+    # ---- each phase alone (the step overlaps the walk with the SPH passes) ----
+    phases_alone = phase_roofline(ctx, n, stream)
 
     # ---- accuracy at the common initial state (mixed vs FP64 oracle) ----
     err = {}
@@ -428,6 +478,7 @@ def main():
         "accel_err": err,
         "conservation_100_steps_n10k": conservation,
         "phases_ms": phases,
+        "phases_alone": phases_alone,
         "status": final_status,
         "device_gb": ctx.device_bytes() / 1e9,
     }
@@ -437,6 +488,64 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def large_evrard(a, stream, timed):
+    """Evrard collapse at N = 16M (default) in mixed precision with the learned
+    cooling path, beside the plain FP64 method with the exact solve on the same
+    GPU: throughput, device memory, per-phase times and roofline fractions,
+    and energy / momentum after the warm-up and timed steps of both."""
+    from sph_2_b200 import Config, Context, cooling, ic
+    from sph_2_b200 import _lib as L
+    n = a.n if a.n != 1_000_000 else 16_000_000
+    d = ic.evrard(n, seed=42)
+    # physical scale: a 100 cm^-3 mean-density sphere whose u = 0.05 is 1e6 K
+    # (mu = 1.22): the gas cools through the table's 1e5 K peak towards the
+    # 1e4 K cut-off while it falls in
+    kb, mh, gcgs, mu, gam = 1.380649e-16, 1.6726e-24, 6.674e-8, 1.22, 5.0 / 3.0
+    unit_u = kb * 1e6 / ((gam - 1.0) * mu * mh) / 0.05
+    rho_mean = 100.0 * mu * mh
+    R = (3.0 * unit_u / gcgs / (4.0 * np.pi * rho_mean)) ** 0.5
+    M = unit_u * R / gcgs
+    units = {"unit_rho": M / R ** 3, "unit_u": unit_u, "unit_t": (R ** 3 / (gcgs * M)) ** 0.5}
+    res = {}
+    for arm, prec, mlp in (("mixed_mlp", "mixed", True), ("fp64_exact", "fp64", False)):
+        flags = L.FLAG_COOLING | L.FLAG_TIMING | L.FLAG_POTENTIAL | (L.FLAG_COOLING_MLP if mlp else 0)
+        ctx = Context(Config(n_max=n, precision=prec, theta=a.theta, leaf_size=a.leaf,
+                             ngb_lanes=a.lanes, flags=flags))
+        ctx.set_stream(stream.cuda_stream)
+        cooling.setup(ctx, units)
+        if mlp:
+            Xn, yn, norm, _ = cooling.training_set(
+                ctx, n=5_000_000, seed=7,
+                ranges=dict(log_rho=(-23.0, -17.0), log_T=(1.5, 6.5), log_dt=(9.5, 13.5)))
+            ctx.mlp_set(cooling.init_params(seed=0), norm)
+            cooling.train(ctx, Xn, yn, steps=4000, batch=4096, lr=2e-3)
+        ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+        ctx.prologue()
+        e0 = ctx.energies()
+        ms = timed(ctx, a.steps, a.warmup)
+        e1 = ctx.energies()
+        row = {"value": n * a.steps / (ms * 1e-3), "ms_per_step": ms / a.steps,
+               "device_gb": ctx.device_bytes() / 1e9, "phases_ms": ctx.phase_times(),
+               "E_start": e0["KE"] + e0["U"] + e0["PE"], "E_end": e1["KE"] + e1["U"] + e1["PE"],
+               "p_end": float(np.linalg.norm([e1["px"], e1["py"], e1["pz"]])),
+               "status": ctx.status()}
+        if mlp:
+            row["phases_alone"] = phase_roofline(ctx, n, stream)
+        res[arm] = row
+        ctx.close()
+    mx, fp = res["mixed_mlp"], res["fp64_exact"]
+    return {"value": mx["value"], "ms_per_step": mx["ms_per_step"],
+            "config": {"workload": f"evrard_{n}_mixed_mlp_cooling", "n": n, "theta": a.theta,
+                       "units_cgs": units, "steps_advanced": a.warmup + a.steps},
+            "memory": {"device_gb_mixed": mx["device_gb"], "device_gb_fp64": fp["device_gb"],
+                       "neighbour_rows_gb": 4 * 256 * n / 1e9,
+                       "candidate_rows_gb": 4 * 256 * n / 1e9},
+            "mixed_over_fp64": mx["value"] / fp["value"],
+            "energy_vs_fp64": abs(mx["E_end"] - fp["E_end"]) / abs(fp["E_end"]),
+            "momentum_end": {"mixed": mx["p_end"], "fp64": fp["p_end"]},
+            "arms": res}
 
 
 def extra_workload(a, world, rank, local):
@@ -501,6 +610,8 @@ def extra_workload(a, world, rank, local):
                            "parallelism": f"clouds sharded over {world} ranks (LPT)",
                            "per_rank_particles": n},
                    status=ctx.status())
+    elif a.workload == "large":
+        out.update(large_evrard(a, stream, timed))
     else:
         n = a.n if a.n != 1_000_000 else 2_000_000
         d = ic.cooling_cloud(n, seed=42)

@@ -130,15 +130,23 @@ __global__ void k_kick_drift(int n, double *__restrict__ x, double *__restrict__
     z[i] += nz * d;
 }
 
+// u <- u + dt/2 (du/dt + du/dt_prev) (u_updater, hfvCLibs_v7_hfv_v2.h:921-931).
+// keep > 0: with cooling on, the cooled u can be far below the u that
+// du/dt_prev was computed from, and the trapezoid can then overshoot below
+// zero (negative pressure, NaN sound speed); there the step may at most halve
+// u, the limiter of Gadget-2's entropy update.  keep = 0 is the reference's
+// update unchanged.
 __global__ void k_update_u(int n, double *__restrict__ u, double *__restrict__ dudt_prev,
                            const double *__restrict__ dudt, const int *__restrict__ cloud,
-                           const double *__restrict__ dt, int first) {
+                           const double *__restrict__ dt, int first, double keep) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double d = dt[cloud[i]];
     const double du = dudt[i];
-    if (first) u[i] += du * d;
-    else u[i] = u[i] + 0.5 * d * (du + dudt_prev[i]);
+    const double u0 = u[i];
+    double un = first ? u0 + du * d : u0 + 0.5 * d * (du + dudt_prev[i]);
+    if (keep > 0.0 && un < keep * u0) un = keep * u0;
+    u[i] = un;
     dudt_prev[i] = du;
 }
 
@@ -226,7 +234,8 @@ int launch_update_u(sph_ctx *ctx, bool first) {
     if (n <= 0) return SPH_OK;
     k_update_u<<<div_up(n, 256), 256, 0, ctx->stream>>>(n, ctx->st[c][ST_U],
                                                         ctx->st[c][ST_DUDT_PREV], ctx->dudt,
-                                                        ctx->cloud[c], ctx->dt, first ? 1 : 0);
+                                                        ctx->cloud[c], ctx->dt, first ? 1 : 0,
+                                                        (ctx->cfg.flags & SPH_FLAG_COOLING) ? 0.5 : 0.0);
     return ctx_check_launch(ctx, "update_u");
 }
 

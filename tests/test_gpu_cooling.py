@@ -157,3 +157,30 @@ def test_surrogate_gain_over_exact_solve():
           f"({t_exact / t_mlp:.2f}x), answered by the surrogate {acc.mean():.3f}")
     assert t_mlp < t_exact
     c.close()
+
+
+def test_cooling_collapse_stays_positive():
+    """An Evrard sphere scaled so that u = 0.05 is 1e6 K at 100 H/cm^3 cools
+    by orders of magnitude in its first steps; the trapezoidal u update with
+    the pre-cooling du/dt would then overshoot below zero.  The cooled run
+    keeps u positive and every field finite."""
+    from sph_2_b200 import ic
+    n = 20_000
+    d = ic.evrard(n, seed=42)
+    kb, mh, gcgs, mu, gam = 1.380649e-16, 1.6726e-24, 6.674e-8, 1.22, 5.0 / 3.0
+    unit_u = kb * 1e6 / ((gam - 1.0) * mu * mh) / 0.05
+    R = (3.0 * unit_u / gcgs / (4.0 * np.pi * 100.0 * mu * mh)) ** 0.5
+    M = unit_u * R / gcgs
+    units = {"unit_rho": M / R ** 3, "unit_u": unit_u, "unit_t": (R ** 3 / (gcgs * M)) ** 0.5}
+    c = Context(Config(n_max=n, precision="mixed", theta=0.5, flags=2))   # cooling on
+    cooling.setup(c, units)
+    c.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+    c.prologue()
+    c.step(10)
+    c.sync()
+    u = c.get("u")
+    assert np.all(u > 0) and u.max() < 0.05
+    assert np.isfinite(c.get("x")).all() and np.isfinite(c.get("vx")).all()
+    st = c.status()
+    assert st["nonfinite"] == 0 and st["h_noconv"] == 0 and st["cool_noconv"] == 0
+    c.close()
