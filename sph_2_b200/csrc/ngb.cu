@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
 // rounding), j's list may miss i and j is marked for the tree search.  A row
 // that is not a complete candidate set (overflow, or h above the candidate
 // radius after the last round) sends every particle to the tree search.
-__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, 6)
     k_lists_cand(const int *__restrict__ ngroup_p, SearchArgs A, const double *__restrict__ hc,
                  int *__restrict__ full, int *__restrict__ full_all, int *__restrict__ full_any) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
