@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--theta", type=float, default=0.38)
+    ap.add_argument("--theta-local", type=float, default=0.13,
+                    help="mixed walk: far cells through group Taylor expansions (0: off)")
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=8)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
@@ -272,7 +274,8 @@ def main():
 
     def make(precision, flags=0, vel=None):
         cfg = Config(n_max=n, precision=precision, theta=a.theta, leaf_size=a.leaf,
-                     ngb_lanes=a.lanes, flags=flags)
+                     ngb_lanes=a.lanes, flags=flags,
+                     theta_local=a.theta_local if precision == "mixed" else 0.0)
         c = Context(cfg)
         c.set_stream(stream.cuda_stream)
         c.load(d["pos"], d["vel"] if vel is None else vel, d["m"], d["h"], d["u"])
@@ -329,7 +332,10 @@ def main():
     torch.cuda.synchronize()
     walk_ms = w0.elapsed_time(w1) / reps
     cnt = ctx.counters()
-    flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"]
+    # far cells: 150 flop each, once per group; 65 per particle to evaluate
+    # the expansion
+    flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"] + 150.0 * cnt["far_cells"] + \
+        (65.0 * n if cnt["far_cells"] else 0.0)
     fp32_peak = ctx.fp32_peak_tflops()
     achieved = flops / (walk_ms * 1e-3) / 1e12
     roofline = {"kernel": "k_walk<float> (gravity walk)", "bound": "fp32",
@@ -337,9 +343,12 @@ def main():
                 "frac": achieved / fp32_peak, "traffic": None,
                 "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json "
                                "has no FP32 figure)",
-                "algorithmic": "60 flop per quadrupole cell + 20 per particle interaction",
+                "algorithmic": ("60 flop per quadrupole cell + 20 per particle interaction "
+                                "+ 150 per far cell (once per group) + 65 per particle for "
+                                "the group expansion"),
                 "interactions_per_particle": {"cells": cnt["cells"] / n,
-                                              "particles": cnt["particles"] / n},
+                                              "particles": cnt["particles"] / n,
+                                              "far_cells_per_particle_equiv": cnt["far_cells"] / n},
                 "walk_ms": walk_ms}
     try:
         with open(os.path.join(ROOT, "profiles", "walk_traffic.json")) as f:
@@ -463,7 +472,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64 (mixed)",
         "data": "synthetic (seeded Evrard sphere, numpy default_rng)",
         "config": {"workload": "evrard_1M_mixed" if n == 1_000_000 else f"evrard_{n}_mixed",
-                   "n": n, "theta": a.theta, "leaf_size": a.leaf, "ngb_lanes": a.lanes,
+                   "n": n, "theta": a.theta, "theta_local_mixed": a.theta_local,
+                   "leaf_size": a.leaf, "ngb_lanes": a.lanes,
                    "n_ngb": 64, "eps": 1e-2, "av": "monaghan-gingold alpha=1 beta=2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "working set > L2 (neighbour rows ~0.3 GB + tree ~0.5 GB per step)",
@@ -512,7 +522,8 @@ def large_evrard(a, stream, timed):
     for arm, prec, mlp in (("mixed_mlp", "mixed", True), ("fp64_exact", "fp64", False)):
         flags = L.FLAG_COOLING | L.FLAG_TIMING | L.FLAG_POTENTIAL | (L.FLAG_COOLING_MLP if mlp else 0)
         ctx = Context(Config(n_max=n, precision=prec, theta=a.theta, leaf_size=a.leaf,
-                             ngb_lanes=a.lanes, flags=flags))
+                             ngb_lanes=a.lanes, flags=flags,
+                             theta_local=a.theta_local if prec == "mixed" else 0.0))
         ctx.set_stream(stream.cuda_stream)
         cooling.setup(ctx, units)
         if mlp:
@@ -595,7 +606,8 @@ def extra_workload(a, world, rank, local):
         mine = local_ensemble(e, owner, rank)
         n = len(mine["m"])
         ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
-                             theta=a.theta, leaf_size=a.leaf, ngb_lanes=a.lanes))
+                             theta=a.theta, leaf_size=a.leaf, ngb_lanes=a.lanes,
+                             theta_local=a.theta_local))
         ctx.set_stream(stream.cuda_stream)
         ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
         ctx.prologue()
@@ -619,6 +631,7 @@ def extra_workload(a, world, rank, local):
         for mode in ("exact", "mlp"):
             flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
             ctx = Context(Config(n_max=n, precision="mixed", theta=a.theta, leaf_size=a.leaf,
+                                 theta_local=a.theta_local,
                                  flags=flags))
             ctx.set_stream(stream.cuda_stream)
             cooling.setup(ctx, d["units"])

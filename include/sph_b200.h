@@ -121,6 +121,10 @@ typedef struct sph_config {
     double courant;       /* dt = courant * min(h/v_sig, sqrt(h/|a|))             */
     double dt_max;        /* upper bound on dt (0: none)                          */
     double dt_fixed;      /* >0: fixed step (reference drivers), no Courant dt    */
+    double theta_local;   /* mixed-precision walk: accepted cells farther than
+                             R_g / theta_local from a group's centre (R_g its
+                             radius) enter a second-order Taylor expansion at
+                             the centre, once per group; 0: off              */
 } sph_config;
 
 typedef struct sph_ctx sph_ctx;
@@ -244,6 +248,9 @@ int sph_cfl_dt(sph_ctx *ctx, double *dt);
 int sph_energies(sph_ctx *ctx, double *out10);
 /* interaction counters of the last gravity call: [cells, particles] */
 int sph_get_counters(sph_ctx *ctx, int64_t *out2);
+/* far cells of the last walk that went through the group local expansions
+ * (sph_config.theta_local), summed over groups (one per cell and group) */
+int sph_get_far_cells(sph_ctx *ctx, int64_t *out);
 
 /* ---- cooling (DoCooling, myPhotoLibsGPU.h:615-686; hcoolingx, hfvCLibs:1240) ---- */
 int sph_cooling_setup(sph_ctx *ctx, const sph_cooling_params *p, const double *log_lambda);

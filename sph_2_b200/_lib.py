@@ -48,7 +48,7 @@ class SphConfig(C.Structure):
         ("n_ngb", C.c_double), ("h_tol", C.c_double), ("gamma", C.c_double),
         ("alpha", C.c_double), ("beta", C.c_double), ("eta", C.c_double), ("G", C.c_double),
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),
-        ("dt_max", C.c_double), ("dt_fixed", C.c_double),
+        ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
     ]
 
 
@@ -105,6 +105,7 @@ SIGNATURES = [
     ("sph_update_u", C.c_int, [_P, _I]),
     ("sph_cfl_dt", C.c_int, [_P, _P]),
     ("sph_energies", C.c_int, [_P, _P]),
+    ("sph_get_far_cells", C.c_int, [_P, _P]),
     ("sph_get_counters", C.c_int, [_P, _P]),
     ("sph_cooling_setup", C.c_int, [_P, C.POINTER(SphCoolingParams), _P]),
     ("sph_cooling_exact", C.c_int, [_P]),

@@ -46,6 +46,7 @@ class Config:
     courant: float = 0.25
     dt_max: float = 0.0
     dt_fixed: float = 0.0
+    theta_local: float = 0.0
 
     def to_c(self) -> L.SphConfig:
         c = L.SphConfig()
@@ -294,7 +295,9 @@ class Context:
     def counters(self):
         out = np.zeros(2, np.int64)
         self._chk(self._L.sph_get_counters(self._h, _ptr(out)), "counters")
-        return {"cells": int(out[0]), "particles": int(out[1])}
+        far = np.zeros(1, np.int64)
+        self._chk(self._L.sph_get_far_cells(self._h, _ptr(far)), "far cells")
+        return {"cells": int(out[0]), "particles": int(out[1]), "far_cells": int(far[0])}
 
     def kick(self, fac=0.5):
         self._chk(self._L.sph_kick(self._h, fac), "sph_kick")

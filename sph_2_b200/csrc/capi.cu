@@ -83,6 +83,7 @@ int check_cfg(const sph_config *c) {
     if (c->walk_blocks < 0 || c->walk_blocks > 64) return SPH_ERR_ARG;
     if (c->h_max_iter < 1 || c->h_max_iter > 1000) return SPH_ERR_ARG;
     if (!(c->theta > 0.0 && c->theta <= 1.0)) return SPH_ERR_ARG;
+    if (!(c->theta_local >= 0.0 && c->theta_local < 1.0)) return SPH_ERR_ARG;
     if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
     if (!(c->courant > 0.0)) return SPH_ERR_ARG;
     return SPH_OK;
@@ -319,7 +320,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->retry, N); DAF(ctx->hcand, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
     DAF(ctx->status, SPH_NSTATUS);
-    DAF(ctx->counters, 2);
+    DAF(ctx->counters, 3);
     DAF(ctx->work, 16);
     DAF(ctx->red, std::max<size_t>(2 * N, 8192));
     if (cudaMemsetAsync(ctx->status, 0, SPH_NSTATUS * sizeof(long long), ctx->stream) ||
@@ -771,6 +772,17 @@ int sph_energies(sph_ctx *ctx, double *out10) {
     if (!out10) return SPH_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream_g));
     return launch_energies(ctx, out10);
+}
+
+int sph_get_far_cells(sph_ctx *ctx, int64_t *out) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaMemcpyAsync(out, ctx->counters + 2, sizeof(long long), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SPH_OK;
 }
 
 int sph_get_counters(sph_ctx *ctx, int64_t *out2) {

@@ -28,6 +28,10 @@
 namespace {
 
 constexpr int WALK_WARPS = 4;
+// coefficients of the group local expansion: field (3), its gradient J
+// (xx yy zz xy xz yz), the monopole's second derivatives H (xxx yyy zzz xxy
+// xxz yyx yyz zzx zzy xyz) and the potential
+constexpr int NLOC = 20;
 constexpr int WSTK = 1024;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -50,6 +54,11 @@ struct WalkSmemF {
     int plist[96];
     // cells: com x y z, -mass, Qxx Qyy Qzz Qxy Qxz Qyz, trace
     __align__(8) float f[11][32];
+    // far cells of the group's local expansion: their node ids, per-lane
+    // partial sums of the coefficients (one column per lane) and the totals
+    int flist[64];
+    float red[NLOC][32];
+    float ltot[NLOC];
 };
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -82,6 +91,72 @@ __device__ __forceinline__ float box_d2(float x0, float y0, float z0, float x1, 
     return tx * tx + ty * ty + tz * tz;
 }
 
+// Local (Taylor) coefficients at the group centre x0 of one far cell (com c,
+// mass M, second moments Q about c, trace tr), r = x0 - c, Plummer-softened:
+// the monopole + quadrupole field and its gradient J_ij = d a_i / d r_j, the
+// monopole's second derivatives H_ijk, and the potential.  With
+// g_n = (r^2 + eps^2)^(-n/2):
+//   a   = (-M g3 + 1.5 tr g5 - 7.5 (r.Q.r) g7) r + 3 g5 Q.r
+//   J   = delta (A - M g3) + r r^T (B + 3 M g5) + 3 g5 Q - 15 g7 (r (Qr)^T + (Qr) r^T),
+//         A = 1.5 tr g5 - 7.5 (r.Q.r) g7,  B = -7.5 tr g7 + 52.5 (r.Q.r) g9
+//   H   = 3 M g5 (delta_ij r_k + delta_ik r_j + delta_jk r_i) - 15 M g7 r_i r_j r_k
+//   phi = -(M g1 + 0.5 (3 (r.Q.r) g5 - tr g3))
+__device__ __forceinline__ void far_coeffs(float rx, float ry, float rz, float eps2, float M,
+                                           float qxx, float qyy, float qzz, float qxy, float qxz,
+                                           float qyz, float tr, float *L) {
+    const float s2 = rx * rx + ry * ry + rz * rz + eps2;
+    const float g1 = rsqrtf(s2), gi2 = g1 * g1;
+    const float g3 = g1 * gi2, g5 = g3 * gi2, g7 = g5 * gi2, g9 = g7 * gi2;
+    const float qx = qxx * rx + qxy * ry + qxz * rz;
+    const float qy = qxy * rx + qyy * ry + qyz * rz;
+    const float qz = qxz * rx + qyz * ry + qzz * rz;
+    const float dqd = rx * qx + ry * qy + rz * qz;
+    const float A = 1.5f * tr * g5 - 7.5f * dqd * g7;
+    const float sc = A - M * g3;
+    const float t5 = 3.f * g5;
+    L[0] = sc * rx + t5 * qx;
+    L[1] = sc * ry + t5 * qy;
+    L[2] = sc * rz + t5 * qz;
+    const float Bm = -7.5f * tr * g7 + 52.5f * dqd * g9 + 3.f * M * g5;
+    const float c15 = 15.f * g7;
+    L[3] = sc + rx * rx * Bm + t5 * qxx - 2.f * c15 * rx * qx;
+    L[4] = sc + ry * ry * Bm + t5 * qyy - 2.f * c15 * ry * qy;
+    L[5] = sc + rz * rz * Bm + t5 * qzz - 2.f * c15 * rz * qz;
+    L[6] = rx * ry * Bm + t5 * qxy - c15 * (rx * qy + ry * qx);
+    L[7] = rx * rz * Bm + t5 * qxz - c15 * (rx * qz + rz * qx);
+    L[8] = ry * rz * Bm + t5 * qyz - c15 * (ry * qz + rz * qy);
+    const float a3 = 3.f * M * g5, b7 = 15.f * M * g7;
+    const float ex = a3 - b7 * rx * rx, ey = a3 - b7 * ry * ry, ez = a3 - b7 * rz * rz;
+    L[9] = rx * (ex + 2.f * a3);   // xxx
+    L[10] = ry * (ey + 2.f * a3);  // yyy
+    L[11] = rz * (ez + 2.f * a3);  // zzz
+    L[12] = ry * ex;               // xxy
+    L[13] = rz * ex;               // xxz
+    L[14] = rx * ey;               // yyx
+    L[15] = rz * ey;               // yyz
+    L[16] = rx * ez;               // zzx
+    L[17] = ry * ez;               // zzy
+    L[18] = -b7 * rx * ry * rz;    // xyz
+    L[19] = -(M * g1 + 0.5f * (3.f * dqd * g5 - tr * g3));
+}
+
+// value of the local expansion at offset u from the group centre: the field
+// a0 + J u + H:uu/2 and the potential phi0 - a0.u - u.J.u/2
+__device__ __forceinline__ void far_eval(const float *L, float ux, float uy, float uz, float &ax,
+                                         float &ay, float &az, float &phi) {
+    const float jx = L[3] * ux + L[6] * uy + L[7] * uz;
+    const float jy = L[6] * ux + L[4] * uy + L[8] * uz;
+    const float jz = L[7] * ux + L[8] * uy + L[5] * uz;
+    const float xx = ux * ux, yy = uy * uy, zz = uz * uz, xy = ux * uy, xz = ux * uz, yz = uy * uz;
+    const float hx = L[9] * xx + L[14] * yy + L[16] * zz + 2.f * (L[12] * xy + L[13] * xz + L[18] * yz);
+    const float hy = L[12] * xx + L[10] * yy + L[17] * zz + 2.f * (L[14] * xy + L[18] * xz + L[15] * yz);
+    const float hz = L[13] * xx + L[15] * yy + L[11] * zz + 2.f * (L[18] * xy + L[16] * xz + L[17] * yz);
+    ax = L[0] + jx + 0.5f * hx;
+    ay = L[1] + jy + 0.5f * hy;
+    az = L[2] + jz + 0.5f * hz;
+    phi = L[19] - (L[0] * ux + L[1] * uy + L[2] * uz) - 0.5f * (ux * jx + uy * jy + uz * jz);
+}
+
 template <class R, bool POT>
 __global__ void __launch_bounds__(WALK_WARPS * 32)
     k_walk(const int *__restrict__ ngroup_p, const int *__restrict__ gstart, const int *__restrict__ gcount,
@@ -90,7 +165,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
            const typename R4<R>::T *__restrict__ wB, const typename R4<R>::T *__restrict__ wC,
            const int4 *__restrict__ wL, int leaf_size, R eps2, double G, int n,
            double *__restrict__ agrav, double *__restrict__ pot, unsigned *work,
-           unsigned long long *counters, long long *status) {
+           unsigned long long *counters, long long *status, float theta_local) {
     typedef typename R4<R>::T V4;
     constexpr bool PACKED = std::is_same<R, float>::value;
     typedef typename std::conditional<PACKED, WalkSmemF, WalkSmem<R>>::type SM;
@@ -113,10 +188,27 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         const R bx1 = wmax<R>(act ? pi.x : R(-INFINITY)), by1 = wmax<R>(act ? pi.y : R(-INFINITY)),
                 bz1 = wmax<R>(act ? pi.z : R(-INFINITY));
         KSum<R> ax, ay, az, ph;
-        long long nC = 0, nP = 0;
-        int sp = 1, nc = 0, np = 0;
+        long long nC = 0, nP = 0, nF = 0;
+        int sp = 1, nc = 0, np = 0, nfar = 0;
         bool overflow = false;
         if (lane == 0) S.stk[0] = croot[gcloud[g]];
+        // local expansion (FP32 walk, theta_local > 0): accepted cells whose
+        // com is at least R_g / theta_local from the group centre x0 (R_g the
+        // group's radius about x0) enter a Taylor expansion at x0 once per
+        // group instead of being evaluated for every particle
+        R fx0 = R(0), fy0 = R(0), fz0 = R(0), rfar2 = R(INFINITY);
+        if constexpr (PACKED) {
+            if (theta_local > 0.f) {
+                fx0 = 0.5f * (bx0 + bx1);
+                fy0 = 0.5f * (by0 + by1);
+                fz0 = 0.5f * (bz0 + bz1);
+                const float ux = pi.x - fx0, uy = pi.y - fy0, uz = pi.z - fz0;
+                const float rg2 = wmax<float>(act ? ux * ux + uy * uy + uz * uz : 0.f);
+                rfar2 = rg2 / (theta_local * theta_local);
+#pragma unroll
+                for (int q = 0; q < NLOC; q++) S.red[q][lane] = 0.f;
+            }
+        }
         __syncwarp();
 
         auto flush_cells = [&](int m) {
@@ -213,6 +305,23 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
             __syncwarp();
           }
         };
+        // far cells: one per lane, added into the lane's own column of
+        // partial coefficient sums (summed over the warp once per group)
+        auto flush_far = [&](int m) {
+          if constexpr (PACKED) {
+            if (lane < m) {
+                float Lc[NLOC];
+                const int nd = S.flist[lane];
+                const float4 a = wA[nd], b = wB[nd], c = wC[nd];
+                far_coeffs(fx0 - a.x, fy0 - a.y, fz0 - a.z, eps2, b.w, b.x, b.y, b.z, c.x, c.y, c.z,
+                           c.w, Lc);
+#pragma unroll
+                for (int q = 0; q < NLOC; q++) S.red[q][lane] += Lc[q];
+            }
+            nF += m;
+            __syncwarp();
+          }
+        };
         auto flush_parts = [&](int m) {
           if constexpr (PACKED) {
             const int m2 = (m + 1) & ~1;
@@ -274,7 +383,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                 const int take = min(sp, 32);
                 sp -= take;
                 int nd = 0, f = 0, cn = 0;
-                bool accept = false, open = false;
+                bool accept = false, open = false, far = false;
                 int cl = 0, cr = 0;
                 if (lane < take) {
                     nd = S.stk[sp + lane];
@@ -288,14 +397,35 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                     const R d2 = box_d2(bx0, by0, bz0, bx1, by1, bz1, a.x, a.y, a.z);
                     accept = d2 >= a.w && cn > 1;
                     open = !accept;
+                    if constexpr (PACKED) {
+                        if (accept && theta_local > 0.f) {
+                            const float dx = a.x - fx0, dy = a.y - fy0, dz = a.z - fz0;
+                            far = dx * dx + dy * dy + dz * dz >= rfar2;
+                        }
+                    }
                 }
                 __syncwarp();
                 const bool bucket = open && cn <= leaf_size;
                 const bool inner = open && cn > leaf_size;
-                // accepted cells
-                const unsigned am = __ballot_sync(FULL, accept);
-                if (accept) S.clist[nc + __popc(am & lt)] = nd;
+                // accepted cells: near ones to the per-particle list, far
+                // ones (local expansion) to the far list
+                const unsigned am = __ballot_sync(FULL, accept && !far);
+                if (accept && !far) S.clist[nc + __popc(am & lt)] = nd;
                 nc += __popc(am);
+                if constexpr (PACKED) {
+                    const unsigned fm = __ballot_sync(FULL, far);
+                    if (far) S.flist[nfar + __popc(fm & lt)] = nd;
+                    nfar += __popc(fm);
+                    __syncwarp();
+                    if (nfar >= 32) {
+                        flush_far(32);
+                        const int v = S.flist[32 + lane];
+                        __syncwarp();
+                        if (lane + 32 < nfar) S.flist[lane] = v;
+                        nfar -= 32;
+                        __syncwarp();
+                    }
+                }
                 // children of opened inner nodes
                 const unsigned im = __ballot_sync(FULL, inner);
                 const int npush = 2 * __popc(im);
@@ -342,6 +472,27 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
             if (sp == 0) {
                 if (nc > 0) { flush_cells(nc); nc = 0; }
                 if (np > 0) { flush_parts(np); np = 0; }
+                if (nfar > 0) { flush_far(nfar); nfar = 0; }
+            }
+        }
+        if constexpr (PACKED) {
+            if (nF > 0) {
+                __syncwarp();
+                if (lane < NLOC) {  // Kahan sum of the 32 lane columns
+                    KSum<float> t;
+                    for (int k = 0; k < 32; k++) t.add(S.red[lane][k]);
+                    S.ltot[lane] = (float)t.value();
+                }
+                __syncwarp();
+                float Lt[NLOC];
+#pragma unroll
+                for (int q = 0; q < NLOC; q++) Lt[q] = S.ltot[q];
+                float fax, fay, faz, fph;
+                far_eval(Lt, pi.x - fx0, pi.y - fy0, pi.z - fz0, fax, fay, faz, fph);
+                ax.add(fax);
+                ay.add(fay);
+                az.add(faz);
+                if (POT) ph.add(fph);
             }
         }
         if (act) {
@@ -354,6 +505,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         if (lane == 0) {
             atomicAdd(&counters[0], (unsigned long long)(nC * gc));
             atomicAdd(&counters[1], (unsigned long long)(nP * gc));
+            atomicAdd(&counters[2], (unsigned long long)nF);
             if (overflow) status_add(status, SPH_S_STACK_OVERFLOW, 1);
         }
     }
@@ -472,7 +624,7 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
         (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
         (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->wL,
         ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
-        ctx->work, ctx->counters, ctx->status);
+        ctx->work, ctx->counters, ctx->status, (float)ctx->cfg.theta_local);
     return SPH_OK;
 }
 
@@ -480,7 +632,7 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
 
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot) {
     if (ctx->n <= 0) return SPH_OK;
-    CK(cudaMemsetAsync(ctx->counters, 0, 2 * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(unsigned long long), s));
     int rc;
     if (ctx->cfg.precision == SPH_PREC_MIXED)
         rc = pot ? run_walk<float, true>(ctx, s) : run_walk<float, false>(ctx, s);

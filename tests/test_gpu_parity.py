@@ -300,6 +300,28 @@ def test_gravity_walk_mixed_vs_direct(theta, bound):
     assert rms_rel(a, ad) < bound
 
 
+@pytest.mark.parametrize("theta,theta_local,bound", [(0.38, 0.13, 1.6e-4), (0.5, 0.2, 5e-4)])
+def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
+    """Far cells through the groups' Taylor expansions: the error against the
+    FP64 direct sum stays within a small margin of the plain walk's, while
+    the per-particle cell count drops and far cells are counted."""
+    n = 40000
+    ctx, d = prepared(n, "mixed", theta=theta)
+    ctx.gravity()
+    plain = ctx.counters()
+    tg = np.random.default_rng(0).choice(n, 2000, replace=False).astype(np.int32)
+    ad, _ = ctx.gravity_direct(tg)
+    e_plain = rms_rel(ctx.get_acc("grav", True)[tg], ad)
+    ctx2, _ = prepared(n, "mixed", theta=theta, theta_local=theta_local)
+    ctx2.gravity()
+    loc = ctx2.counters()
+    e_loc = rms_rel(ctx2.get_acc("grav", True)[tg], ad)
+    assert loc["far_cells"] > 0 and loc["cells"] < plain["cells"]
+    assert loc["particles"] == plain["particles"]
+    assert e_loc < bound and e_loc < 1.3 * e_plain
+    assert plain["far_cells"] == 0
+
+
 # ------------------------------------------------- status / fault paths ----
 def test_status_counters_without_faults():
     # iteration cap of 1: the h iteration reports non-convergence, no fault
