@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--theta-local", type=float, default=0.13,
                     help="mixed walk: far cells through group Taylor expansions (0: off)")
     ap.add_argument("--leaf", type=int, default=8)
-    ap.add_argument("--lanes", type=int, default=8)
+    ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")

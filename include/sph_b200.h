@@ -106,8 +106,9 @@ typedef struct sph_config {
     int32_t av_mode;      /* SPH_AV_*                                             */
     int32_t balsara;      /* 1: multiply the viscosity by the Balsara factor      */
     int32_t leaf_size;    /* tree bucket size, 1..64                              */
-    int32_t ngb_lanes;    /* lanes per particle in neighbour sums: 4, 8, 16, 32   */
-    int32_t block_size;   /* threads per block of the neighbour-sum passes        */
+    int32_t ngb_lanes;    /* lanes per particle in neighbour sums: 1, 2, 4, 8, 16, 32 */
+    int32_t block_size;   /* threads per block of the neighbour-sum passes: 64..256,
+                             a multiple of 32                                   */
     int32_t max_ngb;      /* neighbour-list row capacity                          */
     int32_t h_max_iter;   /* Newton iteration cap                                 */
     int32_t flags;        /* SPH_FLAG_*                                           */

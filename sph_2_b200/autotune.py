@@ -12,7 +12,7 @@ import itertools
 import time
 
 
-def tune(ctx, lanes=(4, 8, 16), blocks=(128, 256), leaves=(8, 12, 16), steps=2, warmup=1):
+def tune(ctx, lanes=(2, 4, 8), blocks=(128, 256), leaves=(6, 8, 12), steps=2, warmup=1):
     base = {k: getattr(ctx.config, k) for k in ("ngb_lanes", "block_size", "leaf_size")}
     results = []
     for nl, bs, lf in itertools.product(lanes, blocks, leaves):

@@ -28,8 +28,8 @@ class Config:
     av_mode: str = "mg83"
     balsara: bool = False
     leaf_size: int = 8
-    ngb_lanes: int = 8
-    block_size: int = 256
+    ngb_lanes: int = 4
+    block_size: int = 128
     max_ngb: int = 256
     h_max_iter: int = 64
     flags: int = 0

@@ -69,7 +69,7 @@ __global__ void k_gather_by_id(int n, const int *__restrict__ id, const double *
     if (s < n) dst[s] = src[id[s]];
 }
 
-bool valid_lanes(int l) { return l == 4 || l == 8 || l == 16 || l == 32; }
+bool valid_lanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32; }
 
 int check_cfg(const sph_config *c) {
     if (c->n_max < 1 || c->n_cloud_max < 1) return SPH_ERR_ARG;
@@ -78,7 +78,8 @@ int check_cfg(const sph_config *c) {
     if (c->av_mode != SPH_AV_MG83 && c->av_mode != SPH_AV_GADGET) return SPH_ERR_ARG;
     if (c->leaf_size < 1 || c->leaf_size > 64) return SPH_ERR_ARG;
     if (!valid_lanes(c->ngb_lanes)) return SPH_ERR_ARG;
-    if (c->block_size < 64 || c->block_size > 1024 || c->block_size % 32) return SPH_ERR_ARG;
+    // the neighbour-sum kernels are compiled for at most 256 threads per block
+    if (c->block_size < 64 || c->block_size > 256 || c->block_size % 32) return SPH_ERR_ARG;
     if (c->max_ngb < 32 || c->max_ngb > 512) return SPH_ERR_ARG;
     if (c->walk_blocks < 0 || c->walk_blocks > 64) return SPH_ERR_ARG;
     if (c->h_max_iter < 1 || c->h_max_iter > 1000) return SPH_ERR_ARG;
@@ -224,8 +225,8 @@ int sph_default_config(sph_config *c) {
     c->av_mode = SPH_AV_MG83;
     c->balsara = 0;
     c->leaf_size = 8;
-    c->ngb_lanes = 8;
-    c->block_size = 256;
+    c->ngb_lanes = 4;
+    c->block_size = 128;
     c->max_ngb = 256;
     c->h_max_iter = 64;
     c->flags = 0;

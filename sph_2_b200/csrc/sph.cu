@@ -331,6 +331,8 @@ int run_force(sph_ctx *ctx, bool acc, bool du) {
 
 #define SPH_DISPATCH_LANES(FN, R, ctx, ...)                 \
     switch ((ctx)->cfg.ngb_lanes) {                         \
+        case 1: rc = FN<R, 1>(ctx, ##__VA_ARGS__); break;   \
+        case 2: rc = FN<R, 2>(ctx, ##__VA_ARGS__); break;   \
         case 4: rc = FN<R, 4>(ctx, ##__VA_ARGS__); break;   \
         case 8: rc = FN<R, 8>(ctx, ##__VA_ARGS__); break;   \
         case 16: rc = FN<R, 16>(ctx, ##__VA_ARGS__); break; \
