@@ -551,7 +551,7 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
 
 }  // namespace
 
-static const double H_GROW = 1.15;
+static const double H_GROW = 1.08;
 
 int launch_smoothing_h(sph_ctx *ctx) {
     const int n = ctx->n;
@@ -560,7 +560,7 @@ int launch_smoothing_h(sph_ctx *ctx) {
     const int c = ctx->cur;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
                                             ctx->retry, H_GROW);
-    const int rounds = ctx->prologue_done ? 3 : 8;
+    const int rounds = ctx->prologue_done ? 4 : 8;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
     NewtonArgs B;

@@ -48,19 +48,50 @@ __global__ void k_box(const double *__restrict__ x, const double *__restrict__ y
     bool fin = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
     if (ok && !fin) status_add(status, SPH_S_NONFINITE, 1);
     for (int d = 0; d < 3; d++) o[d] = dbl_to_ord(p[d]);
+    // one set of atomics per block when the whole block holds one cloud (the
+    // usual case: clouds are contiguous), else per warp or per particle
+    __shared__ unsigned long long smn[3][8], smx[3][8];
+    __shared__ int scl[8];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned same = __match_any_sync(0xffffffffu, c);
-    if (same == 0xffffffffu && c >= 0) {
+    const bool uni = same == 0xffffffffu && c >= 0;
+    if (uni) {
         for (int d = 0; d < 3; d++) {
-            unsigned long long mn = warp_min_u64(o[d]), mx = warp_max_u64(o[d]);
-            if ((threadIdx.x & 31) == 0) {
-                atomicMin(&box[6 * c + d], mn);
-                atomicMax(&box[6 * c + 3 + d], mx);
+            const unsigned long long mn = warp_min_u64(o[d]), mx = warp_max_u64(o[d]);
+            if (lane == 0) {
+                smn[d][w] = mn;
+                smx[d][w] = mx;
             }
         }
     } else if (ok) {
         for (int d = 0; d < 3; d++) {
             atomicMin(&box[6 * c + d], o[d]);
             atomicMax(&box[6 * c + 3 + d], o[d]);
+        }
+    }
+    if (lane == 0) scl[w] = uni ? c : -1;
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        bool block_uni = scl[0] >= 0;
+        for (int k = 1; k < nw; k++) block_uni = block_uni && scl[k] == scl[0];
+        if (block_uni) {
+            for (int d = 0; d < 3; d++) {
+                unsigned long long mn = smn[d][0], mx = smx[d][0];
+                for (int k = 1; k < nw; k++) {
+                    mn = smn[d][k] < mn ? smn[d][k] : mn;
+                    mx = smx[d][k] > mx ? smx[d][k] : mx;
+                }
+                atomicMin(&box[6 * scl[0] + d], mn);
+                atomicMax(&box[6 * scl[0] + 3 + d], mx);
+            }
+        } else {
+            for (int k = 0; k < nw; k++)
+                if (scl[k] >= 0)
+                    for (int d = 0; d < 3; d++) {
+                        atomicMin(&box[6 * scl[k] + d], smn[d][k]);
+                        atomicMax(&box[6 * scl[k] + 3 + d], smx[d][k]);
+                    }
         }
     }
 }

@@ -193,7 +193,7 @@ def test_lists_from_candidate_rows_with_steep_h_contrast(precision):
     st = ctx.status()
     assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0
     flags = ctx.debug_array("tree_search")
-    assert flags[-1] == 0 and 0 < flags[:-1].sum() < n // 2
+    assert flags[-1] == 0 and 0 < flags[:-1].sum() < n
     off, lst = ctx.neighbour_lists()
     x, y, z, m, h = storage_state(ctx)
     oo, ol = O.neighbours(x, y, z, h)
