@@ -87,25 +87,33 @@ __device__ __forceinline__ double cool_error_estimate(const CoolDev &c, double r
     return fabs(r / rp) / u;
 }
 
-// One Newton step of the implicit equation from an approximate solution *u
-// (the surrogate's prediction), then the error estimate of the result:
-// *u <- u - r(u)/r'(u) when r' > 0 and the step keeps u positive, *est <- the
-// relative error estimate of the new *u (+inf when it is void).
+// Newton steps of the implicit equation from an approximate solution *u (the
+// surrogate's prediction): at each iterate r(u) and r'(u) give the error
+// estimate |r/r'|/u; the iterate is kept as soon as that estimate is within
+// tol / 4, else u <- u - r/r' (when r' > 0 and the step keeps u positive),
+// at most four steps.  *est <- the estimate of the returned *u (+inf when it
+// is void).  One cooling-function evaluation per iterate.
 __device__ __forceinline__ void cool_newton_polish(const CoolDev &c, double rho, double u_old,
-                                                   double dt, double *u, double *est) {
+                                                   double dt, double *u, double *est, double tol) {
     const double nH = c.XH * rho / MH_CGS;
     const double ratefact = nH * nH / rho;
-    const double u0 = *u;
-    const double T = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS * u0;
-    double s;
-    const double lam = cool_lambda(c, T, &s);
-    const double r = u0 - u_old - ratefact * (c.gheat / nH - lam) * dt;
-    const double rp = 1.0 + ratefact * dt * s * lam / u0;
-    if (rp > 0.0 && u0 > 0.0) {
-        const double u1 = u0 - r / rp;
-        if (u1 > 0.0) *u = u1;
+    const double kT = (c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS;
+    double uu = *u;
+    *est = INFINITY;
+    for (int it = 0; it < 5; it++) {
+        double s;
+        const double lam = cool_lambda(c, kT * uu, &s);
+        const double r = uu - u_old - ratefact * (c.gheat / nH - lam) * dt;
+        const double rp = 1.0 + ratefact * dt * s * lam / uu;
+        if (!(rp > 0.0) || !(uu > 0.0)) break;  // the estimate is void here
+        const double e = fabs(r / rp) / uu;
+        *u = uu;
+        *est = e;
+        if (e <= 0.25 * tol || it == 4) break;
+        const double u1 = uu - r / rp;
+        if (!(u1 > 0.0)) break;
+        uu = u1;
     }
-    *est = cool_error_estimate(c, rho, u_old, dt, *u);
 }
 
 // True when r(u) = u - u_old - ratefact*net(u)*dt is strictly increasing on

@@ -3,8 +3,8 @@
 // (mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32), forward, backward and
 // Adam kernels written here, and the in-step use: predict
 // dlog10(u) = log10(u_new/u_old) from (log10 rho, log10 u, log10 dt) [cgs],
-// estimate the error of the prediction with one Newton residual of the
-// implicit equation after one Newton step from the prediction, and fall back
+// estimate the error of the prediction with the Newton residual of the
+// implicit equation after up to four Newton steps from it, and fall back
 // to the exact solver where it exceeds the tolerance or where the implicit
 // equation is not monotone between u_old and the prediction (there it can have
 // several roots and the surrogate may have found another one).  No reference counterpart: the reference always runs the
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(128)
         if (own) {
             const double dl = (double)y * norm[7] + norm[6];
             double un = u0 * exp10(dl), est;
-            cool_newton_polish(c, rho_c, u0, dt_c, &un, &est);
+            cool_newton_polish(c, rho_c, u0, dt_c, &un, &est, err_tol);
             if (cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
                 u[i] = un / uu;
             } else {
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(128)
         if (own) {
             const double dl = (double)y * norm[7] + norm[6];
             double un = u0 * exp10(dl), est;
-            cool_newton_polish(c, r, u0, d, &un, &est);
+            cool_newton_polish(c, r, u0, d, &un, &est, err_tol);
             int fb = 0;
             if (cool_accept(c, r, u0, d, un, est, err_tol)) {
                 u_new[i] = un;
