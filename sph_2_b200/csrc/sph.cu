@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(256)
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
             const R rr = sqrt(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
-            const R inv = R(1) / hij;
+            const R inv = qdiv<R>(R(1), hij);
             S.add(mj * kern_w<R>(rr * inv, inv * inv * inv));
         }
     }
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256)
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
             const R rr = sqrt(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
-            const R inv = R(1) / hij;
+            const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;
             const R nW = kern_nw<R>(rr * inv, i2 * i2 * inv);
             const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256)
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
             const R rr = sqrt(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
-            const R inv = R(1) / hij;
+            const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;
             const R q = rr * inv;
             const R mj = vj.w;
@@ -207,23 +207,23 @@ __global__ void __launch_bounds__(256)
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
             const R rr = sqrt(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
-            const R inv = R(1) / hij;
+            const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;
             const R nW = kern_nw<R>(rr * inv, i2 * i2 * inv);
             const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
             const R ux = vi.x - vj.x, uy = vi.y - vj.y, uz = vi.z - vj.z;
             const R vr = ux * dx + uy * dy + uz * dz;
-            const R w = vr / (rr + R(1e-5));
+            const R w = qdiv<R>(vr, rr + R(1e-5));
             R PI = R(0);
             if (vr <= R(0)) {
                 const R rhoij = R(0.5) * (qi.x + qj.x);
                 if (av_mode == SPH_AV_MG83) {
                     const R cij = R(0.5) * (qi.z + qj.z);
-                    const R mu = hij * vr / (rr * rr + hij * hij * eta2);
-                    PI = (-alpha * cij * mu + beta * mu * mu) / rhoij;
+                    const R mu = qdiv<R>(hij * vr, rr * rr + hij * hij * eta2);
+                    PI = qdiv<R>(-alpha * cij * mu + beta * mu * mu, rhoij);
                 } else {
                     const R sig = qi.z + qj.z - R(3) * w;
-                    PI = R(-0.5) * alpha * sig * w / rhoij;
+                    PI = qdiv<R>(R(-0.5) * alpha * sig * w, rhoij);
                 }
             }
             if (balsara) PI = R(0.5) * (qi.w + qj.w) * PI;

@@ -176,6 +176,11 @@ __device__ __forceinline__ bool ngb_pred(double xi, double yi, double zi, double
     return r2 <= xmul(s, s);
 }
 
+// a / b in the neighbour sums: the fast single-precision divide (about 2 ulp)
+// in FP32, where the sums' own rounding is far larger; IEEE division in FP64
+template <class R> __device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
+template <> __device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
+
 // M4 cubic spline (sigma = 1/pi, support 2h): W and nW with gradW = nW * dr
 // (libsx.py:69-80, shear.py:109-121; the q+1e-20 guard of the reference)
 template <class R>
@@ -192,7 +197,7 @@ __device__ __forceinline__ R kern_nw(R q, R inv_h5) {
     if (q <= R(1)) return R(SPH_SIG) * inv_h5 * (R(-3) + R(2.25) * q);
     if (q <= R(2)) {
         R t = R(2) - q;
-        return R(-0.75 * SPH_SIG) * inv_h5 * t * t / (q + R(1e-20));
+        return qdiv<R>(R(-0.75 * SPH_SIG) * inv_h5 * t * t, q + R(1e-20));
     }
     return R(0);
 }
