@@ -77,7 +77,7 @@ template <class R> struct HSums {
 template <class R>
 __device__ __forceinline__ R pair_r(const double4 &pi, const double4 &pj) {
     const R rx = (R)(pi.x - pj.x), ry = (R)(pi.y - pj.y), rz = (R)(pi.z - pj.z);
-    return sqrt(rx * rx + ry * ry + rz * rz);
+    return qsqrt<R>(rx * rx + ry * ry + rz * rz);
 }
 
 __device__ __forceinline__ double wmin(double v) {

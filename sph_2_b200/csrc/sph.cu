@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256)
             const double4 pj = p0[j];
             const R mj = p1[j].w;
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
-            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R rr = qsqrt<R>(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
             const R inv = qdiv<R>(R(1), hij);
             S.add(mj * kern_w<R>(rr * inv, inv * inv * inv));
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256)
             const double4 pj = p0[j];
             const typename R4<R>::T vj = p1[j];
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
-            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R rr = qsqrt<R>(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
             const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256)
             const double4 pj = p0[j];
             const typename R4<R>::T vj = p1[j];
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
-            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R rr = qsqrt<R>(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
             const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256)
             const double4 pj = p0[j];
             const typename R4<R>::T vj = p1[j], qj = p2[j];
             const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
-            const R rr = sqrt(dx * dx + dy * dy + dz * dz);
+            const R rr = qsqrt<R>(dx * dx + dy * dy + dz * dz);
             const R hij = (R)(0.5 * (pi.w + pj.w));
             const R inv = qdiv<R>(R(1), hij);
             const R i2 = inv * inv;

@@ -180,6 +180,9 @@ __device__ __forceinline__ bool ngb_pred(double xi, double yi, double zi, double
 // in FP32, where the sums' own rounding is far larger; IEEE division in FP64
 template <class R> __device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
 template <> __device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
+// sqrt(x) the same way: x * rsqrt(x) in FP32 (0 at x = 0), IEEE sqrt in FP64
+template <class R> __device__ __forceinline__ R qsqrt(R x) { return sqrt(x); }
+template <> __device__ __forceinline__ float qsqrt<float>(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
 
 // M4 cubic spline (sigma = 1/pi, support 2h): W and nW with gradW = nW * dr
 // (libsx.py:69-80, shear.py:109-121; the q+1e-20 guard of the reference)
