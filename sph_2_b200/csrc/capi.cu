@@ -174,9 +174,9 @@ int step_body(sph_ctx *ctx) {
     CK(cudaEventRecord(ctx->ev_join, ctx->stream_g));
     if ((rc = launch_smoothing_h(ctx))) return rc;
     MARK(4, ctx->stream);
-    if ((rc = launch_neighbours(ctx))) return rc;
+    // lists and density in one pass over the candidate rows of the h iteration
     MARK(5, ctx->stream);
-    if ((rc = launch_density_divcurl(ctx))) return rc;
+    if ((rc = launch_lists_density(ctx))) return rc;
     MARK(6, ctx->stream);
     MARK(7, ctx->stream);
     if ((rc = launch_forces(ctx, true, fused, false))) return rc;

@@ -15,7 +15,7 @@
 // sph_get_neighbours exports them sorted.
 //
 // h iteration (fused with the candidate search): the search writes each
-// lane's candidate slots into rows laid out k-major over the group's slots and
+// lane's candidate slots into its particle's row (max_ngb entries) and
 // accumulates the kernel sums of the first Newton evaluation on the way; every
 // lane then runs a bracketed Newton iteration on (4pi/3)(2h)^3 rho(h) = n_ngb m
 // with FP64 updates and convergence test, gathering its row again only for
@@ -99,7 +99,7 @@ struct SearchArgs {
     int *ngb_cnt;  // list counts written by k_lists_cand (cnt holds candidate counts)
     double *hnb;   // per particle: the largest h_j of its list (written by the list builds)
     // candidate rows of the h iteration: the slots j inside the particle's
-    // candidate radius, laid out k-major over the group (see group_search)
+    // candidate radius, max_ngb entries per particle (row i at i K)
     int *cidx;
     const void *p1;  // Real4 (v, m)
     // exact search restricted to the particles with only[i] != 0, or to all
@@ -125,11 +125,8 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const double rmax = wmax(act ? ri : 0.0);
     const double ri2 = ri * ri;
     const int K = A.K;
-    // candidate rows of the group's slots [s0, s0 + gc) occupy entries
-    // [s0 K, (s0 + gc) K) k-major: entry k of lane l at s0 K + k gc + l, so
-    // the lanes of the Newton loop read entry k of their rows coalesced
-    const size_t cbase = MODE == 0 ? (size_t)A.gstart[g] * K + lane : 0;
-    const int cstride = MODE == 0 ? A.gcount[g] : 0;
+    // candidate row of particle i: entries [i K, i K + K)
+    const size_t cbase = MODE == 0 ? (size_t)i * K : 0;
     int count = 0;
     double hnb = 0.0;
     int sp = 1, nflat = 0;
@@ -190,7 +187,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                     // the first Newton evaluation (at h = pi.w) rides on the
                     // search: rows are only re-read by later iterations
                     hs->add(pair_r<R>(pi, pj), (R)S.smass[k]);
-                    if (count < K) A.cidx[cbase + (size_t)count * cstride] = S.flat[k];
+                    if (count < K) A.cidx[cbase + count] = S.flat[k];
                     count++;
                 }
             } else {
@@ -322,7 +319,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 6)
             *full_any = 1;
             continue;
         }
-        const int *crow = A.cidx + (size_t)s0 * K + lane;
+        const int *crow = A.cidx + (size_t)i * K;
         const double4 *__restrict__ p0 = A.p0;
         int count = 0;
         double hnb = 0.0;
@@ -334,7 +331,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 6)
             double4 pj[U];
             double hj[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) jj[u] = k0 + u < craw ? __ldg(&crow[(size_t)(k0 + u) * gc]) : i;
+            for (int u = 0; u < U; u++) jj[u] = k0 + u < craw ? __ldg(&crow[k0 + u]) : i;
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 pj[u] = p0[jj[u]];
@@ -386,12 +383,12 @@ struct NewtonArgs {
 // sums with FP64 update and convergence test.  The first evaluation (at
 // h = pi.w) comes from the search (hs0); later ones, rare once h has settled
 // from step to step, gather the candidates again through the particle's slot
-// row (entry k at row[k * gc], see group_search) in the same order, so every
+// row in the same order, so every
 // evaluation sums the same terms in the same order.  No warp collectives:
 // lanes run independent iteration counts.
 template <class R>
 __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArgs &B, int i,
-                                            const double4 &pi, const int *row, int gc,
+                                            const double4 &pi, const int *row,
                                             const HSums<R> &hs0) {
     typedef typename R4<R>::T V4;
     const V4 *p1 = (const V4 *)B.p1;
@@ -433,7 +430,7 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
             HSums<R> hs;
             hs.inv_h = R(1.0 / h);
             for (int k = 0; k < c; k++) {
-                const int j = row[(size_t)k * gc];
+                const int j = row[k];
                 hs.add(pair_r<R>(pi, A.p0[j]), (R)(double)p1[j].w);
             }
             Ssum = hs.S.value();
@@ -500,7 +497,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
         hs.inv_h = R(1.0 / pi.w);
         group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i], &hs);
         // each lane reads back only the row entries it wrote itself
-        if (act) newton_lane<R>(A, B, i, pi, A.cidx + (size_t)s0 * A.K + lane, gc, hs);
+        if (act) newton_lane<R>(A, B, i, pi, A.cidx + (size_t)i * A.K, hs);
         __syncwarp();
     }
 }
@@ -607,6 +604,21 @@ int launch_neighbours(sph_ctx *ctx) {
     ctx->lists_ok = true;
     ctx->rho_ok = ctx->divcurl_ok = false;
     return ctx_check_launch(ctx, "neighbours");
+}
+
+// the tree search for the particles marked in ctx->lflag (all of them when
+// lflag[n] is set), after the node h_max refit (skipped when nothing is marked)
+int launch_lists_marked(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    SearchArgs A = search_args(ctx, ctx->ngb, ctx->ngb_cnt);
+    A.only = ctx->lflag;
+    A.only_all = ctx->lflag + n;
+    int rc = launch_refit_hmax(ctx, ctx->lflag + n + 1);
+    if (rc) return rc;
+    k_lists<<<grid, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup, A);
+    return ctx_check_launch(ctx, "lists_marked");
 }
 
 int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap) {

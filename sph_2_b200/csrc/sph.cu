@@ -121,10 +121,13 @@ __global__ void __launch_bounds__(256)
                       const double *__restrict__ u, double gamma, int balsara,
                       double *__restrict__ rho_out, double *__restrict__ P_out,
                       double *__restrict__ c_out, double *__restrict__ divV,
-                      double *__restrict__ curlV) {
+                      double *__restrict__ curlV, const int *__restrict__ only = nullptr,
+                      const int *__restrict__ only_all = nullptr) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (int)(t / LANES), sl = (int)(t % LANES);
-    const bool valid = i < n;
+    // only (may be null): recompute just the particles with only[i] != 0
+    // (all of them when *only_all != 0)
+    const bool valid = i < n && (!only || *only_all || only[i]);
     KSum<R> S, s, cx, cy, cz;
     double hi = 1.0;
     if (valid) {
@@ -176,6 +179,129 @@ __global__ void __launch_bounds__(256)
         q.z = (R)cs;
         q.w = balsara ? (R)(d / (d + cv + 0.0001 * cs / hi)) : R(0);
         p2[i] = q;
+    }
+}
+
+// The exact lists and the density pass in one: each particle's LANES lanes
+// walk its candidate row from the h iteration (rows i K .. i K + ccnt - 1),
+// keep the pairs with |r| <= h_i + h_j (the FP64 predicate of the tree
+// search), write them to the list row in candidate order (a segment ballot
+// per round of LANES entries) and add their density, div and curl terms.  The
+// list of a particle is complete from its own row unless a partner j with the
+// larger h held it in its row only: such a j (|r| beyond 2 hc_j, with a margin
+// for rounding) is marked for the tree search and its density recomputed
+// from that list; a row that is not a complete candidate set (overflow, or h
+// above the candidate radius) marks every particle.
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_cand_density_divcurl(int n, const double4 *__restrict__ p0,
+                           const typename R4<R>::T *__restrict__ p1,
+                           typename R4<R>::T *__restrict__ p2, const int *__restrict__ crows,
+                           const int *__restrict__ ccnt, const double *__restrict__ hc, int K,
+                           int *__restrict__ rows, int *__restrict__ cnt, double *__restrict__ hnb,
+                           int *__restrict__ full, int *__restrict__ full_all,
+                           int *__restrict__ full_any, long long *status,
+                           const double *__restrict__ u, double gamma, int balsara,
+                           double *__restrict__ rho_out, double *__restrict__ P_out,
+                           double *__restrict__ c_out, double *__restrict__ divV,
+                           double *__restrict__ curlV) {
+    typedef typename R4<R>::T V4;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    const int lane = threadIdx.x & 31;
+    const unsigned seg = LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << (lane & ~(LANES - 1)));
+    const unsigned below = (1u << lane) - 1u;
+    const bool valid = i < n;
+    KSum<R> S, s, cx, cy, cz;
+    double hi = 1.0, hmx = 0.0;
+    int craw = 0;
+    double4 pi = make_double4(0.0, 0.0, 0.0, 1.0);
+    V4 vi;
+    vi.x = vi.y = vi.z = vi.w = R(0);
+    if (valid) {
+        pi = p0[i];
+        hi = pi.w;
+        vi = p1[i];
+        craw = ccnt[i];
+        if (!(craw <= K && pi.w <= hc[i])) {
+            if (sl == 0) {
+                *full_all = 1;
+                *full_any = 1;
+            }
+            craw = 0;
+        }
+    }
+    // one trip count for the warp: the segment ballot needs every lane
+    int kmax = craw;
+    for (int o = 16; o; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    const int *crow = crows + (size_t)(valid ? i : 0) * K;
+    int count = 0;
+    for (int k0 = 0; k0 < kmax; k0 += LANES) {
+        const int k = k0 + sl;
+        bool hit = false;
+        int j = 0;
+        double4 pj = pi;
+        if (k < craw) {
+            j = crow[k];
+            pj = p0[j];
+            hit = ngb_pred(pi.x, pi.y, pi.z, pi.w, pj.x, pj.y, pj.z, pj.w);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit) & seg;
+        if (hit) {
+            const int pos = count + __popc(m & below);
+            if (pos < K) rows[(size_t)i * K + pos] = j;
+            const V4 vj = p1[j];
+            const R dx = (R)(pi.x - pj.x), dy = (R)(pi.y - pj.y), dz = (R)(pi.z - pj.z);
+            const R rr = qsqrt<R>(dx * dx + dy * dy + dz * dz);
+            const R hij = (R)(0.5 * (pi.w + pj.w));
+            const R inv = qdiv<R>(R(1), hij);
+            const R i2 = inv * inv;
+            const R q = rr * inv;
+            const R mj = vj.w;
+            S.add(mj * kern_w<R>(q, i2 * inv));
+            const R nW = kern_nw<R>(q, i2 * i2 * inv);
+            const R gx = nW * dx, gy = nW * dy, gz = nW * dz;
+            const R ux = vi.x - vj.x, uy = vi.y - vj.y, uz = vi.z - vj.z;
+            s.add(-mj * (ux * gx + uy * gy + uz * gz));
+            cx.add(mj * (uy * gz - uz * gy));
+            cy.add(mj * (uz * gx - ux * gz));
+            cz.add(mj * (ux * gy - uy * gx));
+            hmx = fmax(hmx, pj.w);
+            const double ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+            const double rj = 2.0 * hc[j];
+            if (ex * ex + ey * ey + ez * ez > rj * rj * (1.0 - 1e-9)) {
+                full[j] = 1;
+                *full_any = 1;
+            }
+        }
+        count += __popc(m);
+    }
+    const double rho = seg_sum<LANES>(S.value());
+    const double Sd = seg_sum<LANES>(s.value());
+    const double X = seg_sum<LANES>(cx.value()), Y = seg_sum<LANES>(cy.value()),
+                 Z = seg_sum<LANES>(cz.value());
+    hmx = seg_max<LANES>(hmx);
+    if (valid && sl == 0) {
+        cnt[i] = min(count, K);
+        if (count > K) status_add(status, SPH_S_NGB_OVERFLOW, 1);
+        hnb[i] = hmx;
+        const double ui = u[i];
+        const double P = (gamma - 1.0) * rho * ui;
+        const double cs = sqrt(gamma * (gamma - 1.0) * ui);
+        const double inv_rho = 1.0 / rho;
+        const double d = fabs(Sd * inv_rho);
+        const double cv = sqrt(X * X + Y * Y + Z * Z) * inv_rho;
+        rho_out[i] = rho;
+        P_out[i] = P;
+        c_out[i] = cs;
+        divV[i] = d;
+        curlV[i] = cv;
+        typename R4<R>::T qq;
+        qq.x = (R)rho;
+        qq.y = (R)(P / (rho * rho));
+        qq.z = (R)cs;
+        qq.w = balsara ? (R)(d / (d + cv + 0.0001 * cs / hi)) : R(0);
+        p2[i] = qq;
     }
 }
 
@@ -309,6 +435,28 @@ int run_density_divcurl(sph_ctx *ctx) {
     return SPH_OK;
 }
 template <class R, int L>
+int run_density_divcurl_only(sph_ctx *ctx, const int *only, const int *only_all) {
+    const int n = ctx->n, c = ctx->cur;
+    const int bs = ctx->cfg.block_size;
+    k_density_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb,
+        ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara,
+        ctx->rho, ctx->P, ctx->c, ctx->divV, ctx->curlV, only, only_all);
+    return SPH_OK;
+}
+template <class R, int L>
+int run_cand_density_divcurl(sph_ctx *ctx) {
+    const int n = ctx->n, c = ctx->cur;
+    const int bs = ctx->cfg.block_size;
+    k_cand_density_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
+        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2,
+        ctx->cand_idx, ctx->cand_cnt, ctx->hcand, ctx->cfg.max_ngb, ctx->ngb, ctx->ngb_cnt,
+        ctx->st[c][ST_HNB], ctx->lflag, ctx->lflag + n, ctx->lflag + n + 1, ctx->status,
+        ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara, ctx->rho, ctx->P, ctx->c, ctx->divV,
+        ctx->curlV);
+    return SPH_OK;
+}
+template <class R, int L>
 int run_divcurl(sph_ctx *ctx) {
     const int n = ctx->n;
     const int bs = ctx->cfg.block_size;
@@ -349,6 +497,32 @@ int launch_density(sph_ctx *ctx) {
     if (rc) return rc;
     ctx->rho_ok = true;
     return ctx_check_launch(ctx, "density");
+}
+
+// Exact lists + density + EOS + div/curl + Balsara from the h iteration's
+// candidate rows (the step's path once smoothing_h has run): the fused pass,
+// the tree search for the particles it marks, and their density recomputed
+// from those lists.
+int launch_lists_density(sph_ctx *ctx) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    if (!ctx->cand_ok) return SPH_ERR_STATE;
+    CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 2), ctx->stream));
+    int rc;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_cand_density_divcurl, float, ctx); }
+    else { SPH_DISPATCH_LANES(run_cand_density_divcurl, double, ctx); }
+    if (rc) return rc;
+    if ((rc = launch_lists_marked(ctx))) return rc;
+    const int *only = ctx->lflag, *only_all = ctx->lflag + n;
+    if (ctx->cfg.precision == SPH_PREC_MIXED) {
+        SPH_DISPATCH_LANES(run_density_divcurl_only, float, ctx, only, only_all);
+    } else {
+        SPH_DISPATCH_LANES(run_density_divcurl_only, double, ctx, only, only_all);
+    }
+    if (rc) return rc;
+    ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;
+    ctx->p2_dirty = false;
+    return ctx_check_launch(ctx, "lists_density");
 }
 
 int launch_density_divcurl(sph_ctx *ctx) {

@@ -254,6 +254,8 @@ int launch_neighbours(sph_ctx *ctx);
 int launch_density(sph_ctx *ctx);
 int launch_divcurl(sph_ctx *ctx);
 int launch_density_divcurl(sph_ctx *ctx);
+int launch_lists_density(sph_ctx *ctx);
+int launch_lists_marked(sph_ctx *ctx);
 int launch_forces(sph_ctx *ctx, bool want_acc, bool want_du, bool update_u);
 int launch_repack_p2(sph_ctx *ctx);
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot);
