@@ -9,6 +9,8 @@
 // node, the moments are combined bottom-up with the left child always first
 // (so every node record is the same bit pattern on every run and equals the
 // oracle's), and the Morton order is the walk order.
+#include <cuda/atomic>
+
 #include "sph_internal.cuh"
 
 namespace {
@@ -152,9 +154,10 @@ __global__ void k_bottom_up(int n, const int *__restrict__ parent, const int *__
     if (p >= n || n < 2) return;
     int nd = parent[n - 1 + p];
     while (nd >= 0) {
-        __threadfence();
-        if (atomicAdd(&flag[nd], 1) == 0) return;
-        __threadfence();
+        // acquire-release on the arrival counter: the first thread's node
+        // record is visible to the second, which combines the two
+        cuda::atomic_ref<int, cuda::thread_scope_device> arrived(flag[nd]);
+        if (arrived.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
         int L = child[2 * nd], Rr = child[2 * nd + 1];
         double a[16], b[16], o[16];
         const double *pa = node + (size_t)16 * L, *pb = node + (size_t)16 * Rr;
@@ -193,9 +196,8 @@ __global__ void k_refit_up(int n, const int *__restrict__ parent, const int *__r
     if (p >= n || n < 2 || (need && !*need)) return;
     int nd = parent[n - 1 + p];
     while (nd >= 0) {
-        __threadfence();
-        if (atomicAdd(&flag[nd], 1) == 0) return;
-        __threadfence();
+        cuda::atomic_ref<int, cuda::thread_scope_device> arrived(flag[nd]);
+        if (arrived.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
         double hm = fmax(__ldcg(hmax + child[2 * nd]), __ldcg(hmax + child[2 * nd + 1]));
         hmax[nd] = hm;
         sA[nd].w = hm;
