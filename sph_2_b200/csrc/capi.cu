@@ -636,14 +636,19 @@ int sph_get_neighbours(sph_ctx *ctx, int64_t *off, int32_t *lst, int64_t cap, in
     CK(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < n; i++) o[i + 1] = o[i] + cnt[i];
     if (host) memcpy(off, o.data(), sizeof(long long) * (n + 1));
-    else CK(cudaMemcpy(off, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice));
+    else {
+        CK(cudaMemcpyAsync(off, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     if (!lst) return SPH_OK;
     if (o[n] > cap) return SPH_ERR_CAPACITY;
     long long *doff = nullptr;
     int *dl = nullptr;
     CK(cudaMalloc(&doff, sizeof(long long) * (n + 1)));
     CK(cudaMalloc(&dl, sizeof(int) * std::max<long long>(o[n], 1)));
-    CK(cudaMemcpy(doff, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(doff, o.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
+                       ctx->stream));
     rc = launch_export_neighbours(ctx, (int64_t *)doff, dl, o[n]);
     if (!rc) {
         CK(cudaMemcpyAsync(lst, dl, sizeof(int) * o[n],
@@ -707,10 +712,11 @@ static int direct_common(sph_ctx *ctx, const double *eps, int32_t nt, const int3
     CK(cudaMalloc(&dt_, sizeof(int) * nt));
     CK(cudaMalloc(&dout, sizeof(double) * width * nt));
     cudaMemcpyKind kin = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    CK(cudaMemcpy(dt_, targets, sizeof(int) * nt, kin));
+    // copies on the context's non-blocking stream, ordered before the kernels
+    CK(cudaMemcpyAsync(dt_, targets, sizeof(int) * nt, kin, ctx->stream));
     if (eps) {
         CK(cudaMalloc(&deps, sizeof(double) * ctx->n));
-        CK(cudaMemcpy(deps, eps, sizeof(double) * ctx->n, kin));
+        CK(cudaMemcpyAsync(deps, eps, sizeof(double) * ctx->n, kin, ctx->stream));
         // eps is given in the caller's original order: bring it to storage order
         k_gather_by_id<<<div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->id[ctx->cur],
                                                                       deps, ctx->red);

@@ -69,15 +69,16 @@ int sph_cooling_setup(sph_ctx *ctx, const sph_cooling_params *p, const double *l
         ctx->dev_bytes += sizeof(double) * 2 * 4097;
         ctx->cool_table = (double *)q;
     }
-    CK(cudaMemcpy(ctx->cool_table, log_lambda, sizeof(double) * (p->n_bins + 1),
-                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(ctx->cool_table, log_lambda, sizeof(double) * (p->n_bins + 1),
+                       cudaMemcpyHostToDevice, ctx->stream));
     {
         // Lambda(T_e) / T_e at the bin edges, for the surrogate's monotonicity test
         const double dl = (p->logT1 - p->logT0) / p->n_bins;
         std::vector<double> lamT(p->n_bins + 1);
         for (int e = 0; e <= p->n_bins; e++) lamT[e] = pow(10.0, log_lambda[e] - (p->logT0 + e * dl));
-        CK(cudaMemcpy(ctx->cool_table + 4097, lamT.data(), sizeof(double) * (p->n_bins + 1),
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(ctx->cool_table + 4097, lamT.data(), sizeof(double) * (p->n_bins + 1),
+                           cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
     }
     ctx->cool = *p;
     ctx->cool_ok = true;
@@ -108,9 +109,10 @@ int sph_cool_solve(sph_ctx *ctx, int32_t n, const double *rho, const double *u_o
     int *di = nullptr;
     CK(cudaMalloc(&d, sizeof(double) * 4 * n));
     if (iters) CK(cudaMalloc(&di, sizeof(int) * n));
-    CK(cudaMemcpy(d, rho, sizeof(double) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d + n, u_old, sizeof(double) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d + 2 * (size_t)n, dt, sizeof(double) * n, cudaMemcpyHostToDevice));
+    // stream-ordered before the solve on the context's non-blocking stream
+    CK(cudaMemcpyAsync(d, rho, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d + n, u_old, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d + 2 * (size_t)n, dt, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_cool_solve(ctx, n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, di);
     if (!rc) {
         CK(cudaStreamSynchronize(ctx->stream));

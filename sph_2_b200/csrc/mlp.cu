@@ -537,7 +537,7 @@ int ensure_mlp(sph_ctx *ctx) {
         ctx->dev_bytes += sizeof(int) * ((size_t)ctx->cfg.n_max + 1);
         ctx->cool_list = (int *)l;
     }
-    CK(cudaMemset(q, 0, bytes));
+    CK(cudaMemsetAsync(q, 0, bytes, ctx->stream));  // ordered before the parameter copies
     ctx->allocs.push_back(q);
     ctx->dev_bytes += bytes;
     float *f = (float *)q;
@@ -670,7 +670,8 @@ static int to_device(sph_ctx *ctx, const void *src, size_t bytes, int host, void
         return SPH_OK;
     }
     CK(cudaMalloc(dst, bytes));
-    CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    // on the context's (non-blocking) stream, so the kernel that reads it is ordered after it
+    CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
     return SPH_OK;
 }
 
