@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--theta", type=float, default=0.38)
-    ap.add_argument("--theta-local", type=float, default=0.13,
+    ap.add_argument("--theta-local", type=float, default=0.25,
                     help="mixed walk: far cells through group Taylor expansions (0: off)")
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=4)
@@ -332,10 +332,10 @@ def main():
     torch.cuda.synchronize()
     walk_ms = w0.elapsed_time(w1) / reps
     cnt = ctx.counters()
-    # far cells: 150 flop each, once per group; 65 per particle to evaluate
-    # the expansion
-    flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"] + 150.0 * cnt["far_cells"] + \
-        (65.0 * n if cnt["far_cells"] else 0.0)
+    # far cells: 190 flop each (35 Taylor coefficients), once per group; 115
+    # per particle to evaluate the expansion
+    flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"] + 190.0 * cnt["far_cells"] + \
+        (115.0 * n if cnt["far_cells"] else 0.0)
     fp32_peak = ctx.fp32_peak_tflops()
     achieved = flops / (walk_ms * 1e-3) / 1e12
     roofline = {"kernel": "k_walk<float> (gravity walk)", "bound": "fp32",
@@ -344,7 +344,7 @@ def main():
                 "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json "
                                "has no FP32 figure)",
                 "algorithmic": ("60 flop per quadrupole cell + 20 per particle interaction "
-                                "+ 150 per far cell (once per group) + 65 per particle for "
+                                "+ 190 per far cell (once per group) + 115 per particle for "
                                 "the group expansion"),
                 "interactions_per_particle": {"cells": cnt["cells"] / n,
                                               "particles": cnt["particles"] / n,

@@ -30,9 +30,14 @@ namespace {
 constexpr int WALK_WARPS = 4;
 // coefficients of the group local expansion: field (3), its gradient J
 // (xx yy zz xy xz yz), the monopole's second derivatives H (xxx yyy zzz xxy
-// xxz yyx yyz zzx zzy xyz) and the potential
-constexpr int NLOC = 20;
-constexpr int WSTK = 1024;
+// xxz yyx yyz zzx zzy xyz), the potential, and the monopole's third
+// derivatives T (xxxx yyyy zzzz xxxy xxxz yyyx yyyz zzzx zzzy xxyy xxzz yyzz
+// xxyz yyxz zzxy)
+constexpr int NLOC = 35;
+#ifndef SPH_WALK_STACK
+#define SPH_WALK_STACK 512
+#endif
+constexpr int WSTK = SPH_WALK_STACK;
 constexpr unsigned FULL = 0xffffffffu;
 
 template <class R> __device__ __forceinline__ R rsq(R x);
@@ -101,6 +106,9 @@ __device__ __forceinline__ float box_d2(float x0, float y0, float z0, float x1, 
 //         A = 1.5 tr g5 - 7.5 (r.Q.r) g7,  B = -7.5 tr g7 + 52.5 (r.Q.r) g9
 //   H   = 3 M g5 (delta_ij r_k + delta_ik r_j + delta_jk r_i) - 15 M g7 r_i r_j r_k
 //   phi = -(M g1 + 0.5 (3 (r.Q.r) g5 - tr g3))
+//   T   = 3 M g5 d4 - 15 M g7 d2rr + 105 M g9 r_i r_j r_k r_l, with
+//         d4 = d_ij d_kl + d_ik d_jl + d_il d_jk and d2rr the six d_ab r_c r_d
+//         terms over the pairings of (ijkl)
 __device__ __forceinline__ void far_coeffs(float rx, float ry, float rz, float eps2, float M,
                                            float qxx, float qyy, float qzz, float qxy, float qxz,
                                            float qyz, float tr, float *L) {
@@ -138,10 +146,29 @@ __device__ __forceinline__ void far_coeffs(float rx, float ry, float rz, float e
     L[17] = ry * ez;               // zzy
     L[18] = -b7 * rx * ry * rz;    // xyz
     L[19] = -(M * g1 + 0.5f * (3.f * dqd * g5 - tr * g3));
+    const float p9 = 105.f * M * g9, X = rx * rx, Y = ry * ry, Z = rz * rz;
+    const float cx = p9 * X - 3.f * b7, cy = p9 * Y - 3.f * b7, cz = p9 * Z - 3.f * b7;
+    const float dx = p9 * X - b7, dy = p9 * Y - b7, dz = p9 * Z - b7;
+    const float xy = rx * ry, xz = rx * rz, yz = ry * rz;
+    L[20] = X * (cx - 3.f * b7) + 3.f * a3;  // xxxx
+    L[21] = Y * (cy - 3.f * b7) + 3.f * a3;  // yyyy
+    L[22] = Z * (cz - 3.f * b7) + 3.f * a3;  // zzzz
+    L[23] = xy * cx;                         // xxxy
+    L[24] = xz * cx;                         // xxxz
+    L[25] = xy * cy;                         // yyyx
+    L[26] = yz * cy;                         // yyyz
+    L[27] = xz * cz;                         // zzzx
+    L[28] = yz * cz;                         // zzzy
+    L[29] = X * dy - b7 * Y + a3;            // xxyy
+    L[30] = X * dz - b7 * Z + a3;            // xxzz
+    L[31] = Y * dz - b7 * Z + a3;            // yyzz
+    L[32] = yz * dx;                         // xxyz
+    L[33] = xz * dy;                         // yyxz
+    L[34] = xy * dz;                         // zzxy
 }
 
 // value of the local expansion at offset u from the group centre: the field
-// a0 + J u + H:uu/2 and the potential phi0 - a0.u - u.J.u/2
+// a0 + J u + H:uu/2 + T:uuu/6 and the potential phi0 - a0.u - u.J.u/2
 __device__ __forceinline__ void far_eval(const float *L, float ux, float uy, float uz, float &ax,
                                          float &ay, float &az, float &phi) {
     const float jx = L[3] * ux + L[6] * uy + L[7] * uz;
@@ -151,9 +178,18 @@ __device__ __forceinline__ void far_eval(const float *L, float ux, float uy, flo
     const float hx = L[9] * xx + L[14] * yy + L[16] * zz + 2.f * (L[12] * xy + L[13] * xz + L[18] * yz);
     const float hy = L[12] * xx + L[10] * yy + L[17] * zz + 2.f * (L[14] * xy + L[18] * xz + L[15] * yz);
     const float hz = L[13] * xx + L[15] * yy + L[11] * zz + 2.f * (L[18] * xy + L[16] * xz + L[17] * yz);
-    ax = L[0] + jx + 0.5f * hx;
-    ay = L[1] + jy + 0.5f * hy;
-    az = L[2] + jz + 0.5f * hz;
+    const float xxx = xx * ux, yyy = yy * uy, zzz = zz * uz, xxy = xx * uy, xxz = xx * uz;
+    const float xyy = yy * ux, yyz = yy * uz, xzz = zz * ux, yzz = zz * uy, xyz = xy * uz;
+    const float tx = L[20] * xxx + L[25] * yyy + L[27] * zzz + 6.f * L[32] * xyz +
+                     3.f * (L[23] * xxy + L[24] * xxz + L[29] * xyy + L[30] * xzz + L[33] * yyz + L[34] * yzz);
+    const float ty = L[23] * xxx + L[21] * yyy + L[28] * zzz + 6.f * L[33] * xyz +
+                     3.f * (L[29] * xxy + L[32] * xxz + L[25] * xyy + L[34] * xzz + L[26] * yyz + L[31] * yzz);
+    const float tz = L[24] * xxx + L[26] * yyy + L[22] * zzz + 6.f * L[34] * xyz +
+                     3.f * (L[32] * xxy + L[30] * xxz + L[33] * xyy + L[27] * xzz + L[31] * yyz + L[28] * yzz);
+    const float s6 = 1.f / 6.f;
+    ax = L[0] + jx + 0.5f * hx + s6 * tx;
+    ay = L[1] + jy + 0.5f * hy + s6 * ty;
+    az = L[2] + jz + 0.5f * hz + s6 * tz;
     phi = L[19] - (L[0] * ux + L[1] * uy + L[2] * uz) - 0.5f * (ux * jx + uy * jy + uz * jz);
 }
 
@@ -478,10 +514,10 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         if constexpr (PACKED) {
             if (nF > 0) {
                 __syncwarp();
-                if (lane < NLOC) {  // Kahan sum of the 32 lane columns
+                for (int q = lane; q < NLOC; q += 32) {  // Kahan sum of the 32 lane columns
                     KSum<float> t;
-                    for (int k = 0; k < 32; k++) t.add(S.red[lane][k]);
-                    S.ltot[lane] = (float)t.value();
+                    for (int k = 0; k < 32; k++) t.add(S.red[q][k]);
+                    S.ltot[q] = (float)t.value();
                 }
                 __syncwarp();
                 float Lt[NLOC];

@@ -300,7 +300,7 @@ def test_gravity_walk_mixed_vs_direct(theta, bound):
     assert rms_rel(a, ad) < bound
 
 
-@pytest.mark.parametrize("theta,theta_local,bound", [(0.38, 0.13, 1.6e-4), (0.5, 0.2, 5e-4)])
+@pytest.mark.parametrize("theta,theta_local,bound", [(0.38, 0.13, 1.6e-4), (0.38, 0.25, 1.6e-4), (0.5, 0.2, 5e-4)])
 def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
     """Far cells through the groups' Taylor expansions: the error against the
     FP64 direct sum stays within a small margin of the plain walk's, while
@@ -320,6 +320,8 @@ def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
     assert loc["particles"] == plain["particles"]
     assert e_loc < bound and e_loc < 1.3 * e_plain
     assert plain["far_cells"] == 0
+    st = ctx2.status()
+    assert st["stack_overflow"] == 0 and 0 < st["walk_stack_max"] <= 512
 
 
 # ------------------------------------------------- status / fault paths ----
