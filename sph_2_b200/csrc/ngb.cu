@@ -55,6 +55,20 @@ template <> struct R2<double> { typedef double2 T; };
 template <class R> struct HSums {
     KSum<R> S, D;
     R inv_h;
+    // kernel terms at distance r: false outside the support
+    __device__ __forceinline__ bool terms(R r, R &w, R &dw) const {
+        const R q = r * inv_h;
+        if (!(q < R(2))) return false;
+        if (q <= R(1)) {
+            w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
+            dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
+        } else {
+            const R t = R(2) - q;
+            w = R(0.25) * t * t * t;
+            dw = R(1.5) * t * t * (R(1) - q);
+        }
+        return true;
+    }
     __device__ __forceinline__ void add(R r, R m) {
         const R q = r * inv_h;
         if (q < R(2)) {
@@ -142,6 +156,12 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const float2 pfx = bc2((float)(pi.x - cx)), pfy = bc2((float)(pi.y - cy)),
                  pfz = bc2((float)(pi.z - cz));
     const float2 ri2f = bc2((float)ri2 * 1.0001f), hif = bc2((float)pi.w);
+    // FP32 h iteration: a candidate whose FP32 distance is below the
+    // threshold narrowed by 1e-4 is inside in FP64 too and skips the FP64
+    // test; its kernel terms use the FP32 relative coordinates and are summed
+    // plainly over the chunk (at most 32 terms), then added to the Kahan sums
+    constexpr bool FAST = MODE == 0 && std::is_same<R, float>::value;
+    const float2 ri2lo = bc2((float)ri2 * 0.9999f);
     const float2 m1 = bc2(-1.f), widen = bc2(1.0001f);
 
     auto process = [&](int m) {
@@ -152,15 +172,16 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             S.fx[lane] = (float)(q.x - cx);
             S.fy[lane] = (float)(q.y - cy);
             S.fz[lane] = (float)(q.z - cz);
-            S.fh[lane] = (float)q.w;
-            if (MODE == 0) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
+            if (FAST) S.fh[lane] = (float)((const V4 *)A.p1)[j].w;  // the mass
+            else S.fh[lane] = (float)q.w;
+            if (MODE == 0 && !FAST) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
         } else if (lane < ((m + 1) & ~1)) {
             // the odd tail of a chunk: an entry that never passes
             S.fx[lane] = S.fy[lane] = S.fz[lane] = INFINITY;
             S.fh[lane] = 0.f;
         }
         __syncwarp();
-        unsigned hit = 0;
+        unsigned hit = 0, sure = 0;
         if (act) {
 #pragma unroll 4
             for (int k = 0; k < m; k += 2) {
@@ -175,13 +196,36 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                 }
                 hit |= (r2.x <= lim.x ? 1u : 0u) << k;
                 hit |= (r2.y <= lim.y ? 2u : 0u) << k;
+                if (FAST) {
+                    sure |= (r2.x <= ri2lo.x ? 1u : 0u) << k;
+                    sure |= (r2.y <= ri2lo.y ? 2u : 0u) << k;
+                }
             }
         }
+        R cs = R(0), cd = R(0);
         while (hit) {
             const int k = __ffs(hit) - 1;
             hit &= hit - 1;
-            const double4 pj = S.stage[k];
-            if (MODE == 0) {
+            double4 pj;
+            if (!FAST) pj = S.stage[k];
+            if (FAST) {
+                bool in = (sure >> k) & 1u;
+                if (!in) {
+                    pj = S.stage[k];
+                    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    in = dx * dx + dy * dy + dz * dz <= ri2;
+                }
+                if (in) {
+                    const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
+                    R w, dw;
+                    if (hs->terms(qsqrt<float>(rx * rx + ry * ry + rz * rz), w, dw)) {
+                        cs += S.fh[k] * w;
+                        cd += S.fh[k] * dw;
+                    }
+                    if (count < K) A.cidx[cbase + count] = S.flat[k];
+                    count++;
+                }
+            } else if (MODE == 0) {
                 const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                 if (dx * dx + dy * dy + dz * dz <= ri2) {
                     // the first Newton evaluation (at h = pi.w) rides on the
@@ -197,6 +241,10 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                     hnb = fmax(hnb, pj.w);
                 }
             }
+        }
+        if (FAST) {
+            hs->S.add(cs);
+            hs->D.add(cd);
         }
         __syncwarp();
     };
