@@ -332,23 +332,26 @@ def main():
     torch.cuda.synchronize()
     walk_ms = w0.elapsed_time(w1) / reps
     cnt = ctx.counters()
-    # far cells: 190 flop each (35 Taylor coefficients), once per group; 115
-    # per particle to evaluate the expansion
+    # far cells: 190 flop each (35 Taylor coefficients), once per group or
+    # super-group; 115 per particle to evaluate each expansion (the group's
+    # and its super-group's)
     flops = 60.0 * cnt["cells"] + 20.0 * cnt["particles"] + 190.0 * cnt["far_cells"] + \
-        (115.0 * n if cnt["far_cells"] else 0.0)
+        (115.0 * n if cnt["far_cells"] else 0.0) + (115.0 * n if cnt.get("sg_far_cells") else 0.0)
     fp32_peak = ctx.fp32_peak_tflops()
     achieved = flops / (walk_ms * 1e-3) / 1e12
-    roofline = {"kernel": "k_walk<float> (gravity walk)", "bound": "fp32",
+    roofline = {"kernel": "k_sg_walk + k_walk<float> (gravity walk)", "bound": "fp32",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": None,
                 "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json "
                                "has no FP32 figure)",
                 "algorithmic": ("60 flop per quadrupole cell + 20 per particle interaction "
-                                "+ 190 per far cell (once per group) + 115 per particle for "
-                                "the group expansion"),
+                                "+ 190 per far cell (once per group or super-group) + 115 per "
+                                "particle for each of the group and super-group expansions"),
                 "interactions_per_particle": {"cells": cnt["cells"] / n,
                                               "particles": cnt["particles"] / n,
-                                              "far_cells_per_particle_equiv": cnt["far_cells"] / n},
+                                              "far_cells_per_particle_equiv": cnt["far_cells"] / n,
+                                              "supergroup_far_cells_per_particle_equiv":
+                                                  cnt.get("sg_far_cells", 0) / n},
                 "walk_ms": walk_ms}
     try:
         with open(os.path.join(ROOT, "profiles", "walk_traffic.json")) as f:

@@ -249,9 +249,15 @@ int sph_cfl_dt(sph_ctx *ctx, double *dt);
 int sph_energies(sph_ctx *ctx, double *out10);
 /* interaction counters of the last gravity call: [cells, particles] */
 int sph_get_counters(sph_ctx *ctx, int64_t *out2);
-/* far cells of the last walk that went through the group local expansions
- * (sph_config.theta_local), summed over groups (one per cell and group) */
+/* far cells of the last walk that went through the local expansions
+ * (sph_config.theta_local), summed over groups and super-groups (one per
+ * cell and group or super-group) */
 int sph_get_far_cells(sph_ctx *ctx, int64_t *out);
+/* super-groups of the last mixed walk with theta_local > 0 (maximal tree
+ * nodes of at most 128 particles, walked once for the far cells their groups
+ * share): [far cells through their expansions, super-groups whose node list
+ * did not fit (their groups walked from the root)] */
+int sph_get_supergroup_stats(sph_ctx *ctx, int64_t *out2);
 
 /* ---- cooling (DoCooling, myPhotoLibsGPU.h:615-686; hcoolingx, hfvCLibs:1240) ---- */
 int sph_cooling_setup(sph_ctx *ctx, const sph_cooling_params *p, const double *log_lambda);

@@ -106,6 +106,7 @@ SIGNATURES = [
     ("sph_cfl_dt", C.c_int, [_P, _P]),
     ("sph_energies", C.c_int, [_P, _P]),
     ("sph_get_far_cells", C.c_int, [_P, _P]),
+    ("sph_get_supergroup_stats", C.c_int, [_P, _P]),
     ("sph_get_counters", C.c_int, [_P, _P]),
     ("sph_cooling_setup", C.c_int, [_P, C.POINTER(SphCoolingParams), _P]),
     ("sph_cooling_exact", C.c_int, [_P]),

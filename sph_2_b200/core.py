@@ -297,7 +297,10 @@ class Context:
         self._chk(self._L.sph_get_counters(self._h, _ptr(out)), "counters")
         far = np.zeros(1, np.int64)
         self._chk(self._L.sph_get_far_cells(self._h, _ptr(far)), "far cells")
-        return {"cells": int(out[0]), "particles": int(out[1]), "far_cells": int(far[0])}
+        sg = np.zeros(2, np.int64)
+        self._chk(self._L.sph_get_supergroup_stats(self._h, _ptr(sg)), "super-group stats")
+        return {"cells": int(out[0]), "particles": int(out[1]), "far_cells": int(far[0]),
+                "sg_far_cells": int(sg[0]), "sg_fallback": int(sg[1])}
 
     def kick(self, fac=0.5):
         self._chk(self._L.sph_kick(self._h, fac), "sph_kick")

@@ -321,7 +321,16 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->retry, N); DAF(ctx->hcand, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
     DAF(ctx->status, SPH_NSTATUS);
-    DAF(ctx->counters, 3);
+    DAF(ctx->counters, 5);
+    if (ctx->cfg.precision == SPH_PREC_MIXED && ctx->cfg.theta_local > 0.0) {
+        ctx->sg_cap = (int)std::min<size_t>(N, N / 8 + C + 64);
+        DAF(ctx->sg_start, N); DAF(ctx->sg_count, N); DAF(ctx->sg_cloud, N);
+        DAF(ctx->d_nsg, 1);
+        DAF(ctx->g_sg, G);
+        DAF(ctx->sg_nrem, (size_t)ctx->sg_cap);
+        DAF(ctx->sg_pool, (size_t)SG_POOL * N);
+        DAF(ctx->sgL, (size_t)SG_LSTRIDE * ctx->sg_cap);
+    }
     DAF(ctx->work, 16);
     DAF(ctx->red, std::max<size_t>(2 * N, 8192));
     if (cudaMemsetAsync(ctx->status, 0, SPH_NSTATUS * sizeof(long long), ctx->stream) ||
@@ -786,7 +795,20 @@ int sph_get_far_cells(sph_ctx *ctx, int64_t *out) {
     if (rc) return rc;
     if (!out) return SPH_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream_g));
-    CK(cudaMemcpyAsync(out, ctx->counters + 2, sizeof(long long), cudaMemcpyDeviceToHost,
+    long long c[2];
+    CK(cudaMemcpyAsync(c, ctx->counters + 2, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = c[0] + c[1];
+    return SPH_OK;
+}
+
+int sph_get_supergroup_stats(sph_ctx *ctx, int64_t *out2) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out2) return SPH_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaMemcpyAsync(out2, ctx->counters + 3, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return SPH_OK;

@@ -66,6 +66,20 @@ struct WalkSmemF {
     float ltot[NLOC];
 };
 
+// super-group records read by the group walk (g_sg null: none)
+struct SgArgs {
+    const int *g_sg, *start, *nrem, *pool;
+    const float *L;
+    int cap;
+};
+
+// super-group pre-walk: stack, far-cell list, per-lane coefficient columns
+struct SgSmem {
+    int stk[WSTK];
+    int flist[96];
+    float red[NLOC][32];
+};
+
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 
@@ -167,6 +181,37 @@ __device__ __forceinline__ void far_coeffs(float rx, float ry, float rz, float e
     L[34] = xy * dz;                         // zzxy
 }
 
+// far cells flist[lane], flist[lane + 32], ... (below m <= 32 PER) into this
+// lane's column of the partial coefficient sums of an expansion at
+// (x0, y0, z0), summed in registers first (one shared-memory update per
+// coefficient)
+template <int PER>
+__device__ __forceinline__ void far_add(float (*red)[32], int lane, const int *flist, int m,
+                                        float x0, float y0, float z0, float eps2,
+                                        const float4 *__restrict__ wA,
+                                        const float4 *__restrict__ wB,
+                                        const float4 *__restrict__ wC) {
+    if (lane >= m) return;
+    float acc[NLOC];
+    {
+        const int nd = flist[lane];
+        const float4 a = wA[nd], b = wB[nd], c = wC[nd];
+        far_coeffs(x0 - a.x, y0 - a.y, z0 - a.z, eps2, b.w, b.x, b.y, b.z, c.x, c.y, c.z, c.w,
+                   acc);
+    }
+#pragma unroll 1
+    for (int k = lane + 32; k < m && k < 32 * PER; k += 32) {
+        float Lc[NLOC];
+        const int nd = flist[k];
+        const float4 a = wA[nd], b = wB[nd], c = wC[nd];
+        far_coeffs(x0 - a.x, y0 - a.y, z0 - a.z, eps2, b.w, b.x, b.y, b.z, c.x, c.y, c.z, c.w, Lc);
+#pragma unroll
+        for (int q = 0; q < NLOC; q++) acc[q] += Lc[q];
+    }
+#pragma unroll
+    for (int q = 0; q < NLOC; q++) red[q][lane] += acc[q];
+}
+
 // value of the local expansion at offset u from the group centre: the field
 // a0 + J u + H:uu/2 + T:uuu/6 and the potential phi0 - a0.u - u.J.u/2
 __device__ __forceinline__ void far_eval(const float *L, float ux, float uy, float uz, float &ax,
@@ -194,14 +239,14 @@ __device__ __forceinline__ void far_eval(const float *L, float ux, float uy, flo
 }
 
 template <class R, bool POT>
-__global__ void __launch_bounds__(WALK_WARPS * 32)
+__global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value && !POT ? 6 : 1)
     k_walk(const int *__restrict__ ngroup_p, const int *__restrict__ gstart, const int *__restrict__ gcount,
            const int *__restrict__ gcloud, const int *__restrict__ croot,
            const typename R4<R>::T *__restrict__ pw, const typename R4<R>::T *__restrict__ wA,
            const typename R4<R>::T *__restrict__ wB, const typename R4<R>::T *__restrict__ wC,
            const int4 *__restrict__ wL, int leaf_size, R eps2, double G, int n,
            double *__restrict__ agrav, double *__restrict__ pot, unsigned *work,
-           unsigned long long *counters, long long *status, float theta_local) {
+           unsigned long long *counters, long long *status, float theta_local, SgArgs sg) {
     typedef typename R4<R>::T V4;
     constexpr bool PACKED = std::is_same<R, float>::value;
     typedef typename std::conditional<PACKED, WalkSmemF, WalkSmem<R>>::type SM;
@@ -227,7 +272,33 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         long long nC = 0, nP = 0, nF = 0;
         int sp = 1, nc = 0, np = 0, nfar = 0;
         bool overflow = false;
-        if (lane == 0) S.stk[0] = croot[gcloud[g]];
+        // the super-group's node list replaces the root when it has one
+        int rpos = 0, nrem = 0, sgi = -1;
+        const int *rem = nullptr;
+        if constexpr (PACKED) {
+            if (sg.g_sg) {
+                const int s = sg.g_sg[g];
+                const int k = s < sg.cap ? sg.nrem[s] : -1;
+                if (k >= 0) {
+                    sgi = s;
+                    nrem = k;
+                    rem = sg.pool + (size_t)sg.start[s] * SG_POOL;
+                    sp = 0;
+                    // the super-group's expansion at its own centre, first
+                    const float *Ls = sg.L + (size_t)s * SG_LSTRIDE;
+                    float Lt[NLOC];
+#pragma unroll
+                    for (int q = 0; q < NLOC; q++) Lt[q] = Ls[q];
+                    float fax, fay, faz, fph;
+                    far_eval(Lt, pi.x - Ls[36], pi.y - Ls[37], pi.z - Ls[38], fax, fay, faz, fph);
+                    ax.add(fax);
+                    ay.add(fay);
+                    az.add(faz);
+                    if (POT) ph.add(fph);
+                }
+            }
+        }
+        if (lane == 0 && sgi < 0) S.stk[0] = croot[gcloud[g]];
         // local expansion (FP32 walk, theta_local > 0): accepted cells whose
         // com is at least R_g / theta_local from the group centre x0 (R_g the
         // group's radius about x0) enter a Taylor expansion at x0 once per
@@ -345,15 +416,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         // partial coefficient sums (summed over the warp once per group)
         auto flush_far = [&](int m) {
           if constexpr (PACKED) {
-            if (lane < m) {
-                float Lc[NLOC];
-                const int nd = S.flist[lane];
-                const float4 a = wA[nd], b = wB[nd], c = wC[nd];
-                far_coeffs(fx0 - a.x, fy0 - a.y, fz0 - a.z, eps2, b.w, b.x, b.y, b.z, c.x, c.y, c.z,
-                           c.w, Lc);
-#pragma unroll
-                for (int q = 0; q < NLOC; q++) S.red[q][lane] += Lc[q];
-            }
+            far_add<1>(S.red, lane, S.flist, m, fx0, fy0, fz0, eps2, wA, wB, wC);
             nF += m;
             __syncwarp();
           }
@@ -414,7 +477,15 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
           }
         };
 
-        while (sp > 0 || nc > 0 || np > 0) {
+        while (sp > 0 || rpos < nrem || nc > 0 || np > 0) {
+            if (sp == 0 && rpos < nrem) {
+                // next 32 nodes of the super-group's list
+                const int take = min(nrem - rpos, 32);
+                if (lane < take) S.stk[lane] = rem[rpos + lane];
+                rpos += take;
+                sp = take;
+                __syncwarp();
+            }
             if (sp > 0) {
                 const int take = min(sp, 32);
                 sp -= take;
@@ -505,7 +576,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
                     }
                 }
             }
-            if (sp == 0) {
+            if (sp == 0 && rpos >= nrem) {
                 if (nc > 0) { flush_cells(nc); nc = 0; }
                 if (np > 0) { flush_parts(np); np = 0; }
                 if (nfar > 0) { flush_far(nfar); nfar = 0; }
@@ -546,6 +617,145 @@ __global__ void __launch_bounds__(WALK_WARPS * 32)
         }
     }
     if (lane == 0) atomicMax((unsigned long long *)&status[7], (unsigned long long)maxsp);
+}
+
+// Super-group pre-walk of the FP32 walk with group expansions: one warp per
+// super-group (a maximal tree node of at most SGROUP_MAX particles of one
+// cloud) walks the tree with the super-group's box.  Accepted cells whose com
+// lies at least R / theta_local from the box centre c (R the super-group's
+// radius about c) enter the super-group's Taylor expansion at c, which every
+// particle of its groups evaluates.  Accepted cells nearer than that, buckets,
+// and nodes of at most SGROUP_MAX particles that fail the acceptance test go
+// to the node list its groups walk instead of the root (a group's box lies
+// inside the super-group's, so the group accepts at least what this walk
+// accepts); larger nodes that fail it are opened here.  A list longer than
+// SG_POOL slots per particle, or a stack overflow, leaves the super-group
+// without a record (nrem -1): its groups then walk from the root.
+template <bool POT>
+__global__ void __launch_bounds__(WALK_WARPS * 32, 6)
+    k_sg_walk(const int *__restrict__ nsg_p, int cap, const int *__restrict__ sstart,
+              const int *__restrict__ scount, const int *__restrict__ scloud,
+              const int *__restrict__ croot, const float4 *__restrict__ pw,
+              const float4 *__restrict__ wA, const float4 *__restrict__ wB,
+              const float4 *__restrict__ wC, const int4 *__restrict__ wL, float eps2,
+              float theta_local, int *__restrict__ pool, int *__restrict__ nrem_out,
+              float *__restrict__ sgL, unsigned long long *counters) {
+    __shared__ SgSmem smem[WALK_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SgSmem &S = smem[w];
+    const unsigned lt = (1u << lane) - 1u;
+    const int nsg = min(*nsg_p, cap);
+    for (int s = blockIdx.x * WALK_WARPS + w; s < nsg; s += gridDim.x * WALK_WARPS) {
+        const int s0 = sstart[s], sc = scount[s];
+        if (sc <= 32) {
+            // a single group: nothing to share, the group walks from the root
+            if (lane == 0) nrem_out[s] = -1;
+            continue;
+        }
+        float bx0 = INFINITY, by0 = INFINITY, bz0 = INFINITY;
+        float bx1 = -INFINITY, by1 = -INFINITY, bz1 = -INFINITY;
+        for (int k = lane; k < sc; k += 32) {
+            const float4 p = pw[s0 + k];
+            bx0 = fminf(bx0, p.x); by0 = fminf(by0, p.y); bz0 = fminf(bz0, p.z);
+            bx1 = fmaxf(bx1, p.x); by1 = fmaxf(by1, p.y); bz1 = fmaxf(bz1, p.z);
+        }
+        bx0 = wmin<float>(bx0); by0 = wmin<float>(by0); bz0 = wmin<float>(bz0);
+        bx1 = wmax<float>(bx1); by1 = wmax<float>(by1); bz1 = wmax<float>(bz1);
+        const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1), cz = 0.5f * (bz0 + bz1);
+        float r2 = 0.f;
+        for (int k = lane; k < sc; k += 32) {
+            const float4 p = pw[s0 + k];
+            const float dx = p.x - cx, dy = p.y - cy, dz = p.z - cz;
+            r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+        }
+        const float rfar2 = wmax<float>(r2) / (theta_local * theta_local);
+#pragma unroll
+        for (int q = 0; q < NLOC; q++) S.red[q][lane] = 0.f;
+        int *rem = pool + (size_t)s0 * SG_POOL;
+        const int remcap = sc * SG_POOL;
+        int sp = 1, nrem = 0, nfar = 0;
+        long long nF = 0;
+        bool bad = false;
+        if (lane == 0) S.stk[0] = croot[scloud[s]];
+        __syncwarp();
+        while (sp > 0 && !bad) {
+            const int take = min(sp, 32);
+            sp -= take;
+            int nd = 0, cl = 0, cr = 0;
+            bool far = false, keep = false, open = false;
+            if (lane < take) {
+                nd = S.stk[sp + lane];
+                const float4 a = wA[nd];
+                const int4 L = wL[nd];
+                cl = L.z;
+                cr = L.w;
+                const float d2 = box_d2(bx0, by0, bz0, bx1, by1, bz1, a.x, a.y, a.z);
+                if (d2 >= a.w && L.y > 1) {
+                    const float dx = a.x - cx, dy = a.y - cy, dz = a.z - cz;
+                    far = dx * dx + dy * dy + dz * dz >= rfar2;
+                    keep = !far;
+                } else {
+                    open = L.y > SGROUP_MAX;
+                    keep = !open;
+                }
+            }
+            __syncwarp();
+            const unsigned km = __ballot_sync(FULL, keep);
+            if (nrem + __popc(km) > remcap) {
+                bad = true;
+            } else if (keep) {
+                rem[nrem + __popc(km & lt)] = nd;
+            }
+            nrem += __popc(km);
+            const unsigned fm = __ballot_sync(FULL, far);
+            if (far) S.flist[nfar + __popc(fm & lt)] = nd;
+            nfar += __popc(fm);
+            __syncwarp();
+            if (nfar >= 64) {
+                far_add<2>(S.red, lane, S.flist, 64, cx, cy, cz, eps2, wA, wB, wC);
+                nF += 64;
+                const int v = S.flist[64 + lane];
+                __syncwarp();
+                if (lane + 64 < nfar) S.flist[lane] = v;
+                nfar -= 64;
+            }
+            const unsigned om = __ballot_sync(FULL, open);
+            const int npush = 2 * __popc(om);
+            if (sp + npush <= WSTK) {
+                if (open) {
+                    const int pos = sp + 2 * __popc(om & lt);
+                    S.stk[pos] = cr;
+                    S.stk[pos + 1] = cl;
+                }
+                sp += npush;
+            } else {
+                bad = true;
+            }
+            __syncwarp();
+        }
+        if (!bad) {
+            far_add<3>(S.red, lane, S.flist, nfar, cx, cy, cz, eps2, wA, wB, wC);
+            nF += nfar;
+            __syncwarp();
+            float *Ls = sgL + (size_t)s * SG_LSTRIDE;
+            for (int q = lane; q < NLOC; q += 32) {  // Kahan sum of the 32 lane columns
+                KSum<float> t;
+                for (int k = 0; k < 32; k++) t.add(S.red[q][k]);
+                Ls[q] = (float)t.value();
+            }
+            if (lane == 0) {
+                Ls[36] = cx;
+                Ls[37] = cy;
+                Ls[38] = cz;
+            }
+        }
+        if (lane == 0) {
+            nrem_out[s] = bad ? -1 : nrem;
+            if (bad) atomicAdd(&counters[4], 1ull);
+            else atomicAdd(&counters[3], (unsigned long long)nF);
+        }
+        __syncwarp();
+    }
 }
 
 // FP64 Plummer direct sum onto targets from all particles of the same cloud
@@ -655,12 +865,29 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
     int grid = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
     if (ctx->cfg.walk_blocks > 0) grid = min(grid, ctx->num_sms * ctx->cfg.walk_blocks);
     const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
+    SgArgs sg{};
+    if constexpr (std::is_same<R, float>::value) {
+        if (ctx->g_sg && ctx->cfg.theta_local > 0.0) {
+            const int sgrid = max(1, div_up(div_up(ctx->n, 64) + ctx->ncloud, WALK_WARPS));
+            k_sg_walk<POT><<<sgrid, WALK_WARPS * 32, 0, s>>>(
+                ctx->d_nsg, ctx->sg_cap, ctx->sg_start, ctx->sg_count, ctx->sg_cloud, ctx->croot,
+                (const float4 *)ctx->pw, (const float4 *)ctx->wA, (const float4 *)ctx->wB,
+                (const float4 *)ctx->wC, ctx->wL, eps2, (float)ctx->cfg.theta_local, ctx->sg_pool,
+                ctx->sg_nrem, ctx->sgL, ctx->counters);
+            sg.g_sg = ctx->g_sg;
+            sg.start = ctx->sg_start;
+            sg.nrem = ctx->sg_nrem;
+            sg.pool = ctx->sg_pool;
+            sg.L = ctx->sgL;
+            sg.cap = ctx->sg_cap;
+        }
+    }
     k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
         ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
         (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
         (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->wL,
         ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
-        ctx->work, ctx->counters, ctx->status, (float)ctx->cfg.theta_local);
+        ctx->work, ctx->counters, ctx->status, (float)ctx->cfg.theta_local, sg);
     return SPH_OK;
 }
 
@@ -668,7 +895,7 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
 
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot) {
     if (ctx->n <= 0) return SPH_OK;
-    CK(cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(ctx->counters, 0, 5 * sizeof(unsigned long long), s));
     int rc;
     if (ctx->cfg.precision == SPH_PREC_MIXED)
         rc = pot ? run_walk<float, true>(ctx, s) : run_walk<float, false>(ctx, s);

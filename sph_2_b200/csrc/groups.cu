@@ -115,6 +115,32 @@ __global__ void k_write_groups(int n, const int *__restrict__ mark, const int *_
     gnode[g] = nd;
 }
 
+// super-group table (no tree node output)
+__global__ void k_write_sgroups(int n, const int *__restrict__ mark, const int *__restrict__ pos,
+                                const int *__restrict__ node_at, const int *__restrict__ first,
+                                const int *__restrict__ last, const int *__restrict__ cloud,
+                                int *__restrict__ sstart, int *__restrict__ scount,
+                                int *__restrict__ scloud) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n || !mark[p]) return;
+    const int s = pos[p];
+    const int nd = node_at[p];
+    sstart[s] = p;
+    scount[s] = last[nd] - first[nd] + 1;
+    scloud[s] = cloud[p];
+}
+
+// super-group of each group: the last super-group starting at or before the
+// group's first particle (super-groups are unions of whole groups)
+__global__ void k_group_sg(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
+                           const int *__restrict__ smark, const int *__restrict__ spos,
+                           int *__restrict__ g_sg) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= *ngroup_p) return;
+    const int p = gstart[g];
+    g_sg[g] = spos[p] + smark[p] - 1;
+}
+
 }  // namespace
 
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total) {
@@ -141,6 +167,21 @@ int launch_groups(sph_ctx *ctx) {
                                                   ctx->first, ctx->last, ctx->cloud[ctx->cur],
                                                   ctx->gstart, ctx->gcount, ctx->groot_g,
                                                   ctx->gnode);
+    if (ctx->g_sg) {
+        // super-groups, in the marking arrays the group table no longer needs
+        CK(cudaMemsetAsync(ctx->gmark, 0, sizeof(int) * n, s));
+        k_mark_groups<<<div_up(2 * n - 1, 256), 256, 0, s>>>(n, ctx->first, ctx->last,
+                                                              ctx->parent, ctx->cloud[ctx->cur],
+                                                              SGROUP_MAX, ctx->gmark,
+                                                              ctx->gnode_at);
+        rc = launch_scan(ctx, ctx->gmark, ctx->gpos, n, ctx->d_nsg);
+        if (rc) return rc;
+        k_write_sgroups<<<div_up(n, 256), 256, 0, s>>>(n, ctx->gmark, ctx->gpos, ctx->gnode_at,
+                                                       ctx->first, ctx->last, ctx->cloud[ctx->cur],
+                                                       ctx->sg_start, ctx->sg_count, ctx->sg_cloud);
+        k_group_sg<<<div_up(n, 256), 256, 0, s>>>(n, ctx->d_ngroup, ctx->gstart, ctx->gmark,
+                                                  ctx->gpos, ctx->g_sg);
+    }
     return ctx_check_launch(ctx, "groups");
 }
 

@@ -91,6 +91,16 @@ struct sph_ctx {
     int *gmark = nullptr, *gpos = nullptr, *gnode_at = nullptr, *scan_tmp = nullptr;
     int *d_ngroup = nullptr;                    // number of groups (device)
     int ngroup = 0;                             // capacity of the group table
+    // super-groups of the mixed walk with group expansions (theta_local > 0):
+    // maximal tree nodes of at most SGROUP_MAX particles of one cloud, each
+    // walked once for the far cells common to its groups (null otherwise)
+    int *sg_start = nullptr, *sg_count = nullptr, *sg_cloud = nullptr;
+    int *d_nsg = nullptr;                       // number of super-groups (device)
+    int *g_sg = nullptr;                        // group -> super-group
+    int *sg_nrem = nullptr;                     // nodes left to the groups, -1: none (walk from the root)
+    int *sg_pool = nullptr;                     // those nodes, SG_POOL per particle from the first particle
+    float *sgL = nullptr;                       // per super-group: expansion coefficients and centre
+    int sg_cap = 0;                             // super-groups with an index below this have records
     bool tree_ok = false;
 
     // neighbours
@@ -246,6 +256,9 @@ __device__ __forceinline__ void status_add(long long *status, int which, long lo
 int launch_sort(sph_ctx *ctx);
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
 int launch_groups(sph_ctx *ctx);
+constexpr int SGROUP_MAX = 128;  // particles per super-group
+constexpr int SG_POOL = 8;       // node slots per particle of a super-group
+constexpr int SG_LSTRIDE = 40;   // floats per super-group record: 35 coefficients, pad, centre
 int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 int launch_tree(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);

@@ -322,6 +322,9 @@ def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
     assert plain["far_cells"] == 0
     st = ctx2.status()
     assert st["stack_overflow"] == 0 and 0 < st["walk_stack_max"] <= 512
+    # super-groups took the far cells their groups share, every one with a record
+    assert loc["sg_far_cells"] > 0 and loc["sg_fallback"] == 0
+    assert plain["sg_far_cells"] == 0
 
 
 # ------------------------------------------------- status / fault paths ----
