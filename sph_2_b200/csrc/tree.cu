@@ -144,15 +144,109 @@ __device__ __forceinline__ void combine(double *o, const double *a, const double
     }
 }
 
-// one thread per leaf climbs; the second child to finish combines its parent
+// the records of node nd from its combined moments o and h_max hm
 template <class R>
-__global__ void k_bottom_up(int n, const int *__restrict__ parent, const int *__restrict__ child,
-                            double *node, double *hmax, double *ropen2, double4 *sA, double4 *sB,
-                            int *flag, double theta, typename R4<R>::T *wA, typename R4<R>::T *wB,
+__device__ __forceinline__ void store_node(int nd, const double *o, double hm, double theta,
+                                           double *node, double *hmax, double *ropen2,
+                                           double4 *sA, double4 *sB, typename R4<R>::T *wA,
+                                           typename R4<R>::T *wB, typename R4<R>::T *wC) {
+    const double r2 = open_r2(o, theta);
+    double *dst = node + (size_t)16 * nd;
+    for (int q = 0; q < 16; q++) dst[q] = o[q];
+    hmax[nd] = hm;
+    ropen2[nd] = r2;
+    sA[nd] = make_double4(o[10], o[11], o[12], hm);
+    sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
+    write_walk<R>(nd, o, r2, hm, wA, wB, wC);
+}
+
+// the internal nodes inside each group: one warp per group combines them
+// bottom-up in shared memory, a node as soon as both children are done, each
+// with the left child first -- the same operations in the same order as the
+// climb, without its atomics.  A group of c >= 2 particles from s0 owns the
+// c - 1 internal nodes base .. base + c - 2 of the radix tree, base = s0 when
+// the group's node is s0 (a right child: its index is its first particle)
+// and s0 + 1 when it is s0 + c - 1 (a left child); every descendant's index
+// lies strictly inside the range.  The subtree is at most 31 levels deep, so
+// 32 rounds finish it; a round limit and a slot check guard the loop.
+constexpr int GUP_WARPS = 4;
+template <class R>
+__global__ void __launch_bounds__(GUP_WARPS * 32)
+    k_group_up(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
+               const int *__restrict__ gcount, const int *__restrict__ gnode,
+               const int *__restrict__ child, double *node, double *hmax, double *ropen2,
+               double4 *sA, double4 *sB, double theta, typename R4<R>::T *wA,
+               typename R4<R>::T *wB, typename R4<R>::T *wC, long long *status) {
+    __shared__ double rec[GUP_WARPS][32][17];
+    __shared__ double shm[GUP_WARPS][32];
+    __shared__ int rdy[GUP_WARPS][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = blockIdx.x * GUP_WARPS + w; g < ngroup; g += gridDim.x * GUP_WARPS) {
+        const int s0 = gstart[g], ni = gcount[g] - 1;
+        if (ni < 1) continue;  // a single particle: its leaf is the group's node
+        const int base = gnode[g] == s0 ? s0 : s0 + 1;
+        rdy[w][lane] = 0;
+        __syncwarp();
+        bool done = lane >= ni;
+        const int nd = base + lane;
+        int L = 0, Rc = 0;
+        if (!done) {
+            L = child[2 * nd];
+            Rc = child[2 * nd + 1];
+            // an internal child outside the group's slots cannot be waited for
+            const bool okL = L >= n - 1 || (L >= base && L - base < ni);
+            const bool okR = Rc >= n - 1 || (Rc >= base && Rc - base < ni);
+            if (!okL || !okR) {
+                status_add(status, SPH_S_STACK_OVERFLOW, 1);
+                done = true;
+            }
+        }
+        for (int round = 0; round < 32 && __any_sync(0xffffffffu, !done); round++) {
+            bool can = false;
+            if (!done) can = (L >= n - 1 || rdy[w][L - base]) && (Rc >= n - 1 || rdy[w][Rc - base]);
+            if (can) {
+                double a[16], b[16], o[16];
+                if (L >= n - 1) {
+                    for (int q = 0; q < 16; q++) a[q] = __ldcg(node + (size_t)16 * L + q);
+                } else {
+                    for (int q = 0; q < 16; q++) a[q] = rec[w][L - base][q];
+                }
+                if (Rc >= n - 1) {
+                    for (int q = 0; q < 16; q++) b[q] = __ldcg(node + (size_t)16 * Rc + q);
+                } else {
+                    for (int q = 0; q < 16; q++) b[q] = rec[w][Rc - base][q];
+                }
+                combine(o, a, b);
+                const double hl = L >= n - 1 ? __ldcg(hmax + L) : shm[w][L - base];
+                const double hr = Rc >= n - 1 ? __ldcg(hmax + Rc) : shm[w][Rc - base];
+                const double hm = fmax(hl, hr);
+                for (int q = 0; q < 16; q++) rec[w][lane][q] = o[q];
+                shm[w][lane] = hm;
+                store_node<R>(nd, o, hm, theta, node, hmax, ropen2, sA, sB, wA, wB, wC);
+                done = true;
+            }
+            __syncwarp();
+            if (can) rdy[w][lane] = 1;
+            __syncwarp();
+        }
+        if (__any_sync(0xffffffffu, !done) && lane == 0) status_add(status, SPH_S_STACK_OVERFLOW, 1);
+        __syncwarp();
+    }
+}
+
+// one thread per group climbs from the group's node; the second child to
+// finish combines its parent
+template <class R>
+__global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
+                            const int *__restrict__ gnode, const int *__restrict__ parent,
+                            const int *__restrict__ child, double *node, double *hmax,
+                            double *ropen2, double4 *sA, double4 *sB, int *flag, double theta,
+                            typename R4<R>::T *wA, typename R4<R>::T *wB,
                             typename R4<R>::T *wC) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n || n < 2) return;
-    int nd = parent[n - 1 + p];
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= *ngroup_p || n < 2) return;
+    int nd = parent[gnode[g]];
     while (nd >= 0) {
         // acquire-release on the arrival counter: the first thread's node
         // record is visible to the second, which combines the two
@@ -167,14 +261,7 @@ __global__ void k_bottom_up(int n, const int *__restrict__ parent, const int *__
         }
         combine(o, a, b);
         double hm = fmax(__ldcg(hmax + L), __ldcg(hmax + Rr));
-        double r2 = open_r2(o, theta);
-        double *dst = node + (size_t)16 * nd;
-        for (int q = 0; q < 16; q++) dst[q] = o[q];
-        hmax[nd] = hm;
-        ropen2[nd] = r2;
-        sA[nd] = make_double4(o[10], o[11], o[12], hm);
-        sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
-        write_walk<R>(nd, o, r2, hm, wA, wB, wC);
+        store_node<R>(nd, o, hm, theta, node, hmax, ropen2, sA, sB, wA, wB, wC);
         nd = parent[nd];
     }
 }
@@ -220,29 +307,43 @@ int launch_tree(sph_ctx *ctx) {
                                                     ctx->first, ctx->last, ctx->croot, ctx->wL);
     k_single_roots<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->cloud_start, ctx->ncloud, n,
                                                             ctx->croot);
-    // leaf records; the root has no parent
+    // the root has no parent
     CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
+    // leaf records (they complete the leaves' first / last the groups read),
+    // the groups, the nodes inside the groups, then the climb above them
     double4 *boxA = (double4 *)ctx->node_box;
     double4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
+    const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
+    int rc;
     if (mixed) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
             ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->wL);
+        if ((rc = launch_groups(ctx))) return rc;
+        k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->node,
+            ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB,
+            (float4 *)ctx->wC, ctx->status);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
-            ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
+            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
+            ctx->ropen2, boxA, boxB, ctx->flag, ctx->cfg.theta, (float4 *)ctx->wA,
+            (float4 *)ctx->wB, (float4 *)ctx->wC);
     } else {
         k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
             ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->wL);
+        if ((rc = launch_groups(ctx))) return rc;
+        k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->node,
+            ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB,
+            (double4 *)ctx->wC, ctx->status);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->parent, ctx->child, ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag,
-            ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
+            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
+            ctx->ropen2, boxA, boxB, ctx->flag, ctx->cfg.theta, (double4 *)ctx->wA,
+            (double4 *)ctx->wB, (double4 *)ctx->wC);
     }
-    int rc = launch_groups(ctx);
-    if (rc) return rc;
     ctx->tree_ok = true;
     return ctx_check_launch(ctx, "tree");
 }
