@@ -252,6 +252,7 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
         // record is visible to the second, which combines the two
         cuda::atomic_ref<int, cuda::thread_scope_device> arrived(flag[nd]);
         if (arrived.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
+        arrived.store(0, cuda::memory_order_relaxed);  // ready for the next pass
         int L = child[2 * nd], Rr = child[2 * nd + 1];
         double a[16], b[16], o[16];
         const double *pa = node + (size_t)16 * L, *pb = node + (size_t)16 * Rr;
@@ -268,23 +269,52 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
 
 // h_max refit after the smoothing lengths changed
 // need (may be null): skip the refit when *need == 0 (no tree search follows)
-__global__ void k_refit_leaves(int n, const double *__restrict__ h, double *hmax, double4 *sA,
-                               int *flag, const int *__restrict__ need) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n || (need && !*need)) return;
-    hmax[n - 1 + p] = h[p];
-    sA[n - 1 + p].w = h[p];
-    if (p < n - 1) flag[p] = 0;
+// The leaves and the internal nodes inside each group: one warp per group,
+// h of its particles in shared memory, each internal node the maximum over
+// its particle range (the same nodes as k_group_up)
+__global__ void __launch_bounds__(GUP_WARPS * 32)
+    k_refit_groups(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
+                   const int *__restrict__ gcount, const int *__restrict__ gnode,
+                   const int *__restrict__ first, const int *__restrict__ last,
+                   const double *__restrict__ h, double *hmax, double4 *sA,
+                   const int *__restrict__ need) {
+    __shared__ double sh[GUP_WARPS][32];
+    if (need && !*need) return;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = blockIdx.x * GUP_WARPS + w; g < ngroup; g += gridDim.x * GUP_WARPS) {
+        const int s0 = gstart[g], c = gcount[g];
+        if (lane < c) {
+            const double hp = h[s0 + lane];
+            sh[w][lane] = hp;
+            hmax[n - 1 + s0 + lane] = hp;
+            sA[n - 1 + s0 + lane].w = hp;
+        }
+        __syncwarp();
+        if (c >= 2 && lane < c - 1) {
+            const int nd = (gnode[g] == s0 ? s0 : s0 + 1) + lane;
+            const int f = max(first[nd] - s0, 0), l = min(last[nd] - s0, c - 1);
+            double hm = sh[w][f];
+            for (int k = f + 1; k <= l; k++) hm = fmax(hm, sh[w][k]);
+            hmax[nd] = hm;
+            sA[nd].w = hm;
+        }
+        __syncwarp();
+    }
 }
 
-__global__ void k_refit_up(int n, const int *__restrict__ parent, const int *__restrict__ child,
+// above the groups: one thread per group climbs from the group's node; the
+// second arrival combines and clears the counter for the next pass
+__global__ void k_refit_up(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gnode,
+                           const int *__restrict__ parent, const int *__restrict__ child,
                            double *hmax, double4 *sA, int *flag, const int *__restrict__ need) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n || n < 2 || (need && !*need)) return;
-    int nd = parent[n - 1 + p];
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= *ngroup_p || n < 2 || (need && !*need)) return;
+    int nd = parent[gnode[g]];
     while (nd >= 0) {
         cuda::atomic_ref<int, cuda::thread_scope_device> arrived(flag[nd]);
         if (arrived.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
+        arrived.store(0, cuda::memory_order_relaxed);
         double hm = fmax(__ldcg(hmax + child[2 * nd]), __ldcg(hmax + child[2 * nd + 1]));
         hmax[nd] = hm;
         sA[nd].w = hm;
@@ -353,9 +383,11 @@ int launch_refit_hmax(sph_ctx *ctx, const int *need) {
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     double4 *boxA = (double4 *)ctx->node_box;
-    k_refit_leaves<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[ctx->cur][ST_H], ctx->hmax, boxA,
-                                                  ctx->flag, need);
-    k_refit_up<<<div_up(n, 256), 256, 0, s>>>(n, ctx->parent, ctx->child, ctx->hmax, boxA,
-                                              ctx->flag, need);
+    const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
+    k_refit_groups<<<ggrid, GUP_WARPS * 32, 0, s>>>(n, ctx->d_ngroup, ctx->gstart, ctx->gcount,
+                                                    ctx->gnode, ctx->first, ctx->last,
+                                                    ctx->st[ctx->cur][ST_H], ctx->hmax, boxA, need);
+    k_refit_up<<<div_up(n, 256), 256, 0, s>>>(n, ctx->d_ngroup, ctx->gnode, ctx->parent,
+                                              ctx->child, ctx->hmax, boxA, ctx->flag, need);
     return ctx_check_launch(ctx, "refit");
 }
