@@ -171,14 +171,19 @@ __device__ __forceinline__ void store_node(int nd, const double *o, double hm, d
 // 32 rounds finish it; a round limit and a slot check guard the loop.
 constexpr int GUP_WARPS = 4;
 template <class R>
-__global__ void __launch_bounds__(GUP_WARPS * 32)
+__global__ void __launch_bounds__(GUP_WARPS * 32, 4)
     k_group_up(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
                const int *__restrict__ gcount, const int *__restrict__ gnode,
-               const int *__restrict__ child, double *node, double *hmax, double *ropen2,
-               double4 *sA, double4 *sB, double theta, typename R4<R>::T *wA,
-               typename R4<R>::T *wB, typename R4<R>::T *wC, long long *status) {
+               const int *__restrict__ child, const double *__restrict__ x,
+               const double *__restrict__ y, const double *__restrict__ z,
+               const double *__restrict__ m, const double *__restrict__ h, double *node,
+               double *hmax, double *ropen2, double4 *sA, double4 *sB, double theta,
+               typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC,
+               long long *status) {
     __shared__ double rec[GUP_WARPS][32][17];
     __shared__ double shm[GUP_WARPS][32];
+    __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
+        pm[GUP_WARPS][32], ph[GUP_WARPS][32];
     __shared__ int rdy[GUP_WARPS][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
@@ -187,6 +192,14 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
         if (ni < 1) continue;  // a single particle: its leaf is the group's node
         const int base = gnode[g] == s0 ? s0 : s0 + 1;
         rdy[w][lane] = 0;
+        // the group's particles (its leaves' records follow from them)
+        if (lane <= ni) {
+            px[w][lane] = x[s0 + lane];
+            py[w][lane] = y[s0 + lane];
+            pz[w][lane] = z[s0 + lane];
+            pm[w][lane] = m[s0 + lane];
+            ph[w][lane] = h[s0 + lane];
+        }
         __syncwarp();
         bool done = lane >= ni;
         const int nd = base + lane;
@@ -195,8 +208,10 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             L = child[2 * nd];
             Rc = child[2 * nd + 1];
             // an internal child outside the group's slots cannot be waited for
-            const bool okL = L >= n - 1 || (L >= base && L - base < ni);
-            const bool okR = Rc >= n - 1 || (Rc >= base && Rc - base < ni);
+            const bool okL = L >= n - 1 ? (L - (n - 1) - s0 >= 0 && L - (n - 1) - s0 <= ni)
+                                        : (L >= base && L - base < ni);
+            const bool okR = Rc >= n - 1 ? (Rc - (n - 1) - s0 >= 0 && Rc - (n - 1) - s0 <= ni)
+                                         : (Rc >= base && Rc - base < ni);
             if (!okL || !okR) {
                 status_add(status, SPH_S_STACK_OVERFLOW, 1);
                 done = true;
@@ -207,19 +222,28 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             if (!done) can = (L >= n - 1 || rdy[w][L - base]) && (Rc >= n - 1 || rdy[w][Rc - base]);
             if (can) {
                 double a[16], b[16], o[16];
+                // a leaf's record: com and box at the particle, its mass, no moments
+                auto leaf = [&](int c, double *r) {
+                    const int k = c - (n - 1) - s0;
+                    r[0] = r[10] = r[13] = px[w][k];
+                    r[1] = r[11] = r[14] = py[w][k];
+                    r[2] = r[12] = r[15] = pz[w][k];
+                    r[3] = pm[w][k];
+                    for (int q = 4; q < 10; q++) r[q] = 0.0;
+                };
                 if (L >= n - 1) {
-                    for (int q = 0; q < 16; q++) a[q] = __ldcg(node + (size_t)16 * L + q);
+                    leaf(L, a);
                 } else {
                     for (int q = 0; q < 16; q++) a[q] = rec[w][L - base][q];
                 }
                 if (Rc >= n - 1) {
-                    for (int q = 0; q < 16; q++) b[q] = __ldcg(node + (size_t)16 * Rc + q);
+                    leaf(Rc, b);
                 } else {
                     for (int q = 0; q < 16; q++) b[q] = rec[w][Rc - base][q];
                 }
                 combine(o, a, b);
-                const double hl = L >= n - 1 ? __ldcg(hmax + L) : shm[w][L - base];
-                const double hr = Rc >= n - 1 ? __ldcg(hmax + Rc) : shm[w][Rc - base];
+                const double hl = L >= n - 1 ? ph[w][L - (n - 1) - s0] : shm[w][L - base];
+                const double hr = Rc >= n - 1 ? ph[w][Rc - (n - 1) - s0] : shm[w][Rc - base];
                 const double hm = fmax(hl, hr);
                 for (int q = 0; q < 16; q++) rec[w][lane][q] = o[q];
                 shm[w][lane] = hm;
@@ -352,7 +376,8 @@ int launch_tree(sph_ctx *ctx) {
             ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->node,
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
+            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
             ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB,
             (float4 *)ctx->wC, ctx->status);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
@@ -366,7 +391,8 @@ int launch_tree(sph_ctx *ctx) {
             ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->node,
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
+            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
             ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB,
             (double4 *)ctx->wC, ctx->status);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
