@@ -40,9 +40,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--theta", type=float, default=0.38)
+    ap.add_argument("--theta", type=float, default=0.36, help="opening angle, mixed arm")
+    ap.add_argument("--theta-fp64", type=float, default=0.38, help="opening angle, FP64 plain arm")
     ap.add_argument("--theta-local", type=float, default=0.25,
                     help="mixed walk: far cells through group Taylor expansions (0: off)")
+    ap.add_argument("--theta-small", type=float, default=0.45,
+                    help="mixed walk: opening angle of the cells of at most --small-cell particles")
+    ap.add_argument("--small-cell", type=int, default=128)
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
@@ -234,6 +238,15 @@ def rms_rel(a, b):
     return float(np.sqrt(np.mean(num / den)))
 
 
+def walk_kw(a, precision):
+    """Opening-angle settings of one arm: the mixed arm with its group
+    expansions and small-cell angle, the FP64 plain arm with theta alone."""
+    if precision == "mixed":
+        return dict(theta=a.theta, theta_local=a.theta_local, theta_small=a.theta_small,
+                    small_cell=a.small_cell)
+    return dict(theta=a.theta_fp64)
+
+
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -273,9 +286,8 @@ def main():
     stream = torch.cuda.Stream(priority=-10)
 
     def make(precision, flags=0, vel=None):
-        cfg = Config(n_max=n, precision=precision, theta=a.theta, leaf_size=a.leaf,
-                     ngb_lanes=a.lanes, flags=flags,
-                     theta_local=a.theta_local if precision == "mixed" else 0.0)
+        cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf,
+                     ngb_lanes=a.lanes, flags=flags, **walk_kw(a, precision))
         c = Context(cfg)
         c.set_stream(stream.cuda_stream)
         c.load(d["pos"], d["vel"] if vel is None else vel, d["m"], d["h"], d["u"])
@@ -475,7 +487,9 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64 (mixed)",
         "data": "synthetic (seeded Evrard sphere, numpy default_rng)",
         "config": {"workload": "evrard_1M_mixed" if n == 1_000_000 else f"evrard_{n}_mixed",
-                   "n": n, "theta": a.theta, "theta_local_mixed": a.theta_local,
+                   "n": n, "theta_mixed": a.theta, "theta_fp64": a.theta_fp64,
+                   "theta_local_mixed": a.theta_local, "theta_small_mixed": a.theta_small,
+                   "small_cell_mixed": a.small_cell,
                    "leaf_size": a.leaf, "ngb_lanes": a.lanes,
                    "n_ngb": 64, "eps": 1e-2, "av": "monaghan-gingold alpha=1 beta=2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -524,9 +538,8 @@ def large_evrard(a, stream, timed):
     res = {}
     for arm, prec, mlp in (("mixed_mlp", "mixed", True), ("fp64_exact", "fp64", False)):
         flags = L.FLAG_COOLING | L.FLAG_TIMING | L.FLAG_POTENTIAL | (L.FLAG_COOLING_MLP if mlp else 0)
-        ctx = Context(Config(n_max=n, precision=prec, theta=a.theta, leaf_size=a.leaf,
-                             ngb_lanes=a.lanes, flags=flags,
-                             theta_local=a.theta_local if prec == "mixed" else 0.0))
+        ctx = Context(Config(n_max=n, precision=prec, leaf_size=a.leaf,
+                             ngb_lanes=a.lanes, flags=flags, **walk_kw(a, prec)))
         ctx.set_stream(stream.cuda_stream)
         cooling.setup(ctx, units)
         if mlp:
@@ -609,8 +622,7 @@ def extra_workload(a, world, rank, local):
         mine = local_ensemble(e, owner, rank)
         n = len(mine["m"])
         ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
-                             theta=a.theta, leaf_size=a.leaf, ngb_lanes=a.lanes,
-                             theta_local=a.theta_local))
+                             leaf_size=a.leaf, ngb_lanes=a.lanes, **walk_kw(a, "mixed")))
         ctx.set_stream(stream.cuda_stream)
         ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
         ctx.prologue()
@@ -633,9 +645,8 @@ def extra_workload(a, world, rank, local):
         res = {}
         for mode in ("exact", "mlp"):
             flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
-            ctx = Context(Config(n_max=n, precision="mixed", theta=a.theta, leaf_size=a.leaf,
-                                 theta_local=a.theta_local,
-                                 flags=flags))
+            ctx = Context(Config(n_max=n, precision="mixed", leaf_size=a.leaf,
+                                 flags=flags, **walk_kw(a, "mixed")))
             ctx.set_stream(stream.cuda_stream)
             cooling.setup(ctx, d["units"])
             if mode == "mlp":

@@ -123,9 +123,18 @@ typedef struct sph_config {
     double dt_max;        /* upper bound on dt (0: none)                          */
     double dt_fixed;      /* >0: fixed step (reference drivers), no Courant dt    */
     double theta_local;   /* mixed-precision walk: accepted cells farther than
-                             R_g / theta_local from a group's centre (R_g its
-                             radius) enter a second-order Taylor expansion at
-                             the centre, once per group; 0: off              */
+                             R / theta_local from a group's or super-group's
+                             centre (R its radius) enter a Taylor expansion at
+                             that centre (monopole and quadrupole field and
+                             gradient, monopole terms to third order), once
+                             per group or super-group; 0: off                 */
+    double theta_small;   /* opening angle of the cells of at most small_cell
+                             particles (their mass is small, so their
+                             truncation error is too); 0: theta for all cells */
+    int32_t small_cell;   /* see theta_small; the error it adds follows the
+                             cells' mass fraction: 128 was tuned at N = 1M
+                             (theta 0.36, theta_small 0.45), scale it with N  */
+    int32_t reserved0;    /* 0                                                 */
 } sph_config;
 
 typedef struct sph_ctx sph_ctx;

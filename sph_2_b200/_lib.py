@@ -49,6 +49,7 @@ class SphConfig(C.Structure):
         ("alpha", C.c_double), ("beta", C.c_double), ("eta", C.c_double), ("G", C.c_double),
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),
         ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
+        ("theta_small", C.c_double), ("small_cell", C.c_int32), ("reserved0", C.c_int32),
     ]
 
 

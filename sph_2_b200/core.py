@@ -47,6 +47,9 @@ class Config:
     dt_max: float = 0.0
     dt_fixed: float = 0.0
     theta_local: float = 0.0
+    theta_small: float = 0.0
+    small_cell: int = 0
+    reserved0: int = 0
 
     def to_c(self) -> L.SphConfig:
         c = L.SphConfig()

@@ -85,6 +85,7 @@ int check_cfg(const sph_config *c) {
     if (c->h_max_iter < 1 || c->h_max_iter > 1000) return SPH_ERR_ARG;
     if (!(c->theta > 0.0 && c->theta <= 1.0)) return SPH_ERR_ARG;
     if (!(c->theta_local >= 0.0 && c->theta_local < 1.0)) return SPH_ERR_ARG;
+    if (!(c->theta_small >= 0.0 && c->theta_small < 1.0) || c->small_cell < 0) return SPH_ERR_ARG;
     if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
     if (!(c->courant > 0.0)) return SPH_ERR_ARG;
     return SPH_OK;
@@ -401,9 +402,12 @@ int sph_set_params(sph_ctx *ctx, const sph_config *c) {
     t.dt_max = c->dt_max; t.dt_fixed = c->dt_fixed;
     t.ngb_lanes = c->ngb_lanes; t.block_size = c->block_size; t.leaf_size = c->leaf_size;
     t.walk_blocks = c->walk_blocks;
+    t.theta_small = c->theta_small; t.small_cell = c->small_cell;
     int rc = check_cfg(&t);
     if (rc) return rc;
-    if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size) ctx->tree_ok = false;
+    if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size ||
+        t.theta_small != ctx->cfg.theta_small || t.small_cell != ctx->cfg.small_cell)
+        ctx->tree_ok = false;
     ctx->cfg = t;
     drop_graphs(ctx);
     ctx->p2_dirty = true;

@@ -144,6 +144,15 @@ __device__ __forceinline__ void combine(double *o, const double *a, const double
     }
 }
 
+// opening angles: theta_small for the cells of at most small_cell particles
+struct Opening {
+    double theta, theta_small;
+    int small_cell;
+    __device__ __forceinline__ double at(int count) const {
+        return theta_small > 0.0 && count <= small_cell ? theta_small : theta;
+    }
+};
+
 // the records of node nd from its combined moments o and h_max hm
 template <class R>
 __device__ __forceinline__ void store_node(int nd, const double *o, double hm, double theta,
@@ -177,9 +186,9 @@ __global__ void __launch_bounds__(GUP_WARPS * 32, 4)
                const int *__restrict__ child, const double *__restrict__ x,
                const double *__restrict__ y, const double *__restrict__ z,
                const double *__restrict__ m, const double *__restrict__ h, double *node,
-               double *hmax, double *ropen2, double4 *sA, double4 *sB, double theta,
-               typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC,
-               long long *status) {
+               double *hmax, double *ropen2, double4 *sA, double4 *sB, Opening op,
+               const int4 *__restrict__ wL, typename R4<R>::T *wA, typename R4<R>::T *wB,
+               typename R4<R>::T *wC, long long *status) {
     __shared__ double rec[GUP_WARPS][32][17];
     __shared__ double shm[GUP_WARPS][32];
     __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
@@ -247,7 +256,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32, 4)
                 const double hm = fmax(hl, hr);
                 for (int q = 0; q < 16; q++) rec[w][lane][q] = o[q];
                 shm[w][lane] = hm;
-                store_node<R>(nd, o, hm, theta, node, hmax, ropen2, sA, sB, wA, wB, wC);
+                store_node<R>(nd, o, hm, op.at(wL[nd].y), node, hmax, ropen2, sA, sB, wA, wB, wC);
                 done = true;
             }
             __syncwarp();
@@ -265,9 +274,9 @@ template <class R>
 __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
                             const int *__restrict__ gnode, const int *__restrict__ parent,
                             const int *__restrict__ child, double *node, double *hmax,
-                            double *ropen2, double4 *sA, double4 *sB, int *flag, double theta,
-                            typename R4<R>::T *wA, typename R4<R>::T *wB,
-                            typename R4<R>::T *wC) {
+                            double *ropen2, double4 *sA, double4 *sB, int *flag, Opening op,
+                            const int4 *__restrict__ wL, typename R4<R>::T *wA,
+                            typename R4<R>::T *wB, typename R4<R>::T *wC) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= *ngroup_p || n < 2) return;
     int nd = parent[gnode[g]];
@@ -286,7 +295,7 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
         }
         combine(o, a, b);
         double hm = fmax(__ldcg(hmax + L), __ldcg(hmax + Rr));
-        store_node<R>(nd, o, hm, theta, node, hmax, ropen2, sA, sB, wA, wB, wC);
+        store_node<R>(nd, o, hm, op.at(wL[nd].y), node, hmax, ropen2, sA, sB, wA, wB, wC);
         nd = parent[nd];
     }
 }
@@ -368,6 +377,7 @@ int launch_tree(sph_ctx *ctx) {
     double4 *boxA = (double4 *)ctx->node_box;
     double4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
     const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
+    const Opening op{ctx->cfg.theta, ctx->cfg.theta_small, ctx->cfg.small_cell};
     int rc;
     if (mixed) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
@@ -378,11 +388,11 @@ int launch_tree(sph_ctx *ctx) {
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
-            ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (float4 *)ctx->wA, (float4 *)ctx->wB,
+            ctx->hmax, ctx->ropen2, boxA, boxB, op, ctx->wL, (float4 *)ctx->wA, (float4 *)ctx->wB,
             (float4 *)ctx->wC, ctx->status);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
-            ctx->ropen2, boxA, boxB, ctx->flag, ctx->cfg.theta, (float4 *)ctx->wA,
+            ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (float4 *)ctx->wA,
             (float4 *)ctx->wB, (float4 *)ctx->wC);
     } else {
         k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
@@ -393,11 +403,11 @@ int launch_tree(sph_ctx *ctx) {
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
-            ctx->hmax, ctx->ropen2, boxA, boxB, ctx->cfg.theta, (double4 *)ctx->wA, (double4 *)ctx->wB,
+            ctx->hmax, ctx->ropen2, boxA, boxB, op, ctx->wL, (double4 *)ctx->wA, (double4 *)ctx->wB,
             (double4 *)ctx->wC, ctx->status);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
-            ctx->ropen2, boxA, boxB, ctx->flag, ctx->cfg.theta, (double4 *)ctx->wA,
+            ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (double4 *)ctx->wA,
             (double4 *)ctx->wB, (double4 *)ctx->wC);
     }
     ctx->tree_ok = true;

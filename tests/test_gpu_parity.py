@@ -327,6 +327,29 @@ def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
     assert plain["sg_far_cells"] == 0
 
 
+def test_gravity_small_cell_opening_angle():
+    """A wider opening angle for the small cells (their mass, hence their
+    truncation error, is small: at most 26 particles of 200k here, the mass
+    fraction of 128 particles at N = 1M) trades bucket particles for cell
+    interactions; with the main angle lowered to 0.36 the error against the
+    FP64 direct sum stays at the level of the single-angle walk."""
+    n = 200000
+    ctx, d = prepared(n, "mixed", theta=0.38, theta_local=0.25)
+    ctx.gravity()
+    base = ctx.counters()
+    tg = np.random.default_rng(0).choice(n, 2000, replace=False).astype(np.int32)
+    ad, _ = ctx.gravity_direct(tg)
+    e_base = rms_rel(ctx.get_acc("grav", True)[tg], ad)
+    ctx2, _ = prepared(n, "mixed", theta=0.36, theta_local=0.25, theta_small=0.45, small_cell=26)
+    ctx2.gravity()
+    sm = ctx2.counters()
+    e_sm = rms_rel(ctx2.get_acc("grav", True)[tg], ad)
+    assert sm["particles"] < 0.85 * base["particles"]
+    assert e_sm < 1.6e-4 and e_sm < 1.15 * e_base
+    with pytest.raises(Exception):
+        prepared(1000, "mixed", theta_small=1.5, small_cell=128)
+
+
 # ------------------------------------------------- status / fault paths ----
 def test_status_counters_without_faults():
     # iteration cap of 1: the h iteration reports non-convergence, no fault
