@@ -40,9 +40,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--theta", type=float, default=0.36, help="opening angle, mixed arm")
+    ap.add_argument("--theta", type=float, default=0.35, help="opening angle, mixed arm")
     ap.add_argument("--theta-fp64", type=float, default=0.38, help="opening angle, FP64 plain arm")
-    ap.add_argument("--theta-local", type=float, default=0.25,
+    ap.add_argument("--theta-local", type=float, default=0.28,
                     help="mixed walk: far cells through group Taylor expansions (0: off)")
     ap.add_argument("--theta-small", type=float, default=0.45,
                     help="mixed walk: opening angle of the cells of at most --small-cell particles")
