@@ -60,7 +60,8 @@ def lib():
             "orc_force_list": [I] + [f64p] * 13 + [D, D, D, I, I, i64p, i32p, vp, vp, vp, vp, vp],
             "orc_grav_direct": [I, f64p, f64p, f64p, f64p, vp, D, D, I, i32p, f64p, f64p, f64p, vp],
             "orc_build_radix_tree": [I, u64p, i32p, i32p, i32p, i32p],
-            "orc_tree_moments": [I, i32p, f64p, f64p, f64p, f64p, f64p, f64p, f64p],
+            "orc_tree_moments": [I, i32p, i32p, i32p, C.c_void_p, f64p, f64p, f64p, f64p, f64p,
+                                 f64p, f64p],
             "orc_open_r2": [I, f64p, D, f64p],
             "orc_walk": [I, f64p, f64p, f64p, f64p, i32p, i32p, i32p, f64p, f64p, I, i32p, i32p, i32p,
                          I, D, D, f64p, f64p, f64p, vp, vp, vp],
@@ -309,12 +310,19 @@ def build_radix_tree(keys):
     return child, parent, first, last
 
 
-def tree_moments(child, x, y, z, m, h):
+def tree_moments(child, first, last, x, y, z, m, h, cloud=None):
+    """FP64 node records: nodes of at most 32 particles of one cloud (inside
+    a walk group) summed directly over their particle range, larger ones
+    combined from their children, left first (project method; the reference
+    octree accumulates masses with atomics, bh_tree_iteration_v2.h:149-367)."""
     n = len(x)
     nn = 2 * n - 1
     node = np.zeros(16 * nn)
     hmax = np.zeros(nn)
-    lib().orc_tree_moments(n, _c(child, np.int32), _c(x), _c(y), _c(z), _c(m), _c(h), node, hmax)
+    cl = None if cloud is None else _c(cloud, np.int32)
+    lib().orc_tree_moments(n, _c(child, np.int32), _c(first, np.int32), _c(last, np.int32),
+                           None if cl is None else cl.ctypes.data_as(C.c_void_p), _c(x), _c(y),
+                           _c(z), _c(m), _c(h), node, hmax)
     return node.reshape(nn, 16), hmax
 
 
@@ -365,9 +373,9 @@ def bh_walk(x, y, z, m, h, keys_sorted, theta, eps, G=1.0, leaf_size=16, group_s
     if cloud_start is None:
         cloud_start = np.array([0, n], np.int32)
     child, parent, first, last = build_radix_tree(keys_sorted)
-    node, hmax = tree_moments(child, x, y, z, m, h)
-    r2 = open_r2(node, theta)
     cloud = np.repeat(np.arange(len(cloud_start) - 1), np.diff(cloud_start))
+    node, hmax = tree_moments(child, first, last, x, y, z, m, h, cloud)
+    r2 = open_r2(node, theta)
     gs, gc, gk = tree_groups(first, last, parent, cloud, group_size)
     roots = cloud_roots(first, last, cloud_start, n)
     groot = roots[gk].astype(np.int32)

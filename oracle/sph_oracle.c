@@ -746,7 +746,37 @@ static void combine(double *o, const double *a, const double *b)
     for (int d = 0; d < 3; d++) { o[10 + d] = fmin(a[10 + d], b[10 + d]); o[13 + d] = fmax(a[13 + d], b[13 + d]); }
 }
 
-void orc_tree_moments(int N, const int *child, const double *x, const double *y, const double *z,
+/* Moments of a node of at most GROUP_DIRECT particles of one cloud (a node
+ * inside a walk group) summed directly over its particle range f..l in
+ * index order: mass, com = sum(m x) / M, second moments sum((m d_a) d_b)
+ * about the com, box.  Larger nodes combine their children. */
+#define GROUP_DIRECT 32
+static void direct_moments(double *o, int f, int l, const double *x, const double *y,
+                           const double *z, const double *m)
+{
+    double M = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    double lo[3] = {x[f], y[f], z[f]}, hi[3] = {x[f], y[f], z[f]};
+    for (int p = f; p <= l; p++) {
+        M = M + m[p];
+        sx = sx + m[p] * x[p]; sy = sy + m[p] * y[p]; sz = sz + m[p] * z[p];
+        lo[0] = fmin(lo[0], x[p]); lo[1] = fmin(lo[1], y[p]); lo[2] = fmin(lo[2], z[p]);
+        hi[0] = fmax(hi[0], x[p]); hi[1] = fmax(hi[1], y[p]); hi[2] = fmax(hi[2], z[p]);
+    }
+    const double cx = sx / M, cy = sy / M, cz = sz / M;
+    double qxx = 0.0, qyy = 0.0, qzz = 0.0, qxy = 0.0, qxz = 0.0, qyz = 0.0;
+    for (int p = f; p <= l; p++) {
+        const double dx = x[p] - cx, dy = y[p] - cy, dz = z[p] - cz;
+        const double tx = m[p] * dx, ty = m[p] * dy, tz = m[p] * dz;
+        qxx = qxx + tx * dx; qxy = qxy + tx * dy; qxz = qxz + tx * dz;
+        qyy = qyy + ty * dy; qyz = qyz + ty * dz; qzz = qzz + tz * dz;
+    }
+    o[0] = cx; o[1] = cy; o[2] = cz; o[3] = M;
+    o[4] = qxx; o[5] = qyy; o[6] = qzz; o[7] = qxy; o[8] = qxz; o[9] = qyz;
+    for (int d = 0; d < 3; d++) { o[10 + d] = lo[d]; o[13 + d] = hi[d]; }
+}
+
+void orc_tree_moments(int N, const int *child, const int *first, const int *last, const int *cloud,
+                      const double *x, const double *y, const double *z,
                       const double *m, const double *h, double *node, double *hmax)
 {
     int nn = 2 * N - 1;
@@ -772,7 +802,10 @@ void orc_tree_moments(int N, const int *child, const double *x, const double *y,
             if (lpend) stack[sp++] = L;
             continue;
         }
-        combine(node + (size_t)NREC * n, node + (size_t)NREC * L, node + (size_t)NREC * R);
+        if (last[n] - first[n] + 1 <= GROUP_DIRECT && (!cloud || cloud[first[n]] == cloud[last[n]]))
+            direct_moments(node + (size_t)NREC * n, first[n], last[n], x, y, z, m);
+        else
+            combine(node + (size_t)NREC * n, node + (size_t)NREC * L, node + (size_t)NREC * R);
         hmax[n] = fmax(hmax[L], hmax[R]);
         done[n] = 1;
         sp--;

@@ -169,40 +169,34 @@ __device__ __forceinline__ void store_node(int nd, const double *o, double hm, d
     write_walk<R>(nd, o, r2, hm, wA, wB, wC);
 }
 
-// the internal nodes inside each group: one warp per group combines them
-// bottom-up in shared memory, a node as soon as both children are done, each
-// with the left child first -- the same operations in the same order as the
-// climb, without its atomics.  A group of c >= 2 particles from s0 owns the
-// c - 1 internal nodes base .. base + c - 2 of the radix tree, base = s0 when
-// the group's node is s0 (a right child: its index is its first particle)
-// and s0 + 1 when it is s0 + c - 1 (a left child); every descendant's index
-// lies strictly inside the range.  The subtree is at most 31 levels deep, so
-// 32 rounds finish it; a round limit and a slot check guard the loop.
+// the internal nodes inside each group (the nodes of at most 32 particles of
+// one cloud): one warp per group, the group's particles in shared memory,
+// each lane one internal node summed directly over its particle range in
+// index order -- mass, com = sum(m x) / M, second moments sum((m d_a) d_b)
+// about the com, box -- the oracle's direct_moments.  A group of c >= 2
+// particles from s0 owns the c - 1 internal nodes base .. base + c - 2 of
+// the radix tree, base = s0 when the group's node is s0 (a right child: its
+// index is its first particle) and s0 + 1 when it is s0 + c - 1 (a left
+// child); every descendant's index lies strictly inside the range.
 constexpr int GUP_WARPS = 4;
 template <class R>
-__global__ void __launch_bounds__(GUP_WARPS * 32, 4)
+__global__ void __launch_bounds__(GUP_WARPS * 32)
     k_group_up(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
                const int *__restrict__ gcount, const int *__restrict__ gnode,
-               const int *__restrict__ child, const double *__restrict__ x,
-               const double *__restrict__ y, const double *__restrict__ z,
-               const double *__restrict__ m, const double *__restrict__ h, double *node,
-               double *hmax, double *ropen2, double4 *sA, double4 *sB, Opening op,
-               const int4 *__restrict__ wL, typename R4<R>::T *wA, typename R4<R>::T *wB,
-               typename R4<R>::T *wC, long long *status) {
-    __shared__ double rec[GUP_WARPS][32][17];
-    __shared__ double shm[GUP_WARPS][32];
+               const int *__restrict__ first, const int *__restrict__ last,
+               const double *__restrict__ x, const double *__restrict__ y,
+               const double *__restrict__ z, const double *__restrict__ m,
+               const double *__restrict__ h, double *node, double *hmax, double *ropen2,
+               double4 *sA, double4 *sB, Opening op, typename R4<R>::T *wA,
+               typename R4<R>::T *wB, typename R4<R>::T *wC) {
     __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
         pm[GUP_WARPS][32], ph[GUP_WARPS][32];
-    __shared__ int rdy[GUP_WARPS][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
     for (int g = blockIdx.x * GUP_WARPS + w; g < ngroup; g += gridDim.x * GUP_WARPS) {
-        const int s0 = gstart[g], ni = gcount[g] - 1;
-        if (ni < 1) continue;  // a single particle: its leaf is the group's node
-        const int base = gnode[g] == s0 ? s0 : s0 + 1;
-        rdy[w][lane] = 0;
-        // the group's particles (its leaves' records follow from them)
-        if (lane <= ni) {
+        const int s0 = gstart[g], c = gcount[g];
+        if (c < 2) continue;  // a single particle: its leaf is the group's node
+        if (lane < c) {
             px[w][lane] = x[s0 + lane];
             py[w][lane] = y[s0 + lane];
             pz[w][lane] = z[s0 + lane];
@@ -210,60 +204,39 @@ __global__ void __launch_bounds__(GUP_WARPS * 32, 4)
             ph[w][lane] = h[s0 + lane];
         }
         __syncwarp();
-        bool done = lane >= ni;
-        const int nd = base + lane;
-        int L = 0, Rc = 0;
-        if (!done) {
-            L = child[2 * nd];
-            Rc = child[2 * nd + 1];
-            // an internal child outside the group's slots cannot be waited for
-            const bool okL = L >= n - 1 ? (L - (n - 1) - s0 >= 0 && L - (n - 1) - s0 <= ni)
-                                        : (L >= base && L - base < ni);
-            const bool okR = Rc >= n - 1 ? (Rc - (n - 1) - s0 >= 0 && Rc - (n - 1) - s0 <= ni)
-                                         : (Rc >= base && Rc - base < ni);
-            if (!okL || !okR) {
-                status_add(status, SPH_S_STACK_OVERFLOW, 1);
-                done = true;
+        if (lane < c - 1) {
+            const int nd = (gnode[g] == s0 ? s0 : s0 + 1) + lane;
+            const int f = max(first[nd] - s0, 0), l = min(last[nd] - s0, c - 1);
+            double M = 0.0, sx = 0.0, sy = 0.0, sz = 0.0, hm = ph[w][f];
+            double o[16];
+            o[10] = o[13] = px[w][f];
+            o[11] = o[14] = py[w][f];
+            o[12] = o[15] = pz[w][f];
+            for (int k = f; k <= l; k++) {
+                const double xk = px[w][k], yk = py[w][k], zk = pz[w][k], mk = pm[w][k];
+                M = xadd(M, mk);
+                sx = xadd(sx, xmul(mk, xk));
+                sy = xadd(sy, xmul(mk, yk));
+                sz = xadd(sz, xmul(mk, zk));
+                o[10] = fmin(o[10], xk); o[11] = fmin(o[11], yk); o[12] = fmin(o[12], zk);
+                o[13] = fmax(o[13], xk); o[14] = fmax(o[14], yk); o[15] = fmax(o[15], zk);
+                hm = fmax(hm, ph[w][k]);
             }
-        }
-        for (int round = 0; round < 32 && __any_sync(0xffffffffu, !done); round++) {
-            bool can = false;
-            if (!done) can = (L >= n - 1 || rdy[w][L - base]) && (Rc >= n - 1 || rdy[w][Rc - base]);
-            if (can) {
-                double a[16], b[16], o[16];
-                // a leaf's record: com and box at the particle, its mass, no moments
-                auto leaf = [&](int c, double *r) {
-                    const int k = c - (n - 1) - s0;
-                    r[0] = r[10] = r[13] = px[w][k];
-                    r[1] = r[11] = r[14] = py[w][k];
-                    r[2] = r[12] = r[15] = pz[w][k];
-                    r[3] = pm[w][k];
-                    for (int q = 4; q < 10; q++) r[q] = 0.0;
-                };
-                if (L >= n - 1) {
-                    leaf(L, a);
-                } else {
-                    for (int q = 0; q < 16; q++) a[q] = rec[w][L - base][q];
-                }
-                if (Rc >= n - 1) {
-                    leaf(Rc, b);
-                } else {
-                    for (int q = 0; q < 16; q++) b[q] = rec[w][Rc - base][q];
-                }
-                combine(o, a, b);
-                const double hl = L >= n - 1 ? ph[w][L - (n - 1) - s0] : shm[w][L - base];
-                const double hr = Rc >= n - 1 ? ph[w][Rc - (n - 1) - s0] : shm[w][Rc - base];
-                const double hm = fmax(hl, hr);
-                for (int q = 0; q < 16; q++) rec[w][lane][q] = o[q];
-                shm[w][lane] = hm;
-                store_node<R>(nd, o, hm, op.at(wL[nd].y), node, hmax, ropen2, sA, sB, wA, wB, wC);
-                done = true;
+            const double cx = xdiv(sx, M), cy = xdiv(sy, M), cz = xdiv(sz, M);
+            double qxx = 0.0, qyy = 0.0, qzz = 0.0, qxy = 0.0, qxz = 0.0, qyz = 0.0;
+            for (int k = f; k <= l; k++) {
+                const double dx = xsub(px[w][k], cx), dy = xsub(py[w][k], cy),
+                             dz = xsub(pz[w][k], cz);
+                const double mk = pm[w][k];
+                const double tx = xmul(mk, dx), ty = xmul(mk, dy), tz = xmul(mk, dz);
+                qxx = xadd(qxx, xmul(tx, dx)); qxy = xadd(qxy, xmul(tx, dy));
+                qxz = xadd(qxz, xmul(tx, dz)); qyy = xadd(qyy, xmul(ty, dy));
+                qyz = xadd(qyz, xmul(ty, dz)); qzz = xadd(qzz, xmul(tz, dz));
             }
-            __syncwarp();
-            if (can) rdy[w][lane] = 1;
-            __syncwarp();
+            o[0] = cx; o[1] = cy; o[2] = cz; o[3] = M;
+            o[4] = qxx; o[5] = qyy; o[6] = qzz; o[7] = qxy; o[8] = qxz; o[9] = qyz;
+            store_node<R>(nd, o, hm, op.at(l - f + 1), node, hmax, ropen2, sA, sB, wA, wB, wC);
         }
-        if (__any_sync(0xffffffffu, !done) && lane == 0) status_add(status, SPH_S_STACK_OVERFLOW, 1);
         __syncwarp();
     }
 }
@@ -386,10 +359,10 @@ int launch_tree(sph_ctx *ctx) {
             ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
-            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
-            ctx->hmax, ctx->ropen2, boxA, boxB, op, ctx->wL, (float4 *)ctx->wA, (float4 *)ctx->wB,
-            (float4 *)ctx->wC, ctx->status);
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
+            ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
+            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
+            (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (float4 *)ctx->wA,
@@ -401,10 +374,10 @@ int launch_tree(sph_ctx *ctx) {
             ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->child, ctx->st[c][ST_X],
-            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->st[c][ST_H], ctx->node,
-            ctx->hmax, ctx->ropen2, boxA, boxB, op, ctx->wL, (double4 *)ctx->wA, (double4 *)ctx->wB,
-            (double4 *)ctx->wC, ctx->status);
+            n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
+            ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
+            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
+            (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (double4 *)ctx->wA,

@@ -96,7 +96,7 @@ def test_tree_nodes_bitexact(precision):
     keys, _ = ctx.sort_info()
     ks = np.sort(keys)
     child, parent, first, last = O.build_radix_tree(ks)
-    node, hmax = O.tree_moments(child, x, y, z, m, h)
+    node, hmax = O.tree_moments(child, first, last, x, y, z, m, h)
     assert np.array_equal(t["child"], child)
     assert np.array_equal(t["first"], first)
     assert np.array_equal(t["last"], last)
