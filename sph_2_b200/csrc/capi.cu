@@ -611,7 +611,10 @@ int sph_get_tree(sph_ctx *ctx, double *node, int32_t *child, int32_t *first, int
     if (nn == 0) return SPH_OK;
     cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     cudaStream_t s = ctx->stream;
-    if (node) CK(cudaMemcpyAsync(node, ctx->node, 16 * sizeof(double) * nn, k, s));
+    if (node) {
+        if ((rc = launch_leaf_records(ctx))) return rc;
+        CK(cudaMemcpyAsync(node, ctx->node, 16 * sizeof(double) * nn, k, s));
+    }
     if (child) CK(cudaMemcpyAsync(child, ctx->child, 2 * sizeof(int) * nn, k, s));
     if (first) CK(cudaMemcpyAsync(first, ctx->first, sizeof(int) * nn, k, s));
     if (last) CK(cudaMemcpyAsync(last, ctx->last, sizeof(int) * nn, k, s));

@@ -256,6 +256,7 @@ __device__ __forceinline__ void status_add(long long *status, int which, long lo
 int launch_sort(sph_ctx *ctx);
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
 int launch_groups(sph_ctx *ctx);
+int launch_leaf_records(sph_ctx *ctx);  // the leaves' 16-double records (export only)
 constexpr int SGROUP_MAX = 128;  // particles per super-group
 constexpr int SG_POOL = 8;       // node slots per particle of a super-group
 constexpr int SG_LSTRIDE = 40;   // floats per super-group record: 35 coefficients, pad, centre

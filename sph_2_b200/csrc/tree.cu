@@ -105,23 +105,49 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     int nd = n - 1 + p;
-    double o[16];
-    o[0] = x[p]; o[1] = y[p]; o[2] = z[p]; o[3] = m[p];
-    for (int q = 4; q < 10; q++) o[q] = 0.0;
-    o[10] = o[13] = x[p]; o[11] = o[14] = y[p]; o[12] = o[15] = z[p];
-    double *dst = node + (size_t)16 * nd;
-    for (int q = 0; q < 16; q++) dst[q] = o[q];
+    // a leaf is never accepted as a cell (count 1): the walks read its com
+    // and count only, and the climb and the export rebuild its 16-double
+    // record from the particle (leaf_record)
+    (void)node; (void)m; (void)wB; (void)wC;
+    const double xp = x[p], yp = y[p], zp = z[p];
     hmax[nd] = h[p];
     ropen2[nd] = 0.0;
-    sA[nd] = make_double4(o[10], o[11], o[12], h[p]);
-    sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
+    sA[nd] = make_double4(xp, yp, zp, h[p]);
+    sB[nd] = make_double4(xp, yp, zp, 0.0);
     first[nd] = p;
     last[nd] = p;
     child[2 * nd] = -1;
     child[2 * nd + 1] = -1;
     wL[nd] = make_int4(p, 1, -1, -1);
-    write_walk<R>(nd, o, 0.0, h[p], wA, wB, wC);
+    typename R4<R>::T a;
+    a.x = (R)xp; a.y = (R)yp; a.z = (R)zp; a.w = (R)0;
+    wA[nd] = a;
     if (p < n - 1) flag[p] = 0;
+}
+
+// the 16-double record of a leaf (particle p): com and box at the particle,
+// its mass, no second moments
+__device__ __forceinline__ void leaf_record(int p, const double *__restrict__ x,
+                                            const double *__restrict__ y,
+                                            const double *__restrict__ z,
+                                            const double *__restrict__ m, double *o) {
+    o[0] = o[10] = o[13] = x[p];
+    o[1] = o[11] = o[14] = y[p];
+    o[2] = o[12] = o[15] = z[p];
+    o[3] = m[p];
+    for (int q = 4; q < 10; q++) o[q] = 0.0;
+}
+
+// leaf records into the node array (for the export)
+__global__ void k_leaf_records(int n, const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const double *__restrict__ m,
+                               double *__restrict__ node) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    double o[16];
+    leaf_record(p, x, y, z, m, o);
+    double *dst = node + (size_t)16 * (n - 1 + p);
+    for (int q = 0; q < 16; q++) dst[q] = o[q];
 }
 
 __device__ __forceinline__ void combine(double *o, const double *a, const double *b) {
@@ -246,7 +272,9 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
 template <class R>
 __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
                             const int *__restrict__ gnode, const int *__restrict__ parent,
-                            const int *__restrict__ child, double *node, double *hmax,
+                            const int *__restrict__ child, const double *__restrict__ x,
+                            const double *__restrict__ y, const double *__restrict__ z,
+                            const double *__restrict__ m, double *node, double *hmax,
                             double *ropen2, double4 *sA, double4 *sB, int *flag, Opening op,
                             const int4 *__restrict__ wL, typename R4<R>::T *wA,
                             typename R4<R>::T *wB, typename R4<R>::T *wC) {
@@ -261,10 +289,17 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
         arrived.store(0, cuda::memory_order_relaxed);  // ready for the next pass
         int L = child[2 * nd], Rr = child[2 * nd + 1];
         double a[16], b[16], o[16];
-        const double *pa = node + (size_t)16 * L, *pb = node + (size_t)16 * Rr;
-        for (int q = 0; q < 16; q++) {
-            a[q] = __ldcg(pa + q);
-            b[q] = __ldcg(pb + q);
+        if (L >= n - 1) {
+            leaf_record(L - (n - 1), x, y, z, m, a);
+        } else {
+            const double *pa = node + (size_t)16 * L;
+            for (int q = 0; q < 16; q++) a[q] = __ldcg(pa + q);
+        }
+        if (Rr >= n - 1) {
+            leaf_record(Rr - (n - 1), x, y, z, m, b);
+        } else {
+            const double *pb = node + (size_t)16 * Rr;
+            for (int q = 0; q < 16; q++) b[q] = __ldcg(pb + q);
         }
         combine(o, a, b);
         double hm = fmax(__ldcg(hmax + L), __ldcg(hmax + Rr));
@@ -364,7 +399,8 @@ int launch_tree(sph_ctx *ctx) {
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
             (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
+            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
+            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (float4 *)ctx->wA,
             (float4 *)ctx->wB, (float4 *)ctx->wC);
     } else {
@@ -379,12 +415,21 @@ int launch_tree(sph_ctx *ctx) {
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
             (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->node, ctx->hmax,
+            n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
+            ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (double4 *)ctx->wA,
             (double4 *)ctx->wB, (double4 *)ctx->wC);
     }
     ctx->tree_ok = true;
     return ctx_check_launch(ctx, "tree");
+}
+
+int launch_leaf_records(sph_ctx *ctx) {
+    const int n = ctx->n, c = ctx->cur;
+    if (n <= 0) return SPH_OK;
+    k_leaf_records<<<div_up(n, 256), 256, 0, ctx->stream>>>(
+        n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node);
+    return ctx_check_launch(ctx, "leaf records");
 }
 
 int launch_refit_hmax(sph_ctx *ctx, const int *need) {
