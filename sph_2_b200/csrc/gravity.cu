@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
 // accepts); larger nodes that fail it are opened here.  A list longer than
 // SG_POOL slots per particle, or a stack overflow, leaves the super-group
 // without a record (nrem -1): its groups then walk from the root.
-template <bool POT>
+// (the expansion carries the potential too, so one kernel serves both)
 __global__ void __launch_bounds__(WALK_WARPS * 32, 6)
     k_sg_walk(const int *__restrict__ nsg_p, int cap, const int *__restrict__ sstart,
               const int *__restrict__ scount, const int *__restrict__ scloud,
@@ -869,7 +869,7 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
     if constexpr (std::is_same<R, float>::value) {
         if (ctx->g_sg && ctx->cfg.theta_local > 0.0) {
             const int sgrid = max(1, div_up(div_up(ctx->n, 64) + ctx->ncloud, WALK_WARPS));
-            k_sg_walk<POT><<<sgrid, WALK_WARPS * 32, 0, s>>>(
+            k_sg_walk<<<sgrid, WALK_WARPS * 32, 0, s>>>(
                 ctx->d_nsg, ctx->sg_cap, ctx->sg_start, ctx->sg_count, ctx->sg_cloud, ctx->croot,
                 (const float4 *)ctx->pw, (const float4 *)ctx->wA, (const float4 *)ctx->wB,
                 (const float4 *)ctx->wC, ctx->wL, eps2, (float)ctx->cfg.theta_local, ctx->sg_pool,

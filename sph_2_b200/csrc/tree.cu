@@ -95,20 +95,17 @@ __device__ __forceinline__ double open_r2(const double *o, double theta) {
 
 template <class R>
 __global__ void k_leaves(int n, const double *__restrict__ x, const double *__restrict__ y,
-                         const double *__restrict__ z, const double *__restrict__ m,
-                         const double *__restrict__ h, double *__restrict__ node,
+                         const double *__restrict__ z, const double *__restrict__ h,
                          double *__restrict__ hmax, double *__restrict__ ropen2,
                          double4 *__restrict__ sA, double4 *__restrict__ sB, int *__restrict__ flag,
                          int *__restrict__ first, int *__restrict__ last, int *__restrict__ child,
-                         typename R4<R>::T *wA, typename R4<R>::T *wB, typename R4<R>::T *wC,
-                         int4 *__restrict__ wL) {
+                         typename R4<R>::T *wA, int4 *__restrict__ wL) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     int nd = n - 1 + p;
     // a leaf is never accepted as a cell (count 1): the walks read its com
     // and count only, and the climb and the export rebuild its 16-double
     // record from the particle (leaf_record)
-    (void)node; (void)m; (void)wB; (void)wC;
     const double xp = x[p], yp = y[p], zp = z[p];
     hmax[nd] = h[p];
     ropen2[nd] = 0.0;
@@ -389,9 +386,9 @@ int launch_tree(sph_ctx *ctx) {
     int rc;
     if (mixed) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
-            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
-            ctx->last, ctx->child, (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->wL);
+            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
+            ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (float4 *)ctx->wA,
+            ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
@@ -405,9 +402,9 @@ int launch_tree(sph_ctx *ctx) {
             (float4 *)ctx->wB, (float4 *)ctx->wC);
     } else {
         k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
-            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
-            ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, ctx->flag, ctx->first,
-            ctx->last, ctx->child, (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->wL);
+            n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
+            ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (double4 *)ctx->wA,
+            ctx->wL);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
