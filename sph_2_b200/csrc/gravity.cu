@@ -7,20 +7,23 @@
 // eps_i only, G = 1.  And the O(N^2) direct sums acc_g (hfvCLibs_v7_hfv_v2.h:
 // 532-584) / getAcc_g_smth_mimj_mpi (MPI_sph/sph_code/libsx.py:910-947).
 //
-// Walk: a persistent kernel; each warp takes groups of 32 consecutive
-// Morton-ordered particles from a work counter.  The warp walks the tree 32
-// nodes per round (LIFO stack in shared memory) testing each node against the
+// Walk: one warp per group (a maximal tree node of at most 32 particles of
+// one cloud), grid-stride over the groups.  The warp walks the tree 32 nodes
+// per round (LIFO stack in shared memory) testing each node against the
 // group's box: a node is accepted when the squared distance from its centre of
-// mass to the box is >= r_open^2 (r_open = l/theta + |com - box centre|),
-// opened otherwise; opened buckets (<= leaf_size particles) go to a particle
-// list.  Accepted nodes and bucket particles are staged 32 at a time in shared
-// memory and every lane evaluates all 32 against its own particle, so the
-// interaction loop is branch-free FP32 (mixed) or FP64 (plain) FMA work with
-// one reciprocal square root per interaction.  In FP32 every instruction
-// evaluates two staged entries at once with the packed f32x2 arithmetic of
-// sm_100 (__ffma2_rn / __fmul2_rn), which halves the issued instructions of
-// this issue-bound loop.  Each 32-term chunk is summed plainly and folded into
-// a Kahan accumulator (mixed).
+// mass to the box is >= r_open^2 (r_open = l/theta + |com - box centre|, theta
+// possibly wider for small cells, see tree.cu), opened otherwise; opened
+// buckets (<= leaf_size particles) go to a particle list.  Accepted nodes and
+// bucket particles are staged 32 at a time in shared memory and every lane
+// evaluates all 32 against its own particle, so the interaction loop is
+// branch-free FP32 (mixed) or FP64 (plain) FMA work with one reciprocal square
+// root per interaction.  In FP32 every instruction evaluates two staged
+// entries at once with the packed f32x2 arithmetic of sm_100 (__ffma2_rn /
+// __fmul2_rn), which halves the issued instructions of this issue-bound loop.
+// Each 32-term chunk is summed plainly and folded into a Kahan accumulator
+// (mixed).  The FP32 walk with theta_local > 0 also sends far accepted cells
+// through per-group Taylor expansions, and starts each group from its
+// super-group's node list with the super-group's own expansion (k_sg_walk).
 #include <type_traits>
 
 #include "sph_internal.cuh"
