@@ -5,10 +5,12 @@
 // Replaces the reference octree (bh_tree_iteration_v2.h:29-450): a single
 // <<<1,256>>> block inserting bodies under atomicCAS child locks with
 // atomicAdd'ed masses (nondeterministic), a separate centre-of-mass kernel and
-// a busy-waiting tree-order sort.  Here the build is one thread per internal
-// node, the moments are combined bottom-up with the left child always first
-// (so every node record is the same bit pattern on every run and equals the
-// oracle's), and the Morton order is the walk order.
+// a busy-waiting tree-order sort.  Here the topology is one thread per
+// internal node; the nodes inside a walk group (at most 32 particles of one
+// cloud) are summed directly over their particle range in index order, one
+// lane each, and the nodes above the groups are combined bottom-up with the
+// left child always first, so every node record is the same bit pattern on
+// every run and equals the oracle's.  The Morton order is the walk order.
 #include <cuda/atomic>
 
 #include "sph_internal.cuh"
