@@ -69,3 +69,19 @@ def test_context_create_fails_loudly_without_gpu(lib):
     assert L.sph_default_config(C.byref(cfg)) == 0
     h = C.c_void_p()
     assert L.sph_ctx_create(C.byref(cfg), C.byref(h)) != 0
+
+
+def test_python_config_defaults_match_the_library():
+    """Config() and sph_default_config give the same sph_config, field by
+    field (host-only call, no GPU); the walk's optional settings default
+    to off."""
+    from sph_2_b200 import Config, _lib
+    L = _lib.load()
+    c = _lib.SphConfig()
+    assert L.sph_default_config(C.byref(c)) == 0
+    py = Config().to_c()
+    for name, _ in _lib.SphConfig._fields_:
+        assert getattr(py, name) == getattr(c, name), name
+    assert c.theta_local == 0.0 and c.theta_small == 0.0 and c.small_cell == 0
+    on = Config(theta_local=0.28, theta_small=0.45, small_cell=128).to_c()
+    assert (on.theta_local, on.theta_small, on.small_cell) == (0.28, 0.45, 128)
