@@ -8,7 +8,7 @@ an FP64 direct-summation oracle on a seeded 10k-particle subset.
 
 Prints ONE JSON line (rank 0).  Multi-GPU (torchrun): every rank advances its
 own replica of the workload (the single sphere does not shard without a halo
-exchange; see DESIGN.md), timing is the max over ranks, value is the whole-job
+exchange), timing is the max over ranks, value is the whole-job
 throughput.  --impl reference times the reference's CPU implementation of the
 step (the oracle's C restatement of MPI_sph/sph_code/libsx.py + shear.py, the
 reference's all-pairs loops with its row-range decomposition) on the host
