@@ -208,6 +208,18 @@ int sph_get_groups(sph_ctx *ctx, int32_t *ngroup, int32_t *gstart, int32_t *gcou
  * hfvCLibs_v7_hfv_v2.h:367-455, and h_smooth_fast_mpi, libsx.py:854-902).
  * Needs sph_build_tree. */
 int sph_smoothing_h(sph_ctx *ctx);
+/* The reference's own smoothing-length iteration (h_smooth_fast_mpi,
+ * MPI_sph/sph_code/libsx.py:854-902, with n_target 50, n_tol 5, step_frac
+ * 0.003): starting from the current h, h <- h (1 - step_frac) while
+ * #{j : |r_ij| < 2h} > n_target + n_tol and h <- h (1 + step_frac) while it is
+ * below n_target - n_tol (self included, distances rounded as the reference
+ * computes them), so the result is bit-exact with the reference on the same
+ * positions.  The reference iterates without bound (it only prints after 100
+ * iterations); here a particle stops after max_iter iterations and is
+ * counted in SPH_S_H_NOCONV.  n_target + n_tol must not exceed max_ngb.
+ * Needs sph_build_tree. */
+int sph_smoothing_h_count(sph_ctx *ctx, int32_t n_target, int32_t n_tol, double step_frac,
+                          int32_t max_iter);
 /* Exact neighbour lists |r_ij|^2 <= (h_i+h_j)^2 (replaces ngbDB_new_v2,
  * ngb_v3.h:124-238).  Needs sph_build_tree (h_max is refitted here). */
 int sph_neighbours(sph_ctx *ctx);
@@ -345,8 +357,12 @@ int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
  * n <= SPH_NOALLOC_MAX_N (SPH_ERR_CAPACITY above it).  All calls share that
  * array: calls that overlap on the GPU race.  The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  Work is queued on cuda_stream (NULL: the legacy
- * default stream) of the current device. */
+ * before any stream capture.  The address is kept until the process exits: after
+ * a cudaDeviceReset the library must be reloaded before this entry point is used
+ * again.  If a CUDA error from the caller's earlier work is pending on entry,
+ * the call returns SPH_ERR_CUDA without launching and leaves that error set.
+ * Work is queued on cuda_stream (NULL: the legacy default stream) of the
+ * current device. */
 #define SPH_NOALLOC_MAX_N 262144
 int sph_morton_sort_noalloc(const double *x, const double *y, const double *z, int32_t n,
                             uint64_t *keys, int32_t *perm, void *cuda_stream);

@@ -283,6 +283,25 @@ def force_list(x, y, z, vx, vy, vz, rho, P, c, h, m, divV, curlV, alpha, beta, e
     return np.stack([ax, ay, az], 1), du, vs
 
 
+def courant_dt(h, vsig, acc, courant, cloud=None):
+    """Courant step per cloud of the project's global step (the survey's
+    replacement of dt_array_indiv_dt, hfvCLibs_v7_hfv_v2.h:999-1078):
+    dt_c = courant * min over the cloud's particles of min(h / v_sig,
+    sqrt(h / |a|)), a = a_sph + a_grav; particles without a finite positive
+    estimate are skipped."""
+    h, vsig = np.asarray(h, float), np.asarray(vsig, float)
+    amag = np.sqrt(np.sum(np.asarray(acc, float) ** 2, axis=1))
+    t = h / np.maximum(vsig, 1e-300)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ta = np.where(amag > 0, np.sqrt(h / np.where(amag > 0, amag, 1.0)), np.inf)
+    t = courant * np.minimum(t, ta)
+    ok = np.isfinite(t) & (t > 0)
+    cl = np.zeros(len(h), np.int64) if cloud is None else np.asarray(cloud, np.int64)
+    out = np.full(int(cl.max()) + 1 if len(cl) else 1, np.inf)
+    np.minimum.at(out, cl[ok], t[ok])
+    return out
+
+
 def grav_direct(x, y, z, m, G, eps, targets, cloud=None):
     """FP64 Plummer direct sum onto the target indices (all sources of the
     target's cloud).  The reference's direct sums (libsx.py:910-947,

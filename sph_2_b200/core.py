@@ -251,6 +251,14 @@ class Context:
     def smoothing_h(self):
         self._chk(self._L.sph_smoothing_h(self._h), "sph_smoothing_h")
 
+    def smoothing_h_count(self, n_target=50, n_tol=5, step_frac=0.003, max_iter=10000):
+        """The reference's own count iteration (libsx.py:854-902): h moves by
+        -/+ step_frac h until n_target - n_tol <= #(|r_ij| < 2h) <= n_target
+        + n_tol, bit-exact with the reference on the same positions."""
+        self._chk(self._L.sph_smoothing_h_count(self._h, int(n_target), int(n_tol),
+                                                float(step_frac), int(max_iter)),
+                  "sph_smoothing_h_count")
+
     def neighbours(self):
         self._chk(self._L.sph_neighbours(self._h), "sph_neighbours")
 

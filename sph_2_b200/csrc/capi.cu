@@ -319,7 +319,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->cand_idx, K * N);
     DAF(ctx->cand_cnt, N);
     DAF(ctx->lflag, N + 2);
-    DAF(ctx->retry, N); DAF(ctx->hcand, N);
+    DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
     DAF(ctx->status, SPH_NSTATUS);
     DAF(ctx->counters, 5);
@@ -630,6 +630,18 @@ int sph_smoothing_h(sph_ctx *ctx) {
     if (!ctx->tree_ok) return SPH_ERR_STATE;
     drop_graphs(ctx);
     return launch_smoothing_h(ctx);
+}
+
+int sph_smoothing_h_count(sph_ctx *ctx, int32_t n_target, int32_t n_tol, double step_frac,
+                          int32_t max_iter) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    if (n_target < 1 || n_tol < 0 || n_tol >= n_target || n_target + n_tol > ctx->cfg.max_ngb ||
+        !(step_frac > 0.0 && step_frac < 0.5) || max_iter < 1)
+        return SPH_ERR_ARG;
+    drop_graphs(ctx);
+    return launch_smoothing_h_count(ctx, n_target, n_tol, step_frac, max_iter);
 }
 
 int sph_neighbours(sph_ctx *ctx) {

@@ -124,7 +124,9 @@ struct SearchArgs {
 
 // Walk the tree for group g and write the rows of the active lanes.
 // MODE 0: candidates r^2 <= ri^2 (ri = 2 hc_i, the h iteration's gather radius)
+//         with the first Newton evaluation's kernel sums
 // MODE 1: exact lists |r|^2 <= (h_i + h_j)^2
+// MODE 2: candidates r^2 <= ri^2 alone (the count iteration)
 template <int MODE, class R = double>
 __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A, int g, bool act,
                                              int i, const double4 &pi, double ri,
@@ -140,7 +142,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const double ri2 = ri * ri;
     const int K = A.K;
     // candidate row of particle i: entries [i K, i K + K)
-    const size_t cbase = MODE == 0 ? (size_t)i * K : 0;
+    const size_t cbase = MODE != 1 ? (size_t)i * K : 0;
     int count = 0;
     double hnb = 0.0;
     int sp = 1, nflat = 0;
@@ -225,12 +227,12 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                     if (count < K) A.cidx[cbase + count] = S.flat[k];
                     count++;
                 }
-            } else if (MODE == 0) {
+            } else if (MODE != 1) {
                 const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                 if (dx * dx + dy * dy + dz * dz <= ri2) {
                     // the first Newton evaluation (at h = pi.w) rides on the
                     // search: rows are only re-read by later iterations
-                    hs->add(pair_r<R>(pi, pj), (R)S.smass[k]);
+                    if (MODE == 0) hs->add(pair_r<R>(pi, pj), (R)S.smass[k]);
                     if (count < K) A.cidx[cbase + count] = S.flat[k];
                     count++;
                 }
@@ -264,7 +266,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                 double ey = fmax(fmax(a.y - gy1, gy0 - b.y), 0.0);
                 double ez = fmax(fmax(a.z - gz1, gz0 - b.z), 0.0);
                 double d2 = ex * ex + ey * ey + ez * ez;
-                double reach = MODE == 0 ? rmax : (a.w + rmax);
+                double reach = MODE != 1 ? rmax : (a.w + rmax);
                 open = d2 <= reach * reach * (1.0 + 1e-12);
             }
             __syncwarp();
@@ -308,7 +310,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         }
     }
     if (act) {
-        if (MODE == 0) {
+        if (MODE != 1) {
             // the full count: the Newton step shrinks the gather radius of a
             // row that did not fit instead of iterating on a truncated one
             A.cnt[i] = count;
@@ -550,6 +552,104 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
     }
 }
 
+// The reference's count iteration (h_smooth_fast_mpi, MPI_sph/sph_code/
+// libsx.py:854-902) for the particle of one lane: with d_j = |r_j - r_i|
+// (self included) and n(h) = #{j : d_j < 2 h}, h <- h - f h while n(h) > hi_n
+// and h <- h + f h while n(h) < lo_n.  Its only state is h, so a particle
+// whose 2 h would pass its candidate radius 2 hc stops, stores h and
+// resumes in the next round with a wider radius: the sequence of h is that
+// of one uninterrupted iteration.  d_j is rounded as the reference writes it
+// (dx = x_j - x_i, dx dx + dy dy, + dz dz, correctly rounded square root),
+// so the result is bit-exact with it on the same positions.
+struct CountArgs {
+    double *h_out, *hc;
+    int *retry, *iters;
+    int lo_n, hi_n, max_iter, last_round;
+    double frac, grow;
+};
+
+__device__ __forceinline__ double ref_dist(const double4 &pi, const double4 &pj) {
+    const double dx = xsub(pj.x, pi.x), dy = xsub(pj.y, pi.y), dz = xsub(pj.z, pi.z);
+    return __dsqrt_rn(xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz)));
+}
+
+__device__ __forceinline__ void count_lane(const SearchArgs &A, const CountArgs &B, int i,
+                                           const double4 &pi, const int *row) {
+    const int craw = A.cnt[i];
+    double h = pi.w;
+    int it = B.iters[i];
+    const double cap = B.hc[i];
+    bool done = false, ok = false;
+    if (craw > A.K) {
+        // the row cannot hold every candidate: first narrow the radius to 2 h;
+        // a row that overflows even there has n(h) > K > hi_n, so h takes
+        // one decrement of the iteration before the next search
+        if (cap > h) {
+            B.hc[i] = h;
+        } else {
+            h = xsub(h, xmul(B.frac, h));
+            it++;
+            B.hc[i] = h;
+        }
+        status_add(A.status, SPH_S_H_RETRY, 1);
+    } else {
+        // every j with d_j < 2 h is in the row while h stays below the
+        // radius by more than the FP64 rounding of the search's r^2 test
+        const double lim = cap * (1.0 - 1e-12);
+        while (h <= lim) {
+            const double h2 = 2.0 * h;
+            int nn = 0;
+            for (int k = 0; k < craw; k++) nn += ref_dist(pi, A.p0[row[k]]) < h2;
+            if (nn > B.hi_n) {
+                h = xsub(h, xmul(B.frac, h));
+            } else if (nn < B.lo_n) {
+                h = xadd(h, xmul(B.frac, h));
+            } else {
+                ok = true;
+                break;
+            }
+            if (++it > B.max_iter) {
+                done = true;
+                break;
+            }
+        }
+        if (!ok && !done) {
+            B.hc[i] = h * B.grow;  // h passed the radius: search again, wider
+            status_add(A.status, SPH_S_H_RETRY, 1);
+        }
+    }
+    const bool again = !ok && !done && !B.last_round;
+    B.retry[i] = again ? 1 : 0;
+    if (!ok && !again) status_add(A.status, SPH_S_H_NOCONV, 1);
+    B.iters[i] = it;
+    B.h_out[i] = h;
+    A.p0[i].w = h;
+}
+
+// candidate search + count iteration for the flagged particles of each group
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
+    k_cand_count(const int *__restrict__ ngroup_p, SearchArgs A, CountArgs B) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+        const int s0 = A.gstart[g], gc = A.gcount[g];
+        bool act = lane < gc;
+        const int i = s0 + (act ? lane : 0);
+        act = act && B.retry[i];
+        if (!__ballot_sync(FULL, act)) continue;
+        const double4 pi = A.p0[i];
+        group_search<2, double>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
+        if (act) count_lane(A, B, i, pi, A.cidx + (size_t)i * A.K);
+        __syncwarp();
+    }
+}
+
+__global__ void k_zero_int(int n, int *__restrict__ a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0;
+}
+
 // canonical CSR export, each row sorted ascending
 __global__ void k_export(int n, const int *__restrict__ rows, const int *__restrict__ cnt, int K,
                          const long long *__restrict__ off, int *__restrict__ lst) {
@@ -627,6 +727,39 @@ int launch_smoothing_h(sph_ctx *ctx) {
     ctx->lists_ok = false;
     ctx->cand_ok = true;
     return ctx_check_launch(ctx, "smoothing_h");
+}
+
+int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac, int max_iter) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int c = ctx->cur;
+    k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
+                                            ctx->retry, H_GROW);
+    k_zero_int<<<div_up(n, 256), 256, 0, s>>>(n, ctx->hiter);
+    // each round widens the radius by H_GROW; 0.3 % steps need about 26
+    // iterations for that, so 16 rounds cover a 3.4x change of h
+    const int rounds = 16;
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
+    CountArgs B;
+    B.h_out = ctx->st[c][ST_H];
+    B.hc = ctx->hcand;
+    B.retry = ctx->retry;
+    B.iters = ctx->hiter;
+    B.lo_n = n_target - n_tol;
+    B.hi_n = n_target + n_tol;
+    B.max_iter = max_iter;
+    B.frac = frac;
+    B.grow = H_GROW;
+    for (int r = 0; r < rounds; r++) {
+        B.last_round = r == rounds - 1;
+        k_cand_count<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+    }
+    ctx->lists_ok = false;
+    ctx->cand_ok = true;
+    ctx->p2_dirty = true;
+    return ctx_check_launch(ctx, "smoothing_h_count");
 }
 
 int launch_neighbours(sph_ctx *ctx) {

@@ -205,7 +205,10 @@ __global__ void __launch_bounds__(NA_THREADS)
     }
 }
 
-// device address of the scratch array, fetched once per device
+// device address of the scratch array, fetched once per device and kept for
+// the life of the process: a caller that resets the device (cudaDeviceReset)
+// or otherwise destroys its primary context must reload the library before it
+// calls this entry point again, since the address belongs to the old context
 std::mutex g_na_mutex;
 void *g_na_ptr[256] = {};
 
@@ -230,6 +233,9 @@ extern "C" int sph_morton_sort_noalloc(const double *x, const double *y, const d
     if (n > NA_MAX_N) return SPH_ERR_CAPACITY;
     if (n == 0) return SPH_OK;
     if (!x || !y || !z || !keys || !perm) return SPH_ERR_ARG;
+    // an error left pending by the caller's earlier work is not ours to
+    // report or to clear: refuse to launch and leave it for the caller
+    if (cudaPeekAtLastError() != cudaSuccess) return SPH_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return SPH_ERR_CUDA;
     unsigned char *base = nullptr;
@@ -261,5 +267,6 @@ extern "C" int sph_morton_sort_noalloc(const double *x, const double *y, const d
         kin = kout;
         vin = vout;
     }
+    // no error was pending on entry, so one found now comes from these launches
     return cudaGetLastError() == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
 }

@@ -110,6 +110,7 @@ struct sph_ctx {
     int *lflag = nullptr;     // n+2: per particle "needs the tree search", "all do", "any does"
     bool cand_ok = false;     // candidate rows match the current order, positions and h
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
+    int *hiter = nullptr;        // per particle: iterations of the count iteration so far
     double *hcand = nullptr;     // candidate radius / 2 used per particle
     bool lists_ok = false, rho_ok = false, divcurl_ok = false;
 
@@ -264,6 +265,7 @@ int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 int launch_tree(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);
+int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac, int max_iter);
 int launch_neighbours(sph_ctx *ctx);
 int launch_density(sph_ctx *ctx);
 int launch_divcurl(sph_ctx *ctx);

@@ -13,11 +13,15 @@ and returns rows nbeg..nend-1.  Inputs may be NumPy arrays (copied) or torch
 CUDA tensors (device-to-device copies, no host round trip).  There is no CPU
 path: without the library or a GPU every call raises.
 
+h_smooth_fast_mpi / h_smooth_fast run the reference's own +-0.3 % count
+iteration (libsx.py:806-902) on the GPU and return the same h bit for bit.
+The project's Newton smoothing length, which solves (4 pi / 3)(2h)^3 rho(h) =
+N_ngb m, is offered under its own name, h_newton_mpi.
+
 Differences from the reference, by design:
-* h_smooth_fast_mpi / smoothing_length_mpi return the Newton smoothing length
-  that solves (4 pi / 3)(2h)^3 rho(h) = N_ngb m (N_ngb = 50, the centre of the
-  reference's [45, 55] count window) instead of the +-0.3 % count iteration
-  (libsx.py:854-902) or the 50th-neighbour distance (libsx.py:781-803).
+* smoothing_length_mpi returns the Newton smoothing length started from a
+  uniform-density guess instead of half the 50th-neighbour distance
+  (libsx.py:781-803); both are starting values for h_smooth_fast_mpi.
 * getAcc_g_smth_mimj_mpi accepts only the full range (0, N): the reference's
   partial fields exist for its MPI reduction, which a single GPU does not need.
 * getPressure / getCsound / getKE are elementwise host formulas (no kernel is
@@ -38,6 +42,7 @@ __all__ = [
     "getAcc_sph", "getAcc_sph_mpi", "getAcc_sph_mpiXXX", "get_dU", "get_dU_mpi",
     "get_dU_mpiXXXX", "getAcc_sph_shear", "getAcc_sph_shear_mpi", "get_dU_shear",
     "get_dU_shear_mpi", "getAcc_g_smth_mimj_mpi", "h_smooth_fast_mpi", "h_smooth_fast",
+    "h_newton_mpi",
     "smoothing_length_mpi", "getKE", "getPE", "precision", "release",
 ]
 
@@ -310,9 +315,32 @@ def _host(a):
 
 
 # ---- smoothing lengths ---------------------------------------------------
-def h_smooth_fast_mpi(nbeg, nend, pos, h, m=None, n_ngb=50.0):
-    """Smoothing lengths of rows nbeg..nend-1 starting from h (replaces the
-    count iteration of libsx.py:854-902; see the module docstring)."""
+def h_smooth_fast_mpi(nbeg, nend, pos, h, max_iter=10000):
+    """libsx.py:854-902: from h, h <- h - 0.003 h while more than 55
+    particles (self included) lie within |r_ij| < 2h and h <- h + 0.003 h
+    while fewer than 45 do; rows nbeg..nend-1.  Bit-exact with the reference.
+    The reference keeps iterating without bound (it prints after 100
+    iterations); a row still outside the window after max_iter iterations
+    raises SphError (SPH_ERR_NOCONV) here."""
+    n = int(pos.shape[0])
+    mm = np.full(n, 1.0 / n) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + 1.0 / n
+    ctx = _load_state(pos, mm, h)
+    ctx.smoothing_h_count(50, 5, 0.003, max_iter)
+    st = ctx.status(reset=True)
+    if st["h_noconv"]:
+        raise L.SphError(-4, "h_smooth_fast_mpi", f"({st['h_noconv']} rows did not converge)")
+    return _rows(_out(ctx, "h", pos), nbeg, nend)
+
+
+def h_smooth_fast(pos, h, max_iter=10000):
+    """libsx.py:806-850 (all rows)."""
+    return h_smooth_fast_mpi(0, pos.shape[0], pos, h, max_iter)
+
+
+def h_newton_mpi(nbeg, nend, pos, h, m=None, n_ngb=50.0):
+    """The project's smoothing length (no reference counterpart): the
+    bracketed Newton solution of (4 pi / 3)(2h)^3 rho(h) = n_ngb m, started
+    from h; rows nbeg..nend-1."""
     n = int(pos.shape[0])
     mm = (np.full(n, 1.0 / n) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + 1.0 / n) \
         if m is None else m
@@ -322,13 +350,8 @@ def h_smooth_fast_mpi(nbeg, nend, pos, h, m=None, n_ngb=50.0):
     ctx.smoothing_h()
     st = ctx.status(reset=True)
     if st["h_noconv"]:
-        raise L.SphError(-4, "h_smooth_fast_mpi", f"({st['h_noconv']} rows did not converge)")
+        raise L.SphError(-4, "h_newton_mpi", f"({st['h_noconv']} rows did not converge)")
     return _rows(_out(ctx, "h", pos), nbeg, nend)
-
-
-def h_smooth_fast(pos, h, m=None, n_ngb=50.0):
-    """libsx.py:806-850 (all rows)."""
-    return h_smooth_fast_mpi(0, pos.shape[0], pos, h, m, n_ngb)
 
 
 def smoothing_length_mpi(nbeg, nend, pos, m=None, n_ngb=50.0):
@@ -339,7 +362,7 @@ def smoothing_length_mpi(nbeg, nend, pos, m=None, n_ngb=50.0):
     ext = np.ptp(p, axis=0).prod() if n > 1 else 1.0
     h0 = 0.5 * (max(ext, 1e-300) * n_ngb / max(n, 1)) ** (1.0 / 3.0)
     h = np.full(n, h0) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + h0
-    return h_smooth_fast_mpi(nbeg, nend, pos, h, m, n_ngb)
+    return h_newton_mpi(nbeg, nend, pos, h, m, n_ngb)
 
 
 # ---- elementwise formulas and energies -----------------------------------

@@ -27,7 +27,10 @@ def context_keys_perm(pos):
         return ctx.sort_info()
 
 
-def noalloc_keys_perm(pos):
+def noalloc_keys_perm(pos, stream=None, free_bytes=None):
+    """Run the entry point on device copies of pos, on `stream` (default: the
+    current torch stream).  free_bytes: a list that receives the device's free
+    memory just before and just after the call."""
     import torch
     lib = L.load()
     dev = torch.device("cuda:0")
@@ -36,12 +39,17 @@ def noalloc_keys_perm(pos):
     n = len(pos)
     keys = torch.empty(n, dtype=torch.int64, device=dev)
     perm = torch.empty(n, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream()
+    stream = stream or torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    if free_bytes is not None:
+        free_bytes.append(torch.cuda.mem_get_info()[0])
     rc = lib.sph_morton_sort_noalloc(C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
                                      C.c_void_p(z.data_ptr()), n, C.c_void_p(keys.data_ptr()),
                                      C.c_void_p(perm.data_ptr()), C.c_void_p(stream.cuda_stream))
     assert rc == 0
     torch.cuda.synchronize()
+    if free_bytes is not None:
+        free_bytes.append(torch.cuda.mem_get_info()[0])
     return keys.cpu().numpy().view(np.uint64), perm.cpu().numpy()
 
 
@@ -54,6 +62,22 @@ def test_noalloc_matches_context_sort_on_two_calls_in_a_row():
         k, p = noalloc_keys_perm(pos)
         assert np.array_equal(k, k_ref)
         assert np.array_equal(p, p_ref)
+
+
+def test_noalloc_takes_no_device_memory_and_runs_on_any_stream():
+    """A repeated call leaves the device's free memory unchanged, and a call
+    queued on a non-default stream gives the same order."""
+    import torch
+    pos = ic.evrard(100_000, seed=6)["pos"]
+    k_ref, p_ref = context_keys_perm(pos)
+    noalloc_keys_perm(pos)                         # first call on the device: set-up
+    free = []
+    k, p = noalloc_keys_perm(pos, free_bytes=free)
+    assert free[0] == free[1], f"free device memory changed by {free[0] - free[1]} bytes"
+    assert np.array_equal(k, k_ref) and np.array_equal(p, p_ref)
+    side = torch.cuda.Stream()
+    k2, p2 = noalloc_keys_perm(pos, stream=side)
+    assert np.array_equal(k2, k_ref) and np.array_equal(p2, p_ref)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
