@@ -579,24 +579,36 @@ __device__ __forceinline__ void count_lane(const SearchArgs &A, const CountArgs 
     double h = pi.w;
     int it = B.iters[i];
     const double cap = B.hc[i];
-    bool done = false, ok = false;
+    bool ok = false, done = false, again = false;
     if (craw > A.K) {
-        // the row cannot hold every candidate: first narrow the radius to 2 h;
-        // a row that overflows even there has n(h) > K > hi_n, so h takes
-        // one decrement of the iteration before the next search
-        if (cap > h) {
-            B.hc[i] = h;
-        } else {
-            h = xsub(h, xmul(B.frac, h));
-            it++;
-            B.hc[i] = h;
-        }
-        status_add(A.status, SPH_S_H_RETRY, 1);
+        // the row cannot hold every candidate: narrow the radius towards a
+        // half-full row and search again
+        B.hc[i] = cap * fmax(0.5, cbrt(0.5 * A.K / (double)craw));
+        again = true;
     } else {
-        // every j with d_j < 2 h is in the row while h stays below the
-        // radius by more than the FP64 rounding of the search's r^2 test
+        // every j with d_j < 2 lim is in the row: the search's r^2 test is
+        // not rounded as d_j is, so lim keeps a margin below the radius
         const double lim = cap * (1.0 - 1e-12);
-        while (h <= lim) {
+        if (h > lim) {
+            // h beyond the complete radius: n(h) >= n(lim), so while n(lim)
+            // is above the window every decrement is the reference's own
+            const double l2 = 2.0 * lim;
+            int nin = 0;
+            for (int k = 0; k < craw; k++) nin += ref_dist(pi, A.p0[row[k]]) < l2;
+            if (nin > B.hi_n) {
+                while (h > lim) {
+                    h = xsub(h, xmul(B.frac, h));
+                    if (++it > B.max_iter) {
+                        done = true;
+                        break;
+                    }
+                }
+            } else {
+                B.hc[i] = h * B.grow;  // too few inside: search wider
+                again = true;
+            }
+        }
+        while (!done && !again && h <= lim) {
             const double h2 = 2.0 * h;
             int nn = 0;
             for (int k = 0; k < craw; k++) nn += ref_dist(pi, A.p0[row[k]]) < h2;
@@ -608,17 +620,15 @@ __device__ __forceinline__ void count_lane(const SearchArgs &A, const CountArgs 
                 ok = true;
                 break;
             }
-            if (++it > B.max_iter) {
-                done = true;
-                break;
-            }
+            if (++it > B.max_iter) done = true;
         }
-        if (!ok && !done) {
+        if (!ok && !done && !again) {
             B.hc[i] = h * B.grow;  // h passed the radius: search again, wider
-            status_add(A.status, SPH_S_H_RETRY, 1);
+            again = true;
         }
     }
-    const bool again = !ok && !done && !B.last_round;
+    if (again) status_add(A.status, SPH_S_H_RETRY, 1);
+    again = again && !B.last_round;
     B.retry[i] = again ? 1 : 0;
     if (!ok && !again) status_add(A.status, SPH_S_H_NOCONV, 1);
     B.iters[i] = it;

@@ -75,10 +75,15 @@ def test_gravity_and_energies(g):
 
 def test_smoothing_length(g):
     n = len(g["m"])
-    h = X.h_smooth_fast_mpi(0, n, g["pos"], g["h"], m=g["m"])
+    # the reference's count iteration, from its own start: its output bit for bit
+    h = X.h_smooth_fast_mpi(0, n, g["pos"], g["h0"])
+    assert np.array_equal(h, g["h"])
+    assert np.array_equal(X.h_smooth_fast_mpi(100, 300, g["pos"], g["h0"]), g["h"][100:300])
+    # the project's Newton h under its own name
+    hn = X.h_newton_mpi(0, n, g["pos"], g["h"], m=g["m"])
     x, y, z = (g["pos"][:, k].copy() for k in range(3))
     ho, _, bad = O.newton_h(x, y, z, g["m"], g["h"], n_ngb=50.0)
-    assert bad == 0 and np.max(np.abs(h / ho - 1)) < 2e-3
+    assert bad == 0 and np.max(np.abs(hn / ho - 1)) < 2e-3
     h0 = X.smoothing_length_mpi(0, n, g["pos"], m=g["m"])
     assert np.max(np.abs(h0 / ho - 1)) < 2e-3
 
