@@ -57,6 +57,8 @@ def parse():
                     help="evrard: the headline line; ensemble / cooling / large: extra workloads")
     ap.add_argument("--clouds", type=int, default=64)
     ap.add_argument("--tune", action="store_true", help="run the autotuner before timing")
+    ap.add_argument("--no-theta-table", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -152,12 +154,54 @@ def cpu_reference_sample(n, rows_per_thread=64, seed=42):
                         sample_s=round(sum(t.values()), 3))
 
 
+def cpu_reference_full_step(n=10_000, seed=42, steps=3):
+    """Every row of the reference's CPU step at N = 10,000 (the plain FP64
+    Evrard configuration): h_smooth_fast_mpi, getDensity_mpi,
+    getAcc_g_smth_mimj_mpi, div_curlVel_mpi, getAcc_sph_shear_mpi,
+    get_dU_shear_mpi and the KDK updates of sph_mpi4_v4.py:278-416, through
+    the oracle's C restatement on all host threads; measured, not
+    extrapolated.  Returns (mean seconds per step, phase seconds)."""
+    from oracle import oracle as O
+    from sph_2_b200 import ic
+    d = ic.evrard(n, seed=seed)
+    pos = np.ascontiguousarray(d["pos"])
+    m, u = d["m"], d["u"].copy()
+    v = np.zeros_like(pos)
+    eps = np.full(n, 1e-2)
+    gama, dt = 5.0 / 3.0, 1e-3
+    h = O.ref_h_smooth_fast(0, n, pos, d["h"])          # converged start (untimed)
+    acc = np.zeros_like(pos)
+    times, phases = [], {}
+    for _ in range(steps):
+        t = {}
+        t0 = time.perf_counter()
+        v = v + 0.5 * dt * acc
+        pos = pos + dt * v
+        t["kick_drift"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); h = O.ref_h_smooth_fast(0, n, pos, h); t["h_smooth_fast"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); rho = O.ref_getDensity(0, n, pos, m, h); t["density"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); ag = O.ref_getAcc_g_smth_mimj(0, n, pos, m, 1.0, eps); t["gravity"] = time.perf_counter() - t0
+        P = (gama - 1.0) * rho * u
+        c = np.sqrt(gama * (gama - 1.0) * u)
+        t0 = time.perf_counter(); dv, cv = O.ref_div_curlVel(0, n, pos, v, rho, m, h); t["divcurl"] = time.perf_counter() - t0
+        t0 = time.perf_counter(); asph = O.ref_getAcc_sph(0, n, pos, v, rho, P, c, h, m, dv, cv, 1.0); t["acc_sph"] = time.perf_counter() - t0
+        acc = ag + asph
+        v = v + 0.5 * dt * acc
+        t0 = time.perf_counter(); du = O.ref_get_dU(0, n, pos, v, rho, P, c, h, m, dv, cv, 1.0); t["dudt"] = time.perf_counter() - t0
+        u = u + dt * du
+        times.append(sum(t.values()))
+        for k, val in t.items():
+            phases[k] = phases.get(k, 0.0) + val / steps
+    return float(np.mean(times)), {k: round(val, 4) for k, val in phases.items()}
+
+
 def reference_arm(a, rank):
     if rank != 0:
         return
     from oracle import oracle as O
     thr = O.num_threads()
     rpt = 32
+    full_s, full_phases = cpu_reference_full_step()
     for _ in range(a.warmup):
         cpu_reference_sample(a.n, rpt)
     steps = []
@@ -180,6 +224,11 @@ def reference_arm(a, rank):
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "phase_s_extrapolated": info["phase_s"],
+        "cfg0_measured": {"n": 10_000, "s_per_step": full_s,
+                          "particle_steps_per_s": 10_000 / full_s, "threads": thr,
+                          "phase_s": full_phases,
+                          "what": "every row of the reference CPU step at N = 10,000, 3 steps, "
+                                  "oracle C restatement, measured (not extrapolated)"},
     }
     print(json.dumps(line))
 
@@ -285,9 +334,9 @@ def main():
     # low-priority stream beside them
     stream = torch.cuda.Stream(priority=-10)
 
-    def make(precision, flags=0, vel=None):
+    def make(precision, flags=0, vel=None, walk=None):
         cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf,
-                     ngb_lanes=a.lanes, flags=flags, **walk_kw(a, precision))
+                     ngb_lanes=a.lanes, flags=flags, **(walk or walk_kw(a, precision)))
         c = Context(cfg)
         c.set_stream(stream.cuda_stream)
         c.load(d["pos"], d["vel"] if vel is None else vel, d["m"], d["h"], d["u"])
@@ -414,10 +463,48 @@ def main():
         ms64 = timed_steps(ctx64, max(2, a.steps // 2), a.warmup)
         k64 = max(2, a.steps // 2)
         fp64 = {"value": world * n * k64 / (ms64 * 1e-3), "ms_per_step": ms64 / k64, "steps": k64,
-                "phases_ms": ctx64.phase_times()}
+                "phases_ms": ctx64.phase_times(), "walk": walk_kw(a, "fp64")}
         ctx64.close()
+        # the same step in mixed precision with the FP64 arm's walk (theta
+        # alone, no expansions, super-groups or small-cell angle): the
+        # precision's own gain, algorithm for algorithm
+        ctx_s = make("mixed", L.FLAG_TIMING, walk=walk_kw(a, "fp64"))
+        ms_s = timed_steps(ctx_s, k64, a.warmup)
+        same_walk = {"value": world * n * k64 / (ms_s * 1e-3), "ms_per_step": ms_s / k64,
+                     "steps": k64, "phases_ms": ctx_s.phase_times(), "walk": walk_kw(a, "fp64")}
+        ctx_s.close()
     else:
-        fp64 = None
+        fp64 = same_walk = None
+
+    # ---- opening angles theta in {0.4, 0.5, 0.7} at N = 1M: both precisions
+    # with the plain walk, time per step and gravity error against the FP64
+    # direct sum on the seeded subset ----
+    theta_rows = []
+    if not a.no_fp64 and not a.no_theta_table:
+        sub = np.random.default_rng(7).choice(n, min(a.err_subset, n), replace=False)
+        ref = make("fp64")
+        inv = np.empty(n, np.int64)
+        inv[ref.ids()] = np.arange(n)
+        ad, _ = ref.gravity_direct(inv[sub].astype(np.int32))
+        ref.close()
+        kt = max(2, a.steps // 5)
+        for th in (0.4, 0.5, 0.7):
+            row = {"theta": th}
+            for prec in ("mixed", "fp64"):
+                c = make(prec, walk=dict(theta=th))
+                row[f"grav_err_{prec}"] = rms_rel(c.get_acc("grav")[sub], ad)
+                msx = timed_steps(c, kt, max(2, a.warmup // 2))
+                row[f"ms_per_step_{prec}"] = msx / kt
+                row[f"value_{prec}"] = world * n * kt / (msx * 1e-3)
+                c.close()
+            row["mixed_over_fp64"] = row["value_mixed"] / row["value_fp64"]
+            theta_rows.append(row)
+
+    # ---- the 64-cloud ensemble (log-uniform 20k-500k particles per cloud),
+    # one launch per phase over every cloud ----
+    ens = None
+    if not a.no_ensemble:
+        ens = ensemble_run(a, stream, timed_steps)
 
     # ---- energy and momentum drift over 100 steps, N = 10,000 Evrard (the
     # plain FP64 method's own configuration: theta 0.5, Courant 0.25) ----
@@ -501,7 +588,13 @@ def main():
         "gpu_launches": kernels_per_step * a.steps,
         "clocks": clocks,
         "fp64_plain": fp64,
-        "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+        "mixed_same_walk": same_walk,
+        "mixed_over_fp64": (same_walk["value"] / fp64["value"]) if fp64 else None,
+        "mixed_over_fp64_definition": ("same algorithm: the mixed step with the FP64 arm's "
+                                       "walk settings over the FP64 plain step"),
+        "mixed_over_fp64_tuned_walk": (value / fp64["value"]) if fp64 else None,
+        "theta_table_1M": theta_rows,
+        "ensemble": ens,
         "accel_err": err,
         "conservation_100_steps_n10k": conservation,
         "phases_ms": phases,
@@ -515,6 +608,38 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def ensemble_run(a, stream, timed, rank=0, world=1):
+    """The batched ensemble of a.clouds independent Evrard spheres (counts
+    log-uniform in [20k, 500k], mass, radius and u0 jittered by 20 %), each
+    with its own tree and time step, all advanced by the same launches;
+    clouds sharded over the ranks by LPT when world > 1."""
+    from sph_2_b200 import Config, Context, ic
+    from sph_2_b200.distributed import local_ensemble, shard_clouds
+    e = ic.ensemble(n_clouds=a.clouds, seed=42)
+    owner = shard_clouds(e["counts"], world)
+    mine = local_ensemble(e, owner, rank)
+    n = len(mine["m"])
+    ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
+                         leaf_size=a.leaf, ngb_lanes=a.lanes, **walk_kw(a, "mixed")))
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
+    ctx.prologue()
+    tuned = None
+    if a.tune:
+        from sph_2_b200.autotune import tune
+        tuned = tune(ctx)[0]
+    k = max(2, a.steps // 4)
+    ms = timed(ctx, k, a.warmup)
+    total = int(e["counts"].sum())
+    out = {"value": total * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+           "workload": f"ensemble_{a.clouds}_clouds", "particles": total, "clouds": a.clouds,
+           "per_rank_particles": n, "status": ctx.status(), "tuned": tuned,
+           "launch_params": {"ngb_lanes": ctx.config.ngb_lanes, "block_size": ctx.config.block_size,
+                             "leaf_size": ctx.config.leaf_size}}
+    ctx.close()
+    return out
 
 
 def large_evrard(a, stream, timed):
@@ -583,7 +708,6 @@ def extra_workload(a, world, rank, local):
     import torch.distributed as dist
     from sph_2_b200 import Config, Context, cooling, ic
     from sph_2_b200 import _lib as L
-    from sph_2_b200.distributed import local_ensemble, shard_clouds
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -617,26 +741,13 @@ def extra_workload(a, world, rank, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "fp32+fp64 (mixed)", "data": "synthetic"}
     if a.workload == "ensemble":
-        e = ic.ensemble(n_clouds=a.clouds, seed=42)
-        owner = shard_clouds(e["counts"], world)
-        mine = local_ensemble(e, owner, rank)
-        n = len(mine["m"])
-        ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
-                             leaf_size=a.leaf, ngb_lanes=a.lanes, **walk_kw(a, "mixed")))
-        ctx.set_stream(stream.cuda_stream)
-        ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
-        ctx.prologue()
-        if a.tune:
-            from sph_2_b200.autotune import tune
-            out["tuned"] = tune(ctx)[0]
-        ms = timed(ctx, a.steps, a.warmup)
-        total = int(e["counts"].sum())
-        out.update(value=total * a.steps / (ms * 1e-3), ms_per_step=ms / a.steps,
-                   config={"workload": f"ensemble_{a.clouds}_clouds", "particles": total,
+        r = ensemble_run(a, stream, timed, rank, world)
+        out.update(value=r["value"], ms_per_step=r["ms_per_step"],
+                   config={"workload": r["workload"], "particles": r["particles"],
                            "clouds": a.clouds, "theta": a.theta,
                            "parallelism": f"clouds sharded over {world} ranks (LPT)",
-                           "per_rank_particles": n},
-                   status=ctx.status())
+                           "per_rank_particles": r["per_rank_particles"]},
+                   status=r["status"], tuned=r["tuned"], launch_params=r["launch_params"])
     elif a.workload == "large":
         out.update(large_evrard(a, stream, timed))
     else:

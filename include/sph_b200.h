@@ -51,6 +51,9 @@ extern "C" {
                              positions, integration, h convergence, reductions       */
 #define SPH_AV_MG83 0     /* Monaghan & Gingold 1983 (libsx.py:185-262)              */
 #define SPH_AV_GADGET 1   /* signal-velocity form (shear.py:243-330, hfvCLibs:705)   */
+#define SPH_DT_COURANT 0  /* dt = courant min_i min(h/v_sig, sqrt(h/|a|)) per cloud  */
+#define SPH_DT_INDIVIDUAL 1 /* dt = min_i of the six per-particle estimates of
+                             sph_dt_individual, per cloud                       */
 
 /* fields for sph_get_field / sph_set_field (FP64 unless noted) */
 #define SPH_F_X 0
@@ -134,7 +137,8 @@ typedef struct sph_config {
     int32_t small_cell;   /* see theta_small; the error it adds follows the
                              cells' mass fraction: 128 was tuned at N = 1M
                              (theta 0.36, theta_small 0.45), scale it with N  */
-    int32_t reserved0;    /* 0                                                 */
+    int32_t dt_mode;      /* time step of sph_step and sph_prologue when dt_fixed
+                             is 0: SPH_DT_COURANT or SPH_DT_INDIVIDUAL         */
 } sph_config;
 
 typedef struct sph_ctx sph_ctx;
@@ -265,6 +269,21 @@ int sph_update_u(sph_ctx *ctx, int32_t first);
  * (dt_array_indiv_dt, hfvCLibs:999-1078, over neighbours only); stored as
  * the step of the next sph_step and returned in dt (per cloud) if not NULL */
 int sph_cfl_dt(sph_ctx *ctx, double *dt);
+/* Individual time steps (replaces dt_array_indiv_dt, hfvCLibs_v7_hfv_v2.h:
+ * 999-1078, and the min_finder of EVR.cu:1733): for every particle the
+ * smallest of C h / max_j v_sig,ij, C h / (h |div v| + max(c, |v|)(1 + 0.6
+ * alpha)), 0.4 sqrt(eps / |a|), 0.4 eps / |v|, sqrt(h / |a_grav|) and
+ * sqrt(h / |a|), with v_sig,ij = c_i + c_j - 3 v_ij.r_ij / (|r_ij| + 1e-5)
+ * maximised over the particle's neighbour list (the reference loops over all
+ * N particles) and C = courant, eps the Plummer softening, a = a_sph +
+ * a_grav; dh/dt = h div v / 3 with div v signed.  The per-cloud minimum is
+ * stored as the next step (dt_fixed still wins) and returned by sph_get_dt.
+ * bin[i] = the smallest k >= 0 with dt_ref / 2^k <= dt[i] (dt_ref = dt_max if
+ * set, else the cloud's largest dt[i]; -1 for a particle without a finite
+ * positive step).  dt, dhdt and bin (each may be NULL) receive n values in
+ * the caller's original order.  Needs the lists, density and accelerations
+ * of the current state (sph_prologue or sph_step). */
+int sph_dt_individual(sph_ctx *ctx, double *dt, double *dhdt, int32_t *bin, int32_t host);
 /* totals: [KE, U, PE, px, py, pz, Lx, Ly, Lz, M] (getKE/getPE, libsx.py:571-620);
  * PE needs SPH_FLAG_POTENTIAL in the last gravity call */
 int sph_energies(sph_ctx *ctx, double *out10);

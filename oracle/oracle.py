@@ -59,6 +59,7 @@ def lib():
             "orc_divcurl_list": [I, f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p, i64p, i32p, f64p, f64p],
             "orc_force_list": [I] + [f64p] * 13 + [D, D, D, I, I, i64p, i32p, vp, vp, vp, vp, vp],
             "orc_grav_direct": [I, f64p, f64p, f64p, f64p, vp, D, D, I, i32p, f64p, f64p, f64p, vp],
+            "orc_dt_individual": [I] + [f64p] * 12 + [D, D, D, i64p, i32p, f64p, f64p],
             "orc_build_radix_tree": [I, u64p, i32p, i32p, i32p, i32p],
             "orc_tree_moments": [I, i32p, i32p, i32p, C.c_void_p, f64p, f64p, f64p, f64p, f64p,
                                  f64p, f64p],
@@ -300,6 +301,21 @@ def courant_dt(h, vsig, acc, courant, cloud=None):
     out = np.full(int(cl.max()) + 1 if len(cl) else 1, np.inf)
     np.minimum.at(out, cl[ok], t[ok])
     return out
+
+
+def dt_individual(x, y, z, vx, vy, vz, m, h, rho, c, asph, agrav, eps, courant, alpha, off,
+                  lst):
+    """Per-particle steps and dh/dt of dt_array_indiv_dt
+    (hfvCLibs_v7_hfv_v2.h:999-1078) over the neighbour lists (see
+    orc_dt_individual).  asph, agrav: (n, 3)."""
+    n = len(x)
+    dt, dh = np.zeros(n), np.zeros(n)
+    a_s = _c(np.asarray(asph, float).T.reshape(-1))
+    a_g = _c(np.asarray(agrav, float).T.reshape(-1))
+    lib().orc_dt_individual(n, _c(x), _c(y), _c(z), _c(vx), _c(vy), _c(vz), _c(m), _c(h),
+                            _c(rho), _c(c), a_s, a_g, eps, courant, alpha,
+                            _c(off, np.int64), _c(lst, np.int32), dt, dh)
+    return dt, dh
 
 
 def grav_direct(x, y, z, m, G, eps, targets, cloud=None):

@@ -658,6 +658,54 @@ void orc_force_list(int N, const double *x, const double *y, const double *z, co
     }
 }
 
+/* Individual time steps: dt_array_indiv_dt (Particles_in_BH_Tree_II/
+ * Evrard_test/hfvCLibs_v7_hfv_v2.h:999-1078) restated in FP64 with its
+ * signal-velocity maximum (from 0, self included) over the neighbour list
+ * instead of all N particles; the six estimates
+ *   C h / vsig_max, C h / (h |div| + max(c, |v|)(1 + 0.6 alpha)),
+ *   0.4 sqrt(eps / |a|), 0.4 eps / |v|, sqrt(h / |a_grav|), sqrt(h / |a|)
+ * and dh/dt = h div / 3 (:1071-1076) with the signed divergence
+ * div = -(1/rho_i) sum_j m_j v_ij . gradW_ij over the same list. */
+void orc_dt_individual(int N, const double *x, const double *y, const double *z, const double *vx,
+                       const double *vy, const double *vz, const double *m, const double *h,
+                       const double *rho, const double *c, const double *asph,
+                       const double *agrav, double eps, double C, double alpha,
+                       const int64_t *off, const int *lst, double *dt, double *dhdt)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < N; i++) {
+        double vs = 0.0, s = 0.0;
+        for (int64_t k = off[i]; k < off[i + 1]; k++) {
+            int j = lst[k];
+            double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+            double rr = sqrt(dx * dx + dy * dy + dz * dz);
+            double ux = vx[i] - vx[j], uy = vy[i] - vy[j], uz = vz[i] - vz[j];
+            double vr = ux * dx + uy * dy + uz * dz;
+            double w = vr / (rr + 1e-5);
+            double v = c[i] + c[j] - 3.0 * w;
+            if (v > vs) vs = v;
+            s -= m[j] * gradw_m4(rr, 0.5 * (h[i] + h[j])) * vr;
+        }
+        double div = s / rho[i];
+        double gx = agrav[i], gy = agrav[N + i], gz = agrav[2 * (size_t)N + i];
+        double tx = asph[i] + gx, ty = asph[N + i] + gy, tz = asph[2 * (size_t)N + i] + gz;
+        double ag = sqrt(gx * gx + gy * gy + gz * gz), at = sqrt(tx * tx + ty * ty + tz * tz);
+        double va = sqrt(vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+        double e[6];
+        e[0] = C * h[i] / vs;
+        e[1] = C * h[i] / (h[i] * fabs(div) + fmax(c[i], va) * (1.0 + 0.6 * alpha));
+        e[2] = 0.4 * sqrt(eps / at);
+        e[3] = 0.4 * eps / va;
+        e[4] = sqrt(h[i] / ag);
+        e[5] = sqrt(h[i] / at);
+        double d = e[0];
+        for (int q = 1; q < 6; q++)
+            if (e[q] <= d) d = e[q];
+        dt[i] = d;
+        dhdt[i] = h[i] * div / 3.0;
+    }
+}
+
 /* --- Plummer direct summation (FP64) ----------------------------------- */
 void orc_grav_direct(int N, const double *x, const double *y, const double *z, const double *m,
                      const int *cloud, double G, double eps, int ntarget, const int *targets,

@@ -21,6 +21,7 @@ ERRORS = {
 }
 PREC = {"fp64": 0, "mixed": 1}
 AV = {"mg83": 0, "gadget": 1}
+DT_MODE = {"courant": 0, "individual": 1}
 FIELDS = ["x", "y", "z", "vx", "vy", "vz", "m", "h", "u", "rho", "P", "c", "divV", "curlV",
           "ax_sph", "ay_sph", "az_sph", "ax_grav", "ay_grav", "az_grav", "dudt", "vsig", "pot",
           "dudt_prev", "u_prev"]
@@ -49,7 +50,7 @@ class SphConfig(C.Structure):
         ("alpha", C.c_double), ("beta", C.c_double), ("eta", C.c_double), ("G", C.c_double),
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),
         ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
-        ("theta_small", C.c_double), ("small_cell", C.c_int32), ("reserved0", C.c_int32),
+        ("theta_small", C.c_double), ("small_cell", C.c_int32), ("dt_mode", C.c_int32),
     ]
 
 
@@ -106,6 +107,7 @@ SIGNATURES = [
     ("sph_drift", C.c_int, [_P]),
     ("sph_update_u", C.c_int, [_P, _I]),
     ("sph_cfl_dt", C.c_int, [_P, _P]),
+    ("sph_dt_individual", C.c_int, [_P, _P, _P, _P, _I]),
     ("sph_energies", C.c_int, [_P, _P]),
     ("sph_get_far_cells", C.c_int, [_P, _P]),
     ("sph_get_supergroup_stats", C.c_int, [_P, _P]),

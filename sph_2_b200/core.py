@@ -49,7 +49,7 @@ class Config:
     theta_local: float = 0.0
     theta_small: float = 0.0
     small_cell: int = 0
-    reserved0: int = 0
+    dt_mode: str = "courant"
 
     def to_c(self) -> L.SphConfig:
         c = L.SphConfig()
@@ -59,6 +59,8 @@ class Config:
                 v = L.PREC[v]
             elif f.name == "av_mode":
                 v = L.AV[v]
+            elif f.name == "dt_mode":
+                v = L.DT_MODE[v]
             elif f.name == "balsara":
                 v = int(bool(v))
             setattr(c, f.name, v)
@@ -326,6 +328,18 @@ class Context:
         out = np.zeros(max(self.n_clouds, 1))
         self._chk(self._L.sph_cfl_dt(self._h, _ptr(out)), "sph_cfl_dt")
         return out
+
+    def dt_individual(self) -> dict:
+        """Per-particle steps of the reference's six criteria over the
+        neighbour lists (dt_array_indiv_dt, hfvCLibs_v7_hfv_v2.h:999-1078),
+        dh/dt and power-of-two bins, in original order; the per-cloud minimum
+        becomes the next step."""
+        n = self.n
+        dt, dh = np.zeros(n), np.zeros(n)
+        b = np.zeros(n, np.int32)
+        self._chk(self._L.sph_dt_individual(self._h, _ptr(dt), _ptr(dh), _ptr(b), 1),
+                  "sph_dt_individual")
+        return {"dt": dt, "dhdt": dh, "bin": b}
 
     def energies(self) -> dict:
         out = np.zeros(10)

@@ -63,6 +63,11 @@ __global__ void k_scatter_by_id(int n, const int *__restrict__ id, const double 
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < n) dst[id[s]] = src[s];
 }
+__global__ void k_scatter_int_by_id(int n, const int *__restrict__ id, const int *__restrict__ src,
+                                    int *__restrict__ dst) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) dst[id[s]] = src[s];
+}
 __global__ void k_gather_by_id(int n, const int *__restrict__ id, const double *__restrict__ src,
                                double *__restrict__ dst) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -88,6 +93,7 @@ int check_cfg(const sph_config *c) {
     if (!(c->theta_small >= 0.0 && c->theta_small < 1.0) || c->small_cell < 0) return SPH_ERR_ARG;
     if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
     if (!(c->courant > 0.0)) return SPH_ERR_ARG;
+    if (c->dt_mode != SPH_DT_COURANT && c->dt_mode != SPH_DT_INDIVIDUAL) return SPH_ERR_ARG;
     return SPH_OK;
 }
 
@@ -183,7 +189,8 @@ int step_body(sph_ctx *ctx) {
     if ((rc = launch_forces(ctx, true, fused, false))) return rc;
     MARK(8, ctx->stream);
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
-    if ((rc = launch_kick(ctx, 0.5, ctx->cfg.dt_fixed <= 0.0))) return rc;
+    const bool courant = ctx->cfg.dt_fixed <= 0.0 && ctx->cfg.dt_mode == SPH_DT_COURANT;
+    if ((rc = launch_kick(ctx, 0.5, courant))) return rc;
     MARK(9, ctx->stream);
     if (!fused)
         if ((rc = launch_forces(ctx, false, true, false))) return rc;
@@ -194,6 +201,8 @@ int step_body(sph_ctx *ctx) {
         else rc = launch_cooling_exact(ctx);
         if (rc) return rc;
     }
+    if (ctx->cfg.dt_fixed <= 0.0 && ctx->cfg.dt_mode == SPH_DT_INDIVIDUAL)
+        if ((rc = launch_dt_individual(ctx))) return rc;
     rc = launch_dt_commit(ctx);
     MARK(11, ctx->stream);
     return rc;
@@ -320,7 +329,8 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->cand_cnt, N);
     DAF(ctx->lflag, N + 2);
     DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N);
-    DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C);
+    DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C); DAF(ctx->dtmax_bits, C);
+    DAF(ctx->dt_part, N); DAF(ctx->dhdt, N); DAF(ctx->dbin, N);
     DAF(ctx->status, SPH_NSTATUS);
     DAF(ctx->counters, 5);
     if (ctx->cfg.precision == SPH_PREC_MIXED && ctx->cfg.theta_local > 0.0) {
@@ -403,6 +413,7 @@ int sph_set_params(sph_ctx *ctx, const sph_config *c) {
     t.ngb_lanes = c->ngb_lanes; t.block_size = c->block_size; t.leaf_size = c->leaf_size;
     t.walk_blocks = c->walk_blocks;
     t.theta_small = c->theta_small; t.small_cell = c->small_cell;
+    t.dt_mode = c->dt_mode;
     int rc = check_cfg(&t);
     if (rc) return rc;
     if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size ||
@@ -801,6 +812,38 @@ int sph_cfl_dt(sph_ctx *ctx, double *dt) {
     return SPH_OK;
 }
 
+int sph_dt_individual(sph_ctx *ctx, double *dt, double *dhdt, int32_t *bin, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->lists_ok || !ctx->rho_ok) return SPH_ERR_STATE;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    if ((rc = launch_dt_individual(ctx))) return rc;
+    if ((rc = launch_dt_bins(ctx))) return rc;
+    if ((rc = launch_dt_commit(ctx))) return rc;
+    const int n = ctx->n;
+    cudaStream_t s = ctx->stream;
+    const cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const int *id = ctx->id[ctx->cur];
+    double *buf = ctx->red;
+    if (n > 0 && dt) {
+        k_scatter_by_id<<<div_up(n, 256), 256, 0, s>>>(n, id, ctx->dt_part, buf);
+        CK(cudaMemcpyAsync(dt, buf, sizeof(double) * n, k, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    if (n > 0 && dhdt) {
+        k_scatter_by_id<<<div_up(n, 256), 256, 0, s>>>(n, id, ctx->dhdt, buf);
+        CK(cudaMemcpyAsync(dhdt, buf, sizeof(double) * n, k, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    if (n > 0 && bin) {
+        k_scatter_int_by_id<<<div_up(n, 256), 256, 0, s>>>(n, id, ctx->dbin, (int *)buf);
+        CK(cudaMemcpyAsync(bin, buf, sizeof(int) * n, k, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "dt_individual");
+}
+
 int sph_energies(sph_ctx *ctx, double *out10) {
     int rc = enter(ctx);
     if (rc) return rc;
@@ -857,8 +900,14 @@ int sph_prologue(sph_ctx *ctx) {
     if ((rc = launch_neighbours(ctx))) return rc;
     if ((rc = launch_density_divcurl(ctx))) return rc;
     if ((rc = launch_forces(ctx, true, true, false))) return rc;
-    // first dt (fixed or Courant), then u += du/dt dt (sph_mpi4_v4.py:240-244)
-    if ((rc = launch_cfl(ctx))) return rc;
+    // first dt (fixed, Courant or individual), then u += du/dt dt
+    // (sph_mpi4_v4.py:240-244)
+    if (ctx->cfg.dt_fixed <= 0.0 && ctx->cfg.dt_mode == SPH_DT_INDIVIDUAL) {
+        if ((rc = launch_dt_individual(ctx))) return rc;
+        if ((rc = launch_dt_commit(ctx))) return rc;
+    } else if ((rc = launch_cfl(ctx))) {
+        return rc;
+    }
     if ((rc = launch_update_u(ctx, true))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->prologue_done = true;

@@ -22,25 +22,6 @@ __device__ __forceinline__ double courant_dt(double hi, double vs, double ax, do
     return (t > 0.0 && isfinite(t)) ? t : 0.0;
 }
 
-// per-cloud minimum of t over the warp: one atomic per warp when the warp
-// holds one cloud (clouds are contiguous in storage order), else one per
-// lane.  Every lane of the warp calls; t = 0 marks a lane with no estimate.
-__device__ __forceinline__ void cloud_min(unsigned long long *dt_bits, bool valid, int c, double t) {
-    unsigned long long v = (valid && t > 0.0) ? dbl_to_ord(t) : ~0ULL;
-    const int cc = valid ? c : -1;
-    const int c0 = __shfl_sync(0xffffffffu, cc, 0);
-    if (__all_sync(0xffffffffu, !valid || cc == c0)) {
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-            v = w < v ? w : v;
-        }
-        if ((threadIdx.x & 31) == 0 && v != ~0ULL) atomicMin(&dt_bits[c0], v);
-    } else if (v != ~0ULL) {
-        atomicMin(&dt_bits[cc], v);
-    }
-}
-
 template <class R>
 __global__ void k_kick(int n, double *__restrict__ vx, double *__restrict__ vy,
                        double *__restrict__ vz, const double *__restrict__ asph,

@@ -117,6 +117,9 @@ struct sph_ctx {
     // time step, status, counters
     double *dt = nullptr, *dt_next = nullptr;  // per cloud
     unsigned long long *dt_bits = nullptr;     // per cloud ordered min
+    unsigned long long *dtmax_bits = nullptr;  // per cloud ordered max of the individual steps
+    double *dt_part = nullptr, *dhdt = nullptr; // per particle: individual step, dh/dt
+    int *dbin = nullptr;                        // per particle: power-of-two bin of its step
     long long *status = nullptr;               // SPH_NSTATUS
     unsigned long long *counters = nullptr;    // walk: cells, particles
     unsigned *work = nullptr;                  // work counters for persistent kernels (16)
@@ -253,6 +256,25 @@ __device__ __forceinline__ void status_add(long long *status, int which, long lo
     atomicAdd((unsigned long long *)&status[which], (unsigned long long)v);
 }
 
+// per-cloud minimum of t over the warp: one atomic per warp when the warp
+// holds one cloud (clouds are contiguous in storage order), else one per
+// lane.  Every lane of the warp calls; t = 0 marks a lane with no estimate.
+__device__ __forceinline__ void cloud_min(unsigned long long *dt_bits, bool valid, int c, double t) {
+    unsigned long long v = (valid && t > 0.0) ? dbl_to_ord(t) : ~0ULL;
+    const int cc = valid ? c : -1;
+    const int c0 = __shfl_sync(0xffffffffu, cc, 0);
+    if (__all_sync(0xffffffffu, !valid || cc == c0)) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w < v ? w : v;
+        }
+        if ((threadIdx.x & 31) == 0 && v != ~0ULL) atomicMin(&dt_bits[c0], v);
+    } else if (v != ~0ULL) {
+        atomicMin(&dt_bits[cc], v);
+    }
+}
+
 // ---- host-side launch helpers implemented per translation unit ----
 int launch_sort(sph_ctx *ctx);
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
@@ -283,6 +305,9 @@ int launch_drift(sph_ctx *ctx);
 int launch_kick_drift(sph_ctx *ctx);
 int launch_update_u(sph_ctx *ctx, bool first);
 int launch_cfl(sph_ctx *ctx);
+int launch_dt_individual(sph_ctx *ctx);
+int launch_dt_bins(sph_ctx *ctx);
+int launch_dt_commit(sph_ctx *ctx);
 int launch_energies(sph_ctx *ctx, double *out10_host);
 int launch_pack_p1(sph_ctx *ctx);
 int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap);

@@ -251,3 +251,41 @@ def test_courant_dt_vs_oracle(precision, tol):
     dt_o = O.courant_dt(h, vs, a, 0.25, cl)
     assert len(dt_gpu) == 3 and np.all(dt_gpu > 0)
     assert np.max(np.abs(dt_gpu / dt_o - 1)) < tol
+
+
+# ------------------------------------------------- individual time steps ---
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 2e-5)])
+def test_individual_dt_vs_oracle(precision, tol):
+    """Per-particle steps of the reference's six criteria (dt_array_indiv_dt)
+    over the neighbour lists, dh/dt and the power-of-two bins, after a
+    prologue and two steps run with the individual step, against the
+    oracle's restatement on the state the step left behind."""
+    n = 10_000
+    d = ic.evrard(n, seed=42)
+    ctx = Context(Config(n_max=n, precision=precision, theta=0.5, dt_mode="individual",
+                         courant=0.25, alpha=1.0))
+    ctx.load(d["pos"], infall(d), d["m"], d["h"], d["u"])
+    ctx.prologue()
+    ctx.step(2)
+    ctx.sync()
+    dt_step = ctx.dt[0]
+    r = ctx.dt_individual()
+    ids = ctx.ids()
+    x, y, z, m, h = storage(ctx)
+    v = ctx.get_vel(True)
+    off, lst = ctx.neighbour_lists()
+    dto, dho = O.dt_individual(x, y, z, v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy(), m, h,
+                               ctx.get("rho", True), ctx.get("c", True), ctx.get_acc("sph", True),
+                               ctx.get_acc("grav", True), 1e-2, 0.25, 1.0, off, lst)
+    dt_g, dh_g = r["dt"][ids], r["dhdt"][ids]            # storage order
+    assert np.max(np.abs(dt_g / dto - 1)) < tol
+    assert rel(dh_g, dho) < 10 * tol
+    # the step's own dt was the minimum of the same estimates, and the call
+    # stores that minimum again
+    assert abs(dt_step / dto.min() - 1) < tol
+    assert abs(ctx.dt[0] / dto.min() - 1) < tol
+    # bins: ref / 2^k <= dt_i < ref / 2^(k-1), ref = the largest step
+    b = r["bin"]
+    ref = r["dt"].max()
+    assert b.min() >= 0 and np.all(ref / 2.0 ** b <= r["dt"] * (1 + 1e-15))
+    assert np.all((b == 0) | (ref / 2.0 ** (b - 1) > r["dt"]))

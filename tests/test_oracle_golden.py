@@ -140,3 +140,42 @@ def test_docooling_structure_pinned():
     out = np.array([O.do_cooling_f32_with_ref_rate(float(a), float(b), float(c), float(g["XH"]))
                     for a, b, c in zip(g["rho"], g["u_old"], g["dt"])], np.float32)
     assert np.array_equal(out.view(np.uint32), g["u_new"].view(np.uint32))
+
+
+def test_dt_individual_oracle_equals_all_pairs_form():
+    """With every pair inside the lists (h large enough), the oracle's
+    list-restricted individual step equals dt_array_indiv_dt's all-pairs form
+    (hfvCLibs_v7_hfv_v2.h:999-1078, written out here in NumPy, FP64)."""
+    rng = np.random.default_rng(4)
+    n = 40
+    pos = rng.random((n, 3))
+    v = rng.normal(size=(n, 3))
+    m = np.full(n, 1.0 / n)
+    h = np.full(n, 2.0)                       # every |r_ij| <= h_i + h_j
+    c = 0.2 + rng.random(n)
+    asph, agrav = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    x, y, z = (pos[:, k].copy() for k in range(3))
+    off, lst = O.neighbours(x, y, z, h)
+    assert off[-1] == n * n
+    rho = O.density_list(x, y, z, m, h, off, lst)
+    eps, C, alpha = 1e-2, 0.25, 1.0
+    dt, dh = O.dt_individual(x, y, z, v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy(), m, h, rho, c,
+                             asph, agrav, eps, C, alpha, off, lst)
+    d = pos[:, None, :] - pos[None, :, :]
+    rr = np.sqrt(np.sum(d * d, axis=2))
+    u = v[:, None, :] - v[None, :, :]
+    vr = np.sum(u * d, axis=2)
+    vsig = np.maximum(0.0, np.max(c[:, None] + c[None, :] - 3.0 * vr / (rr + 1e-5), axis=1))
+    # signed divergence with the M4 kernel gradient at h_ij
+    hij = 0.5 * (h[:, None] + h[None, :])
+    q = rr / hij
+    nW = np.where(q <= 1.0, (1 / np.pi) / hij ** 5 * (-3.0 + 2.25 * q),
+                  np.where(q <= 2.0, -0.75 / np.pi / hij ** 5 * (2.0 - q) ** 2 / (q + 1e-20), 0.0))
+    div = -np.sum(m[None, :] * nW * vr, axis=1) / rho
+    at = np.linalg.norm(asph + agrav, axis=1)
+    ag = np.linalg.norm(agrav, axis=1)
+    va = np.linalg.norm(v, axis=1)
+    est = np.stack([C * h / vsig, C * h / (h * np.abs(div) + np.maximum(c, va) * (1 + 0.6 * alpha)),
+                    0.4 * np.sqrt(eps / at), 0.4 * eps / va, np.sqrt(h / ag), np.sqrt(h / at)], 1)
+    assert np.allclose(dt, est.min(axis=1), rtol=1e-12, atol=0)
+    assert np.allclose(dh, h * div / 3.0, rtol=1e-10, atol=1e-14)
