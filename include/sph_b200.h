@@ -139,6 +139,11 @@ typedef struct sph_config {
                              (theta 0.36, theta_small 0.45), scale it with N  */
     int32_t dt_mode;      /* time step of sph_step and sph_prologue when dt_fixed
                              is 0: SPH_DT_COURANT or SPH_DT_INDIVIDUAL         */
+    double ext_sigma;     /* > 0: isothermal galaxy potential of this velocity
+                             dispersion added to the gravity, a = -2 sigma^2
+                             r / |r|^2 about the origin (galaxy_isothermal_
+                             potential, hfvCLibs_v7_hfv_v2.h:1215-1235); it is
+                             not part of the potential energy of sph_energies */
 } sph_config;
 
 typedef struct sph_ctx sph_ctx;
@@ -385,6 +390,31 @@ int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
 #define SPH_NOALLOC_MAX_N 262144
 int sph_morton_sort_noalloc(const double *x, const double *y, const double *z, int32_t n,
                             uint64_t *keys, int32_t *perm, void *cuda_stream);
+
+/* ---- outflow injection (outflow_injector2, hfvCLibs_v7_hfv_v2.h:1094-1210) ---- */
+typedef struct sph_outflow_params {
+    double mdot;        /* injected mass per unit time (M_dot_in)                     */
+    double v_in;        /* radial outward speed of the injected particles             */
+    double m_particle;  /* mass of each injected particle (mass_sph_high_res)         */
+    double u_inject;    /* their specific internal energy (u_for_10K_Temp)            */
+    double r_max;       /* radius of the injection sphere about the origin            */
+    double h_first;     /* h of the first pair when nothing was injected before       */
+    uint64_t seed;      /* the pairs' random numbers; vary it from call to call       */
+    int32_t cloud;      /* cloud the pairs join: the last cloud (ncloud - 1)          */
+    int32_t reserved;   /* 0 */
+} sph_outflow_params;
+/* mass = mdot * dt(cloud) + *leftover_mass is spawned as floor(mass / (2 m))
+ * pairs at +r and -r (|r| uniform in [0, r_max), isotropic), with velocities
+ * +-v_in r/|r|, mass m, u = u_inject and h (and softening) of the particle
+ * injected last by an earlier call (h_first before the first one).  The new
+ * particles are appended (original ids n, n+1, ...; sph_count grows) and
+ * join the next step; *leftover_mass (host, in/out) keeps the remainder and
+ * *n_added (host, may be NULL) receives 2 * pairs.  Random numbers come from
+ * SplitMix64 keyed by (seed, pair number), not cuRAND: the distribution is
+ * the reference's, the values are not.  SPH_ERR_CAPACITY (nothing injected)
+ * when n_max would be passed. */
+int sph_outflow_inject(sph_ctx *ctx, const sph_outflow_params *p, double *leftover_mass,
+                       int32_t *n_added);
 
 /* ---- the reference's binary files (host I/O) ---- */
 /* IC file of IC_evrard4.cu:245-260 / readVectorsFromFile

@@ -60,6 +60,8 @@ def lib():
             "orc_force_list": [I] + [f64p] * 13 + [D, D, D, I, I, i64p, i32p, vp, vp, vp, vp, vp],
             "orc_grav_direct": [I, f64p, f64p, f64p, f64p, vp, D, D, I, i32p, f64p, f64p, f64p, vp],
             "orc_dt_individual": [I] + [f64p] * 12 + [D, D, D, i64p, i32p, f64p, f64p],
+            "orc_outflow_pairs": [C.c_uint64, I, D, D] + [f64p] * 6,
+            "orc_isothermal": [I, f64p, f64p, f64p, D, f64p, f64p, f64p],
             "orc_build_radix_tree": [I, u64p, i32p, i32p, i32p, i32p],
             "orc_tree_moments": [I, i32p, i32p, i32p, C.c_void_p, f64p, f64p, f64p, f64p, f64p,
                                  f64p, f64p],
@@ -316,6 +318,22 @@ def dt_individual(x, y, z, vx, vy, vz, m, h, rho, c, asph, agrav, eps, courant, 
                             _c(rho), _c(c), a_s, a_g, eps, courant, alpha,
                             _c(off, np.int64), _c(lst, np.int32), dt, dh)
     return dt, dh
+
+
+def outflow_pairs(seed, npairs, r_max, v_in):
+    """Positions and velocities (2 npairs rows) of the outflow pairs
+    (orc_outflow_pairs; outflow_injector2, hfvCLibs_v7_hfv_v2.h:1094-1210)."""
+    out = [np.zeros(2 * npairs) for _ in range(6)]
+    lib().orc_outflow_pairs(int(seed), int(npairs), float(r_max), float(v_in), *out)
+    return np.stack(out[:3], 1), np.stack(out[3:], 1)
+
+
+def isothermal_acc(x, y, z, sigma):
+    """galaxy_isothermal_potential (hfvCLibs_v7_hfv_v2.h:1215-1235)."""
+    n = len(x)
+    a = [np.zeros(n) for _ in range(3)]
+    lib().orc_isothermal(n, _c(x), _c(y), _c(z), float(sigma), *a)
+    return np.stack(a, 1)
 
 
 def grav_direct(x, y, z, m, G, eps, targets, cloud=None):

@@ -706,6 +706,55 @@ void orc_dt_individual(int N, const double *x, const double *y, const double *z,
     }
 }
 
+/* Outflow pairs of outflow_injector2 (hfvCLibs_v7_hfv_v2.h:1094-1210) with
+ * the project's counter-based uniforms in place of cuRAND: pair j draws
+ * u_k = ((splitmix64(seed + G (3j + k + 1)) >> 11) + 1) 2^-53, k = 0, 1, 2
+ * (G the 64-bit golden-ratio increment, SplitMix64's output function of
+ * Steele, Lea and Flood 2014), then r = u_0 r_max, azimuth 2 pi u_1, polar
+ * angle acos(2 u_2 - 1), velocity v_in along +r; the pair is (+r, +v),
+ * (-r, -v).  Outputs 2 npairs rows. */
+static uint64_t splitmix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+void orc_outflow_pairs(uint64_t seed, int npairs, double r_max, double v_in, double *x, double *y,
+                       double *z, double *vx, double *vy, double *vz)
+{
+    for (int j = 0; j < npairs; j++) {
+        double u[3];
+        for (int k = 0; k < 3; k++) {
+            uint64_t w = splitmix64(seed + 0x9e3779b97f4a7c15ULL * (uint64_t)(3 * (int64_t)j + k + 1));
+            u[k] = (double)((w >> 11) + 1) * 0x1.0p-53;
+        }
+        double rt = u[0] * r_max, th = u[1] * 2.0 * ORC_PI, ph = acos(2.0 * u[2] - 1.0);
+        double sp = sin(ph);
+        double xt = rt * sp * cos(th), yt = rt * sp * sin(th), zt = rt * cos(ph);
+        double rr = sqrt(xt * xt + yt * yt + zt * zt);
+        double s = rr > 0.0 ? v_in / rr : 0.0;
+        for (int side = 0; side < 2; side++) {
+            double sg = side ? -1.0 : 1.0;
+            int i = 2 * j + side;
+            x[i] = sg * xt; y[i] = sg * yt; z[i] = sg * zt;
+            vx[i] = sg * xt * s; vy[i] = sg * yt * s; vz[i] = sg * zt * s;
+        }
+    }
+}
+
+/* galaxy_isothermal_potential (hfvCLibs_v7_hfv_v2.h:1215-1235): M(r) =
+ * 2 sigma^2 r / G, a = -G M(r) x / r^3 = -2 sigma^2 x / r^2 (0 at r = 0) */
+void orc_isothermal(int N, const double *x, const double *y, const double *z, double sigma,
+                    double *ax, double *ay, double *az)
+{
+    for (int i = 0; i < N; i++) {
+        double r2 = x[i] * x[i] + y[i] * y[i] + z[i] * z[i];
+        double f = r2 > 0.0 ? 2.0 * sigma * sigma / r2 : 0.0;
+        ax[i] = -f * x[i]; ay[i] = -f * y[i]; az[i] = -f * z[i];
+    }
+}
+
 /* --- Plummer direct summation (FP64) ----------------------------------- */
 void orc_grav_direct(int N, const double *x, const double *y, const double *z, const double *m,
                      const int *cloud, double G, double eps, int ntarget, const int *targets,

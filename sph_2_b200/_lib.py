@@ -51,6 +51,15 @@ class SphConfig(C.Structure):
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),
         ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
         ("theta_small", C.c_double), ("small_cell", C.c_int32), ("dt_mode", C.c_int32),
+        ("ext_sigma", C.c_double),
+    ]
+
+
+class SphOutflowParams(C.Structure):
+    _fields_ = [
+        ("mdot", C.c_double), ("v_in", C.c_double), ("m_particle", C.c_double),
+        ("u_inject", C.c_double), ("r_max", C.c_double), ("h_first", C.c_double),
+        ("seed", C.c_uint64), ("cloud", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -108,6 +117,7 @@ SIGNATURES = [
     ("sph_update_u", C.c_int, [_P, _I]),
     ("sph_cfl_dt", C.c_int, [_P, _P]),
     ("sph_dt_individual", C.c_int, [_P, _P, _P, _P, _I]),
+    ("sph_outflow_inject", C.c_int, [_P, C.POINTER(SphOutflowParams), _P, _P]),
     ("sph_energies", C.c_int, [_P, _P]),
     ("sph_get_far_cells", C.c_int, [_P, _P]),
     ("sph_get_supergroup_stats", C.c_int, [_P, _P]),

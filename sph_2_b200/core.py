@@ -50,6 +50,7 @@ class Config:
     theta_small: float = 0.0
     small_cell: int = 0
     dt_mode: str = "courant"
+    ext_sigma: float = 0.0
 
     def to_c(self) -> L.SphConfig:
         c = L.SphConfig()
@@ -340,6 +341,20 @@ class Context:
         self._chk(self._L.sph_dt_individual(self._h, _ptr(dt), _ptr(dh), _ptr(b), 1),
                   "sph_dt_individual")
         return {"dt": dt, "dhdt": dh, "bin": b}
+
+    def outflow_inject(self, mdot, v_in, m_particle, u_inject, r_max=1e-3, h_first=1e-3,
+                       seed=0, leftover=0.0, cloud=None):
+        """Spawn mdot * dt + leftover as outflow pairs (outflow_injector2,
+        hfvCLibs_v7_hfv_v2.h:1094-1210); returns (particles added, leftover
+        mass).  The new particles get the next original ids."""
+        p = L.SphOutflowParams(mdot=mdot, v_in=v_in, m_particle=m_particle, u_inject=u_inject,
+                               r_max=r_max, h_first=h_first, seed=int(seed),
+                               cloud=self.n_clouds - 1 if cloud is None else int(cloud))
+        left = C.c_double(leftover)
+        added = C.c_int32(0)
+        self._chk(self._L.sph_outflow_inject(self._h, C.byref(p), C.byref(left), C.byref(added)),
+                  "sph_outflow_inject")
+        return int(added.value), float(left.value)
 
     def energies(self) -> dict:
         out = np.zeros(10)

@@ -94,6 +94,7 @@ int check_cfg(const sph_config *c) {
     if (!(c->eps > 0.0) || !(c->n_ngb > 1.0) || !(c->h_tol > 0.0)) return SPH_ERR_ARG;
     if (!(c->courant > 0.0)) return SPH_ERR_ARG;
     if (c->dt_mode != SPH_DT_COURANT && c->dt_mode != SPH_DT_INDIVIDUAL) return SPH_ERR_ARG;
+    if (!(c->ext_sigma >= 0.0)) return SPH_ERR_ARG;
     return SPH_OK;
 }
 
@@ -343,7 +344,8 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
         DAF(ctx->sgL, (size_t)SG_LSTRIDE * ctx->sg_cap);
     }
     DAF(ctx->work, 16);
-    DAF(ctx->red, std::max<size_t>(2 * N, 8192));
+    DAF(ctx->red, std::max<size_t>(2 * N + 16, 8192));
+    DAF(ctx->st_table, ST_N);
     if (cudaMemsetAsync(ctx->status, 0, SPH_NSTATUS * sizeof(long long), ctx->stream) ||
         cudaMemsetAsync(ctx->pot, 0, N * sizeof(double), ctx->stream) ||
         cudaMemsetAsync(ctx->agrav, 0, 3 * N * sizeof(double), ctx->stream) ||
@@ -414,6 +416,7 @@ int sph_set_params(sph_ctx *ctx, const sph_config *c) {
     t.walk_blocks = c->walk_blocks;
     t.theta_small = c->theta_small; t.small_cell = c->small_cell;
     t.dt_mode = c->dt_mode;
+    t.ext_sigma = c->ext_sigma;
     int rc = check_cfg(&t);
     if (rc) return rc;
     if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size ||
@@ -489,6 +492,7 @@ int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, con
     ctx->p2_dirty = true;
     ctx->prologue_done = false;
     ctx->step_count = 0;
+    ctx->last_injected_id = -1;
     return ctx_check_launch(ctx, "load");
 }
 
@@ -842,6 +846,47 @@ int sph_dt_individual(sph_ctx *ctx, double *dt, double *dhdt, int32_t *bin, int3
     }
     CK(cudaStreamSynchronize(s));
     return ctx_check_launch(ctx, "dt_individual");
+}
+
+int sph_outflow_inject(sph_ctx *ctx, const sph_outflow_params *p, double *leftover_mass,
+                       int32_t *n_added) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!p || !leftover_mass) return SPH_ERR_ARG;
+    if (n_added) *n_added = 0;
+    if (ctx->ncloud < 1 || p->cloud != ctx->ncloud - 1) return SPH_ERR_ARG;
+    if (!(p->m_particle > 0.0) || !(p->mdot >= 0.0) || !(p->r_max >= 0.0) ||
+        !(p->h_first > 0.0) || !(*leftover_mass >= 0.0))
+        return SPH_ERR_ARG;
+    double dt = 0.0;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaMemcpyAsync(&dt, ctx->dt + p->cloud, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double mass = p->mdot * dt + *leftover_mass;
+    const double pairs_d = floor(mass / (2.0 * p->m_particle));
+    if (pairs_d < 0.0 || pairs_d > (double)(ctx->cfg.n_max - ctx->n) / 2.0) return SPH_ERR_CAPACITY;
+    const int npairs = (int)pairs_d;
+    if (npairs > 0) {
+        drop_graphs(ctx);
+        rc = launch_inject_pairs(ctx, npairs, p->seed, p->cloud, p->r_max, p->v_in, p->m_particle,
+                                 p->u_inject, ctx->last_injected_id, p->h_first);
+        if (rc) return rc;
+        const int n1 = ctx->n + 2 * npairs;
+        ctx->cloud_start_h[ctx->ncloud] = n1;
+        CK(cudaMemcpyAsync(ctx->cloud_start + ctx->ncloud, &ctx->cloud_start_h[ctx->ncloud],
+                           sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        ctx->n = n1;
+        ctx->ngroup = n1 + ctx->ncloud;
+        ctx->last_injected_id = n1 - 1;
+        if ((rc = launch_pack_p1(ctx))) return rc;
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = ctx->cand_ok = false;
+        ctx->p2_dirty = true;
+        mass -= 2.0 * p->m_particle * npairs;
+    }
+    *leftover_mass = mass;
+    if (n_added) *n_added = 2 * npairs;
+    return ctx_check_launch(ctx, "outflow_inject");
 }
 
 int sph_energies(sph_ctx *ctx, double *out10) {

@@ -905,6 +905,7 @@ int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot) {
     else
         rc = pot ? run_walk<double, true>(ctx, s) : run_walk<double, false>(ctx, s);
     if (rc) return rc;
+    if ((rc = launch_external_potential(ctx, s))) return rc;
     return ctx_check_launch(ctx, "gravity");
 }
 

@@ -54,6 +54,8 @@ struct sph_ctx {
 
     // persistent state, double buffered
     double *st[2][ST_N] = {};
+    double **st_table = nullptr;  // device copy of one buffer's field pointers
+    int last_injected_id = -1;    // original id of the last particle injected (-1: none)
     int *id[2] = {}, *cloud[2] = {};
     int cur = 0;
 
@@ -305,6 +307,9 @@ int launch_drift(sph_ctx *ctx);
 int launch_kick_drift(sph_ctx *ctx);
 int launch_update_u(sph_ctx *ctx, bool first);
 int launch_cfl(sph_ctx *ctx);
+int launch_external_potential(sph_ctx *ctx, cudaStream_t s);
+int launch_inject_pairs(sph_ctx *ctx, int npairs, unsigned long long seed, int cloud,
+                        double r_max, double v_in, double m, double u, int h_id, double h_first);
 int launch_dt_individual(sph_ctx *ctx);
 int launch_dt_bins(sph_ctx *ctx);
 int launch_dt_commit(sph_ctx *ctx);
