@@ -101,6 +101,8 @@ extern "C" {
 #define SPH_FLAG_NO_GRAPH 8    /* run sph_step eagerly, without CUDA graph replay   */
 #define SPH_FLAG_POTENTIAL 16  /* compute the gravitational potential in the walk   */
 #define SPH_FLAG_TIMING 32     /* record CUDA events between the phases of sph_step */
+#define SPH_FLAG_COOLING_TABLE 64 /* with SPH_FLAG_COOLING: the grid-file backend
+                                  (sph_cooling_table) instead of the implicit solve */
 
 typedef struct sph_config {
     int32_t n_max;        /* particle capacity                                    */
@@ -314,6 +316,32 @@ int sph_cooling_mlp(sph_ctx *ctx);
  * u_old.  iters may be NULL. */
 int sph_cool_solve(sph_ctx *ctx, int32_t n, const double *rho, const double *u_old,
                    const double *dt, double *u_new, int32_t *iters, int32_t host);
+
+/* ---- table cooling with ion fractions (hcoolingx, hfvCLibs_v7_hfv_v2.h:
+ * 1240-1418; grid file coolHeatGridNew.bin read as in
+ * hfvGpuSphBHtree_v3_check_v1_cooling_t3_Evrard.cu:137-179) ---- */
+typedef struct sph_cool_table_params {
+    double unit_rho, unit_u, unit_t; /* code -> cgs                                  */
+    double unit_length;              /* code length in cm                             */
+    double kpc_cm;                   /* 3.086e21                                      */
+    double XH, mH;                   /* n_H = rho X_H / m_H (0.70, 1.6726e-24)        */
+    int32_t z_row;                   /* metallicity row of the grid (the reference: 1) */
+    int32_t reserved;                /* 0 */
+} sph_cool_table_params;
+/* dims6 = N_kpc, N_nH, N_Z, N_T, N_M, N_Time of a grid file, whose size is
+ * checked against them (host only, no GPU) */
+int sph_cooling_table_dims(const char *path, int32_t *dims6);
+/* read the grid file onto the device (replacing an earlier one) */
+int sph_cooling_table_load(sph_ctx *ctx, const char *path, const sph_cool_table_params *p);
+/* new u of every particle over the current dt from the grid: nearest radius
+ * (kpc) and n_H cell, the first u row at or above u and the first time at or
+ * above dt, linear in u between that row and the one below; and the N_M ion
+ * fractions of that cell.  The step applies it with SPH_FLAG_COOLING |
+ * SPH_FLAG_COOLING_TABLE. */
+int sph_cooling_table(sph_ctx *ctx);
+/* ion fractions of the last table cooling, n rows of N_M floats in original
+ * particle order (the snapshot's ionFrac block) */
+int sph_get_ion_frac(sph_ctx *ctx, float *out, int32_t host);
 
 /* ---- cooling-surrogate MLP 3->64->64->1 (GELU), BF16 weights ---- */
 /* parameters in FP32: W1[3*64] b1[64] W2[64*64] b2[64] W3[64] b3[1] and the

@@ -22,6 +22,7 @@ _LIB = None
 
 f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 vp = C.c_void_p
@@ -62,6 +63,7 @@ def lib():
             "orc_dt_individual": [I] + [f64p] * 12 + [D, D, D, i64p, i32p, f64p, f64p],
             "orc_outflow_pairs": [C.c_uint64, I, D, D] + [f64p] * 6,
             "orc_isothermal": [I, f64p, f64p, f64p, D, f64p, f64p, f64p],
+            "orc_cool_table": [i32p, f32p, f32p, f32p, I, I] + [f64p] * 6 + [D] * 7 + [f64p, f32p],
             "orc_build_radix_tree": [I, u64p, i32p, i32p, i32p, i32p],
             "orc_tree_moments": [I, i32p, i32p, i32p, C.c_void_p, f64p, f64p, f64p, f64p, f64p,
                                  f64p, f64p],
@@ -334,6 +336,24 @@ def isothermal_acc(x, y, z, sigma):
     a = [np.zeros(n) for _ in range(3)]
     lib().orc_isothermal(n, _c(x), _c(y), _c(z), float(sigma), *a)
     return np.stack(a, 1)
+
+
+def cool_table(tab, x, y, z, rho, u, dt, unit_rho=1.0, unit_u=1.0, unit_t=1.0, unit_len=1.0,
+               kpc_cm=3.086e21, XH=0.70, mH=1.6726e-24, z_row=1):
+    """hcoolingx (hfvCLibs_v7_hfv_v2.h:1240-1418) on a grid dict of
+    sph_2_b200.cooling.read_table_file: (u_new, ion fractions [n, N_M])."""
+    nk, nt, nh, nz, ntime = tab["u_evol"].shape
+    nm = tab["frac"].shape[4]
+    dims = np.array([nk, nh, nz, nt, nm, ntime], np.int32)
+    grid = np.concatenate([tab[k] for k in ("kpc", "nH", "Z", "T", "time_s")]).astype(np.float32)
+    n = len(x)
+    un = np.zeros(n)
+    ion = np.zeros(n * nm, np.float32)
+    lib().orc_cool_table(dims, grid, _c(tab["u_evol"], np.float32).reshape(-1),
+                         _c(tab["frac"], np.float32).reshape(-1), int(z_row), n, _c(x), _c(y),
+                         _c(z), _c(rho), _c(u), _c(np.broadcast_to(dt, (n,))), unit_rho, unit_u,
+                         unit_t, unit_len, kpc_cm, XH, mH, un, ion)
+    return un, ion.reshape(n, nm)
 
 
 def grav_direct(x, y, z, m, G, eps, targets, cloud=None):

@@ -755,6 +755,63 @@ void orc_isothermal(int N, const double *x, const double *y, const double *z, do
     }
 }
 
+/* Table heating/cooling of hcoolingx (hfvCLibs_v7_hfv_v2.h:1240-1418) in FP64
+ * on the FP32 grid: nearest radius (kpc) and n_H entries (the first grid value
+ * at or above, or the one below when nearer; the last above the grid), the
+ * metallicity row z_row, the first u row at or above u of the column
+ * u_evol[kpc][.][nH][z][0] (the last above it), the first time at or above
+ * dt; u_new linear in u between that row and the one below (the row itself at
+ * the bottom), and the N_M ion fractions of the cell.  dims = N_kpc, N_nH,
+ * N_Z, N_T, N_M, N_Time; grid = kpc, nH, Z, T, time concatenated. */
+static int tab_nearest(const float *g, int n, double v)
+{
+    int k = -1;
+    for (int j = 0; j < n; j++)
+        if (v <= (double)g[j]) { k = j; break; }
+    if (k > 0 && fabs((double)g[k - 1] - v) < fabs((double)g[k] - v)) k -= 1;
+    return k < 0 ? n - 1 : k;
+}
+
+void orc_cool_table(const int *dims, const float *grid, const float *uev, const float *frac,
+                    int z_row, int N, const double *x, const double *y, const double *z,
+                    const double *rho, const double *u, const double *dt, double unit_rho,
+                    double unit_u, double unit_t, double unit_len, double kpc_cm, double XH,
+                    double mH, double *u_new, float *ion)
+{
+    const int nk = dims[0], nh = dims[1], nz = dims[2], nt = dims[3], nm = dims[4], ntime = dims[5];
+    const float *gk = grid, *gh = grid + nk, *gtime = grid + nk + nh + nz + nt;
+    const size_t s_kpc = (size_t)nt * nh * nz * ntime, s_T = (size_t)nh * nz * ntime,
+                 s_nH = (size_t)nz * ntime;
+    for (int i = 0; i < N; i++) {
+        double r = sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        int ik = tab_nearest(gk, nk, r * unit_len / kpc_cm);
+        int ih = tab_nearest(gh, nh, rho[i] * unit_rho * XH / mH);
+        size_t base = ik * s_kpc + ih * s_nH + (size_t)z_row * ntime;
+        double ui = u[i] * unit_u;
+        int iu = -1;
+        for (int j = 0; j < nt; j++)
+            if (ui <= (double)uev[base + j * s_T]) { iu = j; break; }
+        if (iu < 0) iu = nt - 1;
+        double dts = dt[i] * unit_t;
+        int it = -1;
+        for (int j = 0; j < ntime; j++)
+            if (dts <= (double)gtime[j]) { it = j; break; }
+        if (it < 0) it = ntime - 1;
+        double un;
+        if (iu > 0) {
+            double U1 = uev[base + (iu - 1) * s_T], U2 = uev[base + iu * s_T];
+            double e1 = uev[base + (iu - 1) * s_T + it], e2 = uev[base + iu * s_T + it];
+            double fhi = (ui - U1) / (U2 - U1), flo = 1.0 - fhi;
+            un = flo * e1 + fhi * e2;
+        } else {
+            un = uev[base + it];
+        }
+        u_new[i] = un / unit_u;
+        size_t mb = ik * s_kpc * nm + iu * s_T * nm + ih * s_nH * nm + (size_t)z_row * nm * ntime + it;
+        for (int k = 0; k < nm; k++) ion[(size_t)i * nm + k] = frac[mb + (size_t)k * ntime];
+    }
+}
+
 /* --- Plummer direct summation (FP64) ----------------------------------- */
 void orc_grav_direct(int N, const double *x, const double *y, const double *z, const double *m,
                      const int *cloud, double G, double eps, int ntarget, const int *targets,

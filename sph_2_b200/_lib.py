@@ -34,6 +34,7 @@ FLAG_COOLING_MLP = 4
 FLAG_NO_GRAPH = 8
 FLAG_POTENTIAL = 16
 FLAG_TIMING = 32
+FLAG_COOLING_TABLE = 64
 PHASES = ["kick_drift", "sort", "tree", "smoothing_h", "neighbours", "density", "divcurl",
           "forces", "wait_kick", "dudt", "update_dt", "gravity"]
 MLP_NPARAM = 3 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -52,6 +53,14 @@ class SphConfig(C.Structure):
         ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
         ("theta_small", C.c_double), ("small_cell", C.c_int32), ("dt_mode", C.c_int32),
         ("ext_sigma", C.c_double),
+    ]
+
+
+class SphCoolTableParams(C.Structure):
+    _fields_ = [
+        ("unit_rho", C.c_double), ("unit_u", C.c_double), ("unit_t", C.c_double),
+        ("unit_length", C.c_double), ("kpc_cm", C.c_double), ("XH", C.c_double),
+        ("mH", C.c_double), ("z_row", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -126,6 +135,10 @@ SIGNATURES = [
     ("sph_cooling_exact", C.c_int, [_P]),
     ("sph_cooling_mlp", C.c_int, [_P]),
     ("sph_cool_solve", C.c_int, [_P, _I, _P, _P, _P, _P, _P, _I]),
+    ("sph_cooling_table_dims", C.c_int, [C.c_char_p, _P]),
+    ("sph_cooling_table_load", C.c_int, [_P, C.c_char_p, C.POINTER(SphCoolTableParams)]),
+    ("sph_cooling_table", C.c_int, [_P]),
+    ("sph_get_ion_frac", C.c_int, [_P, _P, _I]),
     ("sph_mlp_set", C.c_int, [_P, _P, _P, _I]),
     ("sph_mlp_get", C.c_int, [_P, _P, _P, _I]),
     ("sph_mlp_forward", C.c_int, [_P, _I, _P, _P, _I]),

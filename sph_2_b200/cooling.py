@@ -87,3 +87,77 @@ def train(ctx, Xn, yn, steps=4000, batch=4096, lr=2e-3):
                                 C.byref(loss))
     L.check(rc, "sph_mlp_train", ctx.handle)
     return float(loss.value)
+
+
+# ---- grid files of the table backend ---------------------------------------
+TABLE_DIMS = ("N_kpc", "N_nH", "N_Z", "N_T", "N_M", "N_Time")
+
+
+def write_table_file(path, kpc, nH, Z, T, time_s, u_evol, mu, frac):
+    """Write a heating/cooling grid in the layout of the reference's
+    coolHeatGridNew.bin (read by hfvGpuSphBHtree_v3_check_v1_cooling_t3_
+    Evrard.cu:137-179): int32 N_kpc, N_nH, N_Z, N_T, N_M, N_Time; float32
+    grids kpc, nH, Z, T, time; float32 u_evol and mu [kpc][T][nH][Z][time];
+    float32 ion fractions [kpc][T][nH][Z][M][time]."""
+    kpc, nH, Z, T, time_s = (np.asarray(a, np.float32) for a in (kpc, nH, Z, T, time_s))
+    u_evol = np.asarray(u_evol, np.float32)
+    frac = np.asarray(frac, np.float32)
+    nk, nt, nh, nz, ntime = u_evol.shape
+    nm = frac.shape[4]
+    assert (nk, nh, nz, nt, ntime) == (len(kpc), len(nH), len(Z), len(T), len(time_s))
+    assert frac.shape == (nk, nt, nh, nz, nm, ntime) and np.shape(mu) == u_evol.shape
+    with open(path, "wb") as f:
+        np.array([nk, nh, nz, nt, nm, ntime], np.int32).tofile(f)
+        for a in (kpc, nH, Z, T, time_s, u_evol, np.asarray(mu, np.float32), frac):
+            np.ascontiguousarray(a).tofile(f)
+
+
+def read_table_file(path):
+    """The arrays of a grid file written by write_table_file (or by the
+    reference's own table builder)."""
+    raw = np.fromfile(path, np.uint8)
+    nk, nh, nz, nt, nm, ntime = (int(v) for v in raw[:24].view(np.int32))
+    f = raw[24:].view(np.float32)
+    out, o = {}, 0
+    for name, k in (("kpc", nk), ("nH", nh), ("Z", nz), ("T", nt), ("time_s", ntime)):
+        out[name] = f[o:o + k].copy()
+        o += k
+    c5 = nk * nt * nh * nz * ntime
+    out["u_evol"] = f[o:o + c5].reshape(nk, nt, nh, nz, ntime).copy()
+    o += c5
+    out["mu"] = f[o:o + c5].reshape(nk, nt, nh, nz, ntime).copy()
+    o += c5
+    out["frac"] = f[o:o + c5 * nm].reshape(nk, nt, nh, nz, nm, ntime).copy()
+    return out
+
+
+def synthetic_table(seed=0, n_kpc=4, n_nH=40, n_Z=3, n_T=60, n_M=3, n_time=12, mu=1.22):
+    """A seeded synthetic grid in the reference's layout (the reference's
+    CHIMES-made coolHeatGridNew.bin is not in its repository): radius 0.01-10
+    kpc, n_H 1e-2-1e4 cm^-3, T 1e1-1e8 K, times 1e8-1e14 s; u(t) relaxes from
+    the initial u(T) towards the equilibrium of a cooling time that falls with
+    n_H and is shortest near 1e5 K, and the M ion fractions are a normalised
+    seeded function of (T, n_H)."""
+    rng = np.random.default_rng(seed)
+    kpc = np.logspace(-2, 1, n_kpc)
+    nH = np.logspace(-2, 4, n_nH)
+    Z = np.array([-2.0, -1.0, 0.0][:n_Z] + [0.5] * max(0, n_Z - 3))
+    T = np.logspace(1, 8, n_T)
+    time_s = np.logspace(8, 14, n_time)
+    u0 = u_of_T(T, mu)                                    # [T]
+    u_eq = u_of_T(1e4, mu)
+    lt = np.log10(T)
+    tcool = 1e13 / nH[None, :] * (1.0 + 30.0 * np.exp(-((lt[:, None] - 5.0) / 0.8) ** 2)) ** -1
+    shape = (n_kpc, n_T, n_nH, n_Z, n_time)
+    u_evol = np.empty(shape)
+    for k in range(n_kpc):
+        heat = 1.0 + 0.2 * k
+        for z in range(n_Z):
+            zf = 1.0 + 0.3 * z
+            decay = np.exp(-time_s[None, None, :] * zf / tcool[:, :, None])   # [T, nH, time]
+            u_evol[k, :, :, z, :] = heat * u_eq + (u0[:, None, None] - heat * u_eq) * decay
+    mu_arr = np.full(shape, mu) * (1.0 + 0.05 * rng.random(shape))
+    w = rng.random((n_kpc, n_T, n_nH, n_Z, n_M, n_time)) + 0.1
+    w[:, :, :, :, 0, :] *= (1.0 / (1.0 + (T / 1e4) ** 4))[None, :, None, None, None]
+    frac = w / w.sum(axis=4, keepdims=True)
+    return dict(kpc=kpc, nH=nH, Z=Z, T=T, time_s=time_s, u_evol=u_evol, mu=mu_arr, frac=frac)

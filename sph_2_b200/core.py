@@ -414,6 +414,24 @@ class Context:
     def cooling_mlp(self):
         self._chk(self._L.sph_cooling_mlp(self._h), "cooling_mlp")
 
+    def cooling_table_load(self, path, **params):
+        """Read a heating/cooling grid file in the layout of the reference's
+        coolHeatGridNew.bin (see sph_2_b200.cooling.write_table_file)."""
+        p = L.SphCoolTableParams(unit_rho=1.0, unit_u=1.0, unit_t=1.0, unit_length=1.0,
+                                 kpc_cm=3.086e21, XH=0.70, mH=1.6726e-24, z_row=1)
+        for k, v in params.items():
+            setattr(p, k, v)
+        self._chk(self._L.sph_cooling_table_load(self._h, str(path).encode(), C.byref(p)),
+                  "sph_cooling_table_load")
+
+    def cooling_table(self):
+        self._chk(self._L.sph_cooling_table(self._h), "sph_cooling_table")
+
+    def ion_frac(self, n_species) -> np.ndarray:
+        out = np.zeros((self.n, n_species), np.float32)
+        self._chk(self._L.sph_get_ion_frac(self._h, _ptr(out), 1), "sph_get_ion_frac")
+        return out
+
     # -- cooling surrogate ----------------------------------------------------
     def mlp_set(self, params, norm):
         p = np.ascontiguousarray(params, np.float32)

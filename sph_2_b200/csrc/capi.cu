@@ -198,7 +198,8 @@ int step_body(sph_ctx *ctx) {
     MARK(10, ctx->stream);
     if ((rc = launch_update_u(ctx, false))) return rc;
     if (ctx->cfg.flags & SPH_FLAG_COOLING) {
-        if (ctx->cfg.flags & SPH_FLAG_COOLING_MLP) rc = launch_cooling_mlp(ctx);
+        if (ctx->cfg.flags & SPH_FLAG_COOLING_TABLE) rc = launch_cooling_table(ctx);
+        else if (ctx->cfg.flags & SPH_FLAG_COOLING_MLP) rc = launch_cooling_mlp(ctx);
         else rc = launch_cooling_exact(ctx);
         if (rc) return rc;
     }

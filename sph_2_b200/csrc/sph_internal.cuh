@@ -136,6 +136,12 @@ struct sph_ctx {
     float *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr;
     float *mlp_scratch = nullptr;
     int *cool_list = nullptr;      // surrogate fallback rows (n_max) + their count
+    // table cooling: grids (kpc, nH, Z, T, time), u after each time, ion
+    // fractions, and the ion fractions of the last call per storage slot
+    bool tab_ok = false;
+    sph_cool_table_params tab{};
+    int tab_dims[6] = {};
+    float *tab_grid = nullptr, *tab_uev = nullptr, *tab_frac = nullptr, *ion = nullptr;
     int mlp_step = 0;
     bool mlp_ok = false;
 
@@ -317,6 +323,7 @@ int launch_energies(sph_ctx *ctx, double *out10_host);
 int launch_pack_p1(sph_ctx *ctx);
 int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap);
 int launch_cooling_exact(sph_ctx *ctx);
+int launch_cooling_table(sph_ctx *ctx);
 int launch_cooling_mlp(sph_ctx *ctx);
 int launch_cool_solve(sph_ctx *ctx, int n, const double *rho, const double *u_old,
                       const double *dt, double *u_new, int *iters);

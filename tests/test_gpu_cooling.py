@@ -184,3 +184,43 @@ def test_cooling_collapse_stays_positive():
     st = c.status()
     assert st["nonfinite"] == 0 and st["h_noconv"] == 0 and st["cool_noconv"] == 0
     c.close()
+
+
+# ------------------------------------------------- table backend (hcoolingx) ---
+def test_table_cooling_matches_oracle(tmp_path):
+    """The grid-file backend (hcoolingx, hfvCLibs_v7_hfv_v2.h:1240-1418) on a
+    seeded synthetic grid in the reference's coolHeatGridNew.bin layout: new
+    u and ion fractions bit-exact with the oracle's restatement, inside and
+    outside the grid's ranges; then two steps with the table backend on."""
+    from oracle import oracle as O
+    from sph_2_b200 import Config, Context, cooling, ic
+    from sph_2_b200 import _lib as L
+    path = tmp_path / "coolHeatGridNew.bin"
+    cooling.write_table_file(path, **cooling.synthetic_table(seed=3))
+    tab = cooling.read_table_file(path)
+    n, dt = 5000, 2e-3
+    d = ic.evrard(n, seed=5)
+    rng = np.random.default_rng(9)
+    rho = 10 ** rng.uniform(-3.5, 3.0, n)          # code units; n_H 1e-3 .. 4e4 cm^-3
+    u = 10 ** rng.uniform(-3.0, 3.5, n)
+    units = dict(unit_rho=1.0e-24, unit_u=1.0e10, unit_t=1.0e14, unit_length=3.0 * 3.086e21)
+    ctx = Context(Config(n_max=n, precision="fp64", dt_fixed=dt,
+                         flags=L.FLAG_COOLING | L.FLAG_COOLING_TABLE))
+    ctx.load(d["pos"], d["vel"], d["m"], d["h"], u)
+    ctx.set("rho", rho)
+    ctx.cooling_table_load(path, **units)
+    ctx.cooling_table()
+    un, ion = O.cool_table(tab, *(d["pos"][:, k].copy() for k in range(3)), rho, u, dt,
+                           unit_rho=units["unit_rho"], unit_u=units["unit_u"],
+                           unit_t=units["unit_t"], unit_len=units["unit_length"])
+    assert np.array_equal(ctx.get("u"), un)
+    assert np.array_equal(ctx.ion_frac(tab["frac"].shape[4]), ion)
+    assert np.any(un != u)
+    # in the step: cooling with the table after the u update
+    ctx.load(d["pos"], d["vel"], d["m"], d["h"], np.full(n, 0.05))
+    ctx.prologue()
+    ctx.step(2)
+    ctx.sync()
+    assert np.isfinite(ctx.get("u")).all() and np.all(ctx.get("u") > 0)
+    f = ctx.ion_frac(tab["frac"].shape[4])
+    assert np.allclose(f.sum(axis=1), 1.0, atol=1e-5)

@@ -5,6 +5,7 @@ reference's own readers use (readVectorsFromFile, hfvCLibs_v7_hfv_v2.h:59-101;
 singlex_gpu_data.py:55-72) and compared with this package's writers and
 readers.  sph_ic_count is the library's own header check and needs no GPU.
 """
+import ctypes as C
 import struct
 
 import numpy as np
@@ -87,3 +88,24 @@ def test_library_header_check(tmp_path):
     assert e.value.code == -9
     with pytest.raises(L.SphError):
         ic_count(tmp_path / "missing.bin")
+
+
+def test_cooling_table_file_layout(tmp_path):
+    """The grid file of the table backend: written in the reference's
+    coolHeatGridNew.bin layout, its header and size checked by the library
+    without a GPU, and read back unchanged."""
+    from sph_2_b200 import cooling
+    t = cooling.synthetic_table(seed=1, n_kpc=2, n_nH=5, n_Z=3, n_T=7, n_M=2, n_time=4)
+    p = tmp_path / "grid.bin"
+    cooling.write_table_file(p, **t)
+    dims = np.zeros(6, np.int32)
+    lib = L.load()
+    assert lib.sph_cooling_table_dims(str(p).encode(), dims.ctypes.data_as(C.c_void_p)) == 0
+    assert dims.tolist() == [2, 5, 3, 7, 2, 4]
+    r = cooling.read_table_file(p)
+    for k in ("kpc", "nH", "T", "time_s", "u_evol", "frac"):
+        assert np.array_equal(r[k], np.asarray(t[k], np.float32)), k
+    raw = p.read_bytes()
+    (tmp_path / "short.bin").write_bytes(raw[:-4])
+    assert lib.sph_cooling_table_dims(str(tmp_path / "short.bin").encode(),
+                                      dims.ctypes.data_as(C.c_void_p)) == -9
