@@ -56,8 +56,12 @@ def parse():
     ap.add_argument("--workload", default="evrard", choices=["evrard", "ensemble", "cooling", "large"],
                     help="evrard: the headline line; ensemble / cooling / large: extra workloads")
     ap.add_argument("--clouds", type=int, default=64)
-    ap.add_argument("--tune", action="store_true", help="run the autotuner before timing")
+    ap.add_argument("--tune", action="store_true",
+                    help="run the autotuner before timing the headline (the ensemble is always tuned)")
+    ap.add_argument("--no-tune", action="store_true", help="do not tune the ensemble either")
     ap.add_argument("--no-theta-table", action="store_true")
+    ap.add_argument("--static-grid", action="store_true",
+                    help="group kernels on a grid over the groups instead of the work queue")
     ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
@@ -335,6 +339,8 @@ def main():
     stream = torch.cuda.Stream(priority=-10)
 
     def make(precision, flags=0, vel=None, walk=None):
+        if a.static_grid:
+            flags |= L.FLAG_STATIC_GRID
         cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf,
                      ngb_lanes=a.lanes, flags=flags, **(walk or walk_kw(a, precision)))
         c = Context(cfg)
@@ -627,9 +633,10 @@ def ensemble_run(a, stream, timed, rank=0, world=1):
     ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
     ctx.prologue()
     tuned = None
-    if a.tune:
+    if not a.no_tune:
         from sph_2_b200.autotune import tune
-        tuned = tune(ctx)[0]
+        best, res = tune(ctx, use_cache=False)
+        tuned = {"choice": best, "candidates_ms_per_step": [[ms, p] for ms, p in res]}
     k = max(2, a.steps // 4)
     ms = timed(ctx, k, a.warmup)
     total = int(e["counts"].sum())

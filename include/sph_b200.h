@@ -103,6 +103,9 @@ extern "C" {
 #define SPH_FLAG_TIMING 32     /* record CUDA events between the phases of sph_step */
 #define SPH_FLAG_COOLING_TABLE 64 /* with SPH_FLAG_COOLING: the grid-file backend
                                   (sph_cooling_table) instead of the implicit solve */
+#define SPH_FLAG_STATIC_GRID 128 /* launch the group kernels (walk, searches, h
+                                  iteration) with a grid over the groups instead of
+                                  a persistent grid draining a work queue        */
 
 typedef struct sph_config {
     int32_t n_max;        /* particle capacity                                    */
@@ -390,6 +393,9 @@ int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host);
  *  du/dt, u(+cooling)+dt, gravity (own stream)]; returns the count (12). */
 #define SPH_NPHASE 12
 int sph_get_phase_times(sph_ctx *ctx, float *ms);
+/* run nsteps of sph_step between two CUDA events on the context's stream and
+ * return their device time in ms (the autotuner's clock) */
+int sph_time_steps(sph_ctx *ctx, int32_t nsteps, float *ms);
 /* kernel nodes in the captured step graph (0 before the first graph step) */
 int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
 /* FP32 FMA throughput of this GPU measured by a dependent-chain kernel,

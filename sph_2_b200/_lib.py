@@ -35,6 +35,7 @@ FLAG_NO_GRAPH = 8
 FLAG_POTENTIAL = 16
 FLAG_TIMING = 32
 FLAG_COOLING_TABLE = 64
+FLAG_STATIC_GRID = 128
 PHASES = ["kick_drift", "sort", "tree", "smoothing_h", "neighbours", "density", "divcurl",
           "forces", "wait_kick", "dudt", "update_dt", "gravity"]
 MLP_NPARAM = 3 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -147,6 +148,7 @@ SIGNATURES = [
     ("sph_cool_solve_mlp", C.c_int, [_P, _I, _P, _P, _P, _P, _P]),
     ("sph_debug_copy", C.c_int, [_P, _I, _P, _I]),
     ("sph_get_phase_times", C.c_int, [_P, _P]),
+    ("sph_time_steps", C.c_int, [_P, _I, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),
     ("sph_morton_sort_noalloc", C.c_int, [_P, _P, _P, _I, _P, _P, _P]),

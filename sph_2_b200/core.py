@@ -382,6 +382,13 @@ class Context:
             L.check(rc, "phase_times", self._h)
         return dict(zip(L.PHASES, [float(v) for v in ms]))
 
+    def time_steps(self, nsteps) -> float:
+        """Device time in ms of nsteps of sph_step (CUDA events on the
+        context's stream)."""
+        ms = C.c_float()
+        self._chk(self._L.sph_time_steps(self._h, int(nsteps), C.byref(ms)), "sph_time_steps")
+        return float(ms.value)
+
     def graph_kernel_count(self) -> int:
         c = C.c_int32()
         self._chk(self._L.sph_graph_kernel_count(self._h, C.byref(c)), "graph_kernel_count")

@@ -26,12 +26,30 @@ int ctx_check_launch(sph_ctx *ctx, const char *what) {
 int launch_dt_commit(sph_ctx *ctx);
 
 // blocks for a persistent kernel: every SM filled to its occupancy limit
+// (looked up once per kernel and block size)
 int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem) {
+    const auto key = std::make_pair(kernel, block);
+    auto it = ctx->occupancy.find(key);
+    if (it != ctx->occupancy.end()) return ctx->num_sms * it->second;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
+    ctx->occupancy[key] = per_sm;
     return ctx->num_sms * per_sm;
+}
+
+int queue_launch(sph_ctx *ctx, cudaStream_t s, int slot, const void *kernel, int block,
+                 int static_grid, int *grid, unsigned **queue) {
+    if (ctx->cfg.flags & SPH_FLAG_STATIC_GRID) {
+        *grid = static_grid;
+        *queue = nullptr;
+        return SPH_OK;
+    }
+    *grid = std::min(static_grid, persistent_grid(ctx, kernel, block, 0));
+    *queue = ctx->work + slot;
+    CK(cudaMemsetAsync(*queue, 0, sizeof(unsigned), s));
+    return SPH_OK;
 }
 
 namespace {
@@ -1058,6 +1076,31 @@ int sph_debug_copy(sph_ctx *ctx, int32_t which, void *out, int32_t host) {
     const size_t bytes = (which == 3 ? sizeof(double) : sizeof(int)) * ctx->n;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(out, src, bytes, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    return SPH_OK;
+}
+
+int sph_time_steps(sph_ctx *ctx, int32_t nsteps, float *ms) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ms || nsteps < 0) return SPH_ERR_ARG;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return SPH_ERR_CUDA;
+    }
+    cudaError_t e = cudaEventRecord(a, ctx->stream);
+    if (e == cudaSuccess) rc = sph_step(ctx, nsteps);
+    if (e == cudaSuccess && rc == SPH_OK) {
+        // the step's gravity stream has joined the main stream inside each step
+        e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(ms, a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return ctx_fail(ctx, e, "time_steps", __LINE__);
     return SPH_OK;
 }
 

@@ -262,7 +262,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
     // grid-stride over groups: many short blocks, so the block scheduler can
     // interleave this compute-bound walk with the memory-bound SPH passes
     // running on the other stream
-    for (int g = blockIdx.x * WALK_WARPS + w; g < ngroup; g += gridDim.x * WALK_WARPS) {
+    for (int g = q_first(work, blockIdx.x * WALK_WARPS + w); g < ngroup;
+         g = q_next(work, g, gridDim.x * WALK_WARPS)) {
         const int s0 = gstart[g], gc = gcount[g];
         const bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
@@ -642,13 +643,14 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, 6)
               const float4 *__restrict__ wA, const float4 *__restrict__ wB,
               const float4 *__restrict__ wC, const int4 *__restrict__ wL, float eps2,
               float theta_local, int *__restrict__ pool, int *__restrict__ nrem_out,
-              float *__restrict__ sgL, unsigned long long *counters) {
+              float *__restrict__ sgL, unsigned long long *counters, unsigned *queue) {
     __shared__ SgSmem smem[WALK_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SgSmem &S = smem[w];
     const unsigned lt = (1u << lane) - 1u;
     const int nsg = min(*nsg_p, cap);
-    for (int s = blockIdx.x * WALK_WARPS + w; s < nsg; s += gridDim.x * WALK_WARPS) {
+    for (int s = q_first(queue, blockIdx.x * WALK_WARPS + w); s < nsg;
+         s = q_next(queue, s, gridDim.x * WALK_WARPS)) {
         const int s0 = sstart[s], sc = scount[s];
         if (sc <= 32) {
             // a single group: nothing to share, the group walks from the root
@@ -865,18 +867,23 @@ template <class R, bool POT>
 int run_walk(sph_ctx *ctx, cudaStream_t s) {
     // groups hold 1..32 particles (about 20 on average); size the grid for
     // one group per warp at 16 particles per group, the rest by grid stride
-    int grid = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
-    if (ctx->cfg.walk_blocks > 0) grid = min(grid, ctx->num_sms * ctx->cfg.walk_blocks);
+    int grid0 = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
+    if (ctx->cfg.walk_blocks > 0) grid0 = min(grid0, ctx->num_sms * ctx->cfg.walk_blocks);
     const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
     SgArgs sg{};
+    int rc;
     if constexpr (std::is_same<R, float>::value) {
         if (ctx->g_sg && ctx->cfg.theta_local > 0.0) {
-            const int sgrid = max(1, div_up(div_up(ctx->n, 64) + ctx->ncloud, WALK_WARPS));
+            int sgrid;
+            unsigned *sq;
+            rc = queue_launch(ctx, s, WQ_SG_WALK, (const void *)k_sg_walk, WALK_WARPS * 32,
+                              max(1, div_up(div_up(ctx->n, 64) + ctx->ncloud, WALK_WARPS)), &sgrid, &sq);
+            if (rc) return rc;
             k_sg_walk<<<sgrid, WALK_WARPS * 32, 0, s>>>(
                 ctx->d_nsg, ctx->sg_cap, ctx->sg_start, ctx->sg_count, ctx->sg_cloud, ctx->croot,
                 (const float4 *)ctx->pw, (const float4 *)ctx->wA, (const float4 *)ctx->wB,
                 (const float4 *)ctx->wC, ctx->wL, eps2, (float)ctx->cfg.theta_local, ctx->sg_pool,
-                ctx->sg_nrem, ctx->sgL, ctx->counters);
+                ctx->sg_nrem, ctx->sgL, ctx->counters, sq);
             sg.g_sg = ctx->g_sg;
             sg.start = ctx->sg_start;
             sg.nrem = ctx->sg_nrem;
@@ -885,12 +892,17 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
             sg.cap = ctx->sg_cap;
         }
     }
+    int grid;
+    unsigned *wq;
+    rc = queue_launch(ctx, s, WQ_WALK, (const void *)k_walk<R, POT>, WALK_WARPS * 32, grid0, &grid,
+                      &wq);
+    if (rc) return rc;
     k_walk<R, POT><<<grid, WALK_WARPS * 32, 0, s>>>(
         ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->groot_g, ctx->croot,
         (const typename R4<R>::T *)ctx->pw, (const typename R4<R>::T *)ctx->wA,
         (const typename R4<R>::T *)ctx->wB, (const typename R4<R>::T *)ctx->wC, ctx->wL,
         ctx->cfg.leaf_size, eps2, ctx->cfg.G, ctx->n, ctx->agrav, ctx->pot,
-        ctx->work, ctx->counters, ctx->status, (float)ctx->cfg.theta_local, sg);
+        wq, ctx->counters, ctx->status, (float)ctx->cfg.theta_local, sg);
     return SPH_OK;
 }
 

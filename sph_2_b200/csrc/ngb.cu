@@ -326,11 +326,12 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
 
 // exact lists for every particle
 __global__ void __launch_bounds__(SEARCH_WARPS * 32)
-    k_lists(const int *__restrict__ ngroup_p, SearchArgs A) {
+    k_lists(const int *__restrict__ ngroup_p, SearchArgs A, unsigned *queue) {
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
-    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+    for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
+         g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
         bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
@@ -531,11 +532,12 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
 // (latency-bound: 8 blocks per SM, 64 registers, measured faster than 95)
 template <class R>
 __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
-    k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B) {
+    k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B, unsigned *queue) {
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
-    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+    for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
+         g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
         bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
@@ -638,11 +640,12 @@ __device__ __forceinline__ void count_lane(const SearchArgs &A, const CountArgs 
 
 // candidate search + count iteration for the flagged particles of each group
 __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
-    k_cand_count(const int *__restrict__ ngroup_p, SearchArgs A, CountArgs B) {
+    k_cand_count(const int *__restrict__ ngroup_p, SearchArgs A, CountArgs B, unsigned *queue) {
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
-    for (int g = blockIdx.x * SEARCH_WARPS + w; g < ngroup; g += gridDim.x * SEARCH_WARPS) {
+    for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
+         g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
         bool act = lane < gc;
         const int i = s0 + (act ? lane : 0);
@@ -727,12 +730,18 @@ int launch_smoothing_h(sph_ctx *ctx) {
     B.tol = ctx->cfg.h_tol;
     B.grow = H_GROW;
     B.max_iter = ctx->cfg.h_max_iter;
+    const bool mixed = ctx->cfg.precision == SPH_PREC_MIXED;
+    const void *kern = mixed ? (const void *)k_cand_newton<float> : (const void *)k_cand_newton<double>;
     for (int r = 0; r < rounds; r++) {
         B.last_round = r == rounds - 1;
-        if (ctx->cfg.precision == SPH_PREC_MIXED)
-            k_cand_newton<float><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+        int g;
+        unsigned *q;
+        int rc = queue_launch(ctx, s, WQ_SEARCH, kern, SEARCH_WARPS * 32, grid, &g, &q);
+        if (rc) return rc;
+        if (mixed)
+            k_cand_newton<float><<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, q);
         else
-            k_cand_newton<double><<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+            k_cand_newton<double><<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, q);
     }
     ctx->lists_ok = false;
     ctx->cand_ok = true;
@@ -764,7 +773,12 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     B.grow = H_GROW;
     for (int r = 0; r < rounds; r++) {
         B.last_round = r == rounds - 1;
-        k_cand_count<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B);
+        int g;
+        unsigned *q;
+        int rc = queue_launch(ctx, s, WQ_SEARCH, (const void *)k_cand_count, SEARCH_WARPS * 32,
+                              grid, &g, &q);
+        if (rc) return rc;
+        k_cand_count<<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, q);
     }
     ctx->lists_ok = false;
     ctx->cand_ok = true;
@@ -791,7 +805,11 @@ int launch_neighbours(sph_ctx *ctx) {
     // node h_max only matters to the tree search: skipped when no list needs it
     int rc = launch_refit_hmax(ctx, ctx->cand_ok ? ctx->lflag + n + 1 : nullptr);
     if (rc) return rc;
-    k_lists<<<grid, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A);
+    int g;
+    unsigned *q;
+    if ((rc = queue_launch(ctx, s, WQ_SEARCH, (const void *)k_lists, SEARCH_WARPS * 32, grid, &g, &q)))
+        return rc;
+    k_lists<<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, q);
     ctx->lists_ok = true;
     ctx->rho_ok = ctx->divcurl_ok = false;
     return ctx_check_launch(ctx, "neighbours");
@@ -808,7 +826,12 @@ int launch_lists_marked(sph_ctx *ctx) {
     A.only_all = ctx->lflag + n;
     int rc = launch_refit_hmax(ctx, ctx->lflag + n + 1);
     if (rc) return rc;
-    k_lists<<<grid, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup, A);
+    int g;
+    unsigned *q;
+    if ((rc = queue_launch(ctx, ctx->stream, WQ_SEARCH, (const void *)k_lists, SEARCH_WARPS * 32,
+                           grid, &g, &q)))
+        return rc;
+    k_lists<<<g, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup, A, q);
     return ctx_check_launch(ctx, "lists_marked");
 }
 

@@ -19,7 +19,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/sph_b200.h"
@@ -125,6 +127,7 @@ struct sph_ctx {
     long long *status = nullptr;               // SPH_NSTATUS
     unsigned long long *counters = nullptr;    // walk: cells, particles
     unsigned *work = nullptr;                  // work counters for persistent kernels (16)
+    std::map<std::pair<const void *, int>, int> occupancy;  // resident blocks per SM per kernel
     double *red = nullptr;                     // reduction scratch
 
     // cooling
@@ -283,6 +286,23 @@ __device__ __forceinline__ void cloud_min(unsigned long long *dt_bits, bool vali
     }
 }
 
+// Work queue of the persistent group kernels: with a counter (queue mode)
+// every warp takes its next group from an atomic counter, so a persistent
+// grid of one block per resident slot drains the (cloud, group) list in order
+// however uneven the groups' costs are; without one (null) the warp strides
+// over the groups by the grid size.  All lanes of the warp call both.
+__device__ __forceinline__ int q_first(unsigned *q, int static_first) {
+    if (!q) return static_first;
+    int g = 0;
+    if ((threadIdx.x & 31) == 0) g = (int)atomicAdd(q, 1u);
+    return __shfl_sync(0xffffffffu, g, 0);
+}
+__device__ __forceinline__ int q_next(unsigned *q, int g, int stride) {
+    return q ? q_first(q, 0) : g + stride;
+}
+// work-counter slots (sph_ctx::work) of the queued kernels
+enum { WQ_WALK = 0, WQ_SG_WALK = 1, WQ_SEARCH = 2, WQ_N = 3 };
+
 // ---- host-side launch helpers implemented per translation unit ----
 int launch_sort(sph_ctx *ctx);
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
@@ -292,6 +312,11 @@ constexpr int SGROUP_MAX = 128;  // particles per super-group
 constexpr int SG_POOL = 8;       // node slots per particle of a super-group
 constexpr int SG_LSTRIDE = 40;   // floats per super-group record: 35 coefficients, pad, centre
 int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
+// grid and queue counter of a group kernel: the persistent grid with its
+// counter zeroed on the stream, or the static grid and no counter when
+// SPH_FLAG_STATIC_GRID is set
+int queue_launch(sph_ctx *ctx, cudaStream_t s, int slot, const void *kernel, int block,
+                 int static_grid, int *grid, unsigned **queue);
 int launch_tree(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);

@@ -97,3 +97,33 @@ def test_mixed_walk_with_supergroups_per_cloud():
         err = np.sqrt(np.mean(np.sum((ag - ad) ** 2, 1) / np.sum(ad ** 2, 1)))
         assert err < 3e-4, (k, err)
     ctx.close()
+
+
+def test_autotuner_picks_valid_parameters_and_keeps_accuracy(tmp_path):
+    """The autotuner searches leaf size 8..64, lanes per particle and block
+    size on an uneven 4-cloud ensemble, stores its choice per workload, applies
+    a cached choice without timing, and the gravity at the chosen settings
+    stays within the opening angle's error bound against the FP64 direct sum."""
+    from sph_2_b200.autotune import BLOCKS, LANES, LEAVES, tune
+    e = ic.ensemble(n_clouds=4, nmin=20_000, nmax=60_000, seed=3)
+    n = len(e["m"])
+    ctx = Context(Config(n_max=n, n_cloud_max=4, precision="mixed", theta=0.5))
+    ctx.load(e["pos"], e["vel"], e["m"], e["h"], e["u"], cloud=e["cloud"])
+    ctx.prologue()
+    cache = str(tmp_path / "tune.json")
+    best, res = tune(ctx, cache=cache, steps=1, warmup=1)
+    assert best["leaf_size"] in LEAVES and best["ngb_lanes"] in LANES
+    assert best["block_size"] in BLOCKS
+    assert len(res) >= len(LEAVES) and all(ms > 0 for ms, _ in res)
+    assert res[0][1] == best
+    best2, res2 = tune(ctx, cache=cache)
+    assert best2 == best and res2[0][0] is None
+    st = ctx.status()
+    assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0 and st["stack_overflow"] == 0, st
+    ctx.load(e["pos"], e["vel"], e["m"], e["h"], e["u"], cloud=e["cloud"])
+    ctx.prologue()
+    tg = np.random.default_rng(0).choice(n, 2000, replace=False).astype(np.int32)
+    ad, _ = ctx.gravity_direct(tg)
+    a = ctx.get_acc("grav", True)[tg]
+    err = np.sqrt(np.mean(np.sum((a - ad) ** 2, 1) / np.sum(ad * ad, 1)))
+    assert err < 3.7e-4
