@@ -267,6 +267,13 @@ int sph_gravity_direct(sph_ctx *ctx, int32_t ntarget, const int32_t *targets, do
  * (eps_ij = (eps_i+eps_j)/2), FP64, out: ntarget*3 */
 int sph_gravity_direct_spline(sph_ctx *ctx, const double *eps, int32_t ntarget,
                               const int32_t *targets, double *out, int32_t host);
+/* the reference's partial field of rows [nbeg, nend) (getAcc_g_smth_mimj_mpi,
+ * libsx.py:910-947): every pair (a, b), a < b in original index with a in
+ * the rows, adds its spline-softened attraction to both a and b, so the sum
+ * of the fields of a partition of [0, N) is the full field.  eps and out
+ * (n x 3, row per particle) in original order, FP64. */
+int sph_gravity_direct_spline_rows(sph_ctx *ctx, const double *eps, int32_t nbeg, int32_t nend,
+                                   double *out, int32_t host);
 /* v += a dt * fac with a = a_sph + a_grav (v_evolve, hfvCLibs:936-949) */
 int sph_kick(sph_ctx *ctx, double fac);
 /* x += v dt (r_evolveT, hfvCLibs:981-994) */

@@ -28,11 +28,18 @@ u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 vp = C.c_void_p
 
 
+def reference_root() -> str:
+    """The reference's 11_Dec_2022 directory: $SPH2_REFERENCE, else its
+    location in the build container."""
+    return os.environ.get("SPH2_REFERENCE", "/root/reference/11_Dec_2022")
+
+
 def build() -> str:
     """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    if os.path.isdir("/root/reference/11_Dec_2022"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    ref = reference_root()
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"SPH2_REFERENCE={ref}"], check=True)
     return os.path.join(_HERE, "liboracle.so")
 
 

@@ -122,6 +122,7 @@ SIGNATURES = [
     ("sph_gravity", C.c_int, [_P]),
     ("sph_gravity_direct", C.c_int, [_P, _I, _P, _P, _I]),
     ("sph_gravity_direct_spline", C.c_int, [_P, _P, _I, _P, _P, _I]),
+    ("sph_gravity_direct_spline_rows", C.c_int, [_P, _P, _I, _I, _P, _I]),
     ("sph_kick", C.c_int, [_P, _D]),
     ("sph_drift", C.c_int, [_P]),
     ("sph_update_u", C.c_int, [_P, _I]),

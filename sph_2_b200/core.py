@@ -306,6 +306,16 @@ class Context:
                   "gravity_direct_spline")
         return out.reshape(-1, 3)
 
+    def gravity_direct_spline_rows(self, eps, nbeg, nend):
+        """The reference's partial field of rows [nbeg, nend) (original order,
+        (n, 3)); fields of a partition of the rows sum to the full field."""
+        e = _f64(eps)
+        out = np.zeros((self.n, 3))
+        self._chk(self._L.sph_gravity_direct_spline_rows(self._h, _ptr(e), int(nbeg), int(nend),
+                                                         _ptr(out), 1),
+                  "gravity_direct_spline_rows")
+        return out
+
     def counters(self):
         out = np.zeros(2, np.int64)
         self._chk(self._L.sph_get_counters(self._h, _ptr(out)), "counters")

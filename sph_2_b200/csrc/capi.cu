@@ -762,7 +762,7 @@ int sph_gravity(sph_ctx *ctx) {
 }
 
 static int direct_common(sph_ctx *ctx, const double *eps, int32_t nt, const int32_t *targets,
-                         double *out, int32_t host, int width) {
+                         double *out, int32_t host, int width, int nbeg = 0, int nend = -1) {
     int rc = enter(ctx);
     if (rc) return rc;
     if (nt < 0 || (nt > 0 && (!targets || !out))) return SPH_ERR_ARG;
@@ -782,7 +782,8 @@ static int direct_common(sph_ctx *ctx, const double *eps, int32_t nt, const int3
         // eps is given in the caller's original order: bring it to storage order
         k_gather_by_id<<<div_up(ctx->n, 256), 256, 0, ctx->stream>>>(ctx->n, ctx->id[ctx->cur],
                                                                       deps, ctx->red);
-        rc = launch_gravity_direct_spline(ctx, ctx->red, nt, dt_, dout);
+        rc = launch_gravity_direct_spline(ctx, ctx->red, nt, dt_, dout, nbeg,
+                                          nend < 0 ? ctx->n : nend);
     } else {
         rc = launch_gravity_direct(ctx, nt, dt_, dout);
     }
@@ -805,6 +806,29 @@ int sph_gravity_direct_spline(sph_ctx *ctx, const double *eps, int32_t nt, const
                               double *out, int32_t host) {
     if (!eps) return SPH_ERR_ARG;
     return direct_common(ctx, eps, nt, targets, out, host, 3);
+}
+
+int sph_gravity_direct_spline_rows(sph_ctx *ctx, const double *eps, int32_t nbeg, int32_t nend,
+                                   double *out, int32_t host) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    const int n = ctx->n;
+    if (!eps || !out || nbeg < 0 || nend < nbeg || nend > n) return SPH_ERR_ARG;
+    if (n == 0) return SPH_OK;
+    // every stored particle is a target; the result is scattered back to the
+    // caller's original order row by row
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    std::vector<double> st(3 * (size_t)n), orig(3 * (size_t)n);
+    rc = direct_common(ctx, eps, n, all.data(), st.data(), 1, 3, nbeg, nend);
+    if (rc) return rc;
+    std::vector<int> id(n);
+    CK(cudaMemcpy(id.data(), ctx->id[ctx->cur], sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < n; s++)
+        for (int k = 0; k < 3; k++) orig[3 * (size_t)id[s] + k] = st[3 * (size_t)s + k];
+    if (host) memcpy(out, orig.data(), sizeof(double) * 3 * n);
+    else CK(cudaMemcpy(out, orig.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    return SPH_OK;
 }
 
 int sph_kick(sph_ctx *ctx, double fac) {

@@ -828,17 +828,25 @@ __device__ __forceinline__ double fk_spline(double rr, double e) {
     return inv_r3;
 }
 
+// With ids (original particle indices) the sum is the reference's partial
+// field of the rows [nbeg, nend): the pairs (a, b), a < b in original index
+// with a in the rows, add to both particles (libsx.py:914-945), so target i
+// takes source s when s > i and i is a row, or s < i and s is a row.
+// ids == null: every s != i.
 __global__ void __launch_bounds__(256)
     k_direct_spline(int nt, const int *__restrict__ targets, const double4 *__restrict__ p0,
                     const double *__restrict__ m, const double *__restrict__ eps, int n, double G,
-                    double *__restrict__ out) {
+                    double *__restrict__ out, const int *__restrict__ ids, int nbeg, int nend) {
     __shared__ double4 sh[256];
     __shared__ double se[256];
+    __shared__ int sid[256];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const bool ok = t < nt;
     const int i = ok ? targets[t] : targets[0];
     const double4 pi = p0[i];
     const double ei = eps[i];
+    const int idi = ids ? ids[i] : 0;
+    const bool irow = idi >= nbeg && idi < nend;
     double ax = 0, ay = 0, az = 0;
     for (int base = 0; base < n; base += 256) {
         const int j = base + threadIdx.x;
@@ -847,11 +855,16 @@ __global__ void __launch_bounds__(256)
             q.w = m[j];
             sh[threadIdx.x] = q;
             se[threadIdx.x] = eps[j];
+            sid[threadIdx.x] = ids ? ids[j] : 0;
         }
         __syncthreads();
         const int lim = min(256, n - base);
         for (int k = 0; k < lim; k++) {
             if (base + k == i) continue;
+            if (ids) {
+                const int ids_ = sid[k];
+                if (!((ids_ > idi && irow) || (ids_ < idi && ids_ >= nbeg && ids_ < nend))) continue;
+            }
             const double4 q = sh[k];
             const double dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
             const double rr = sqrt(dx * dx + dy * dy + dz * dz);
@@ -930,9 +943,11 @@ int launch_gravity_direct(sph_ctx *ctx, int nt, const int *targets, double *out)
 }
 
 int launch_gravity_direct_spline(sph_ctx *ctx, const double *eps, int nt, const int *targets,
-                                 double *out) {
+                                 double *out, int nbeg, int nend) {
     if (nt <= 0) return SPH_OK;
+    const bool rows = !(nbeg == 0 && nend == ctx->n);
     k_direct_spline<<<div_up(nt, 256), 256, 0, ctx->stream>>>(
-        nt, targets, ctx->p0, ctx->st[ctx->cur][ST_M], eps, ctx->n, ctx->cfg.G, out);
+        nt, targets, ctx->p0, ctx->st[ctx->cur][ST_M], eps, ctx->n, ctx->cfg.G, out,
+        rows ? ctx->id[ctx->cur] : nullptr, nbeg, nend);
     return ctx_check_launch(ctx, "gravity_direct_spline");
 }

@@ -151,20 +151,29 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     __syncwarp();
 
     // FP32 prefilter: distances relative to the group's centre, compared
-    // with the threshold widened by 1e-4 (FP32 rounding of the relative
-    // coordinates is below 1e-6 of the threshold); the candidates it passes
-    // get the exact FP64 test, so the rows are the same as an FP64-only scan
+    // with the threshold widened by a margin; the candidates it passes get
+    // the exact FP64 test, so the rows are the same as an FP64-only scan.
+    // The relative error of the FP32 r^2 is at most about 2^-21 (2E/R + 3)
+    // (E the group's half-diagonal, R the search radius: the coordinates are
+    // rounded at their distance from the centre, which is at most E + R), so
+    // the margin is 1e-4 plus a bound of that size: 1e-4 alone while E stays
+    // below about 100 R, wider for a sparse group.
     const double cx = 0.5 * (gx0 + gx1), cy = 0.5 * (gy0 + gy1), cz = 0.5 * (gz0 + gz1);
+    const double ex = 0.5 * sqrt((gx1 - gx0) * (gx1 - gx0) + (gy1 - gy0) * (gy1 - gy0) +
+                                 (gz1 - gz0) * (gz1 - gz0));
+    const double rsearch = MODE == 1 ? pi.w : ri;
+    const float mrg = (float)(1e-4 + ldexp(2.0 * ex / fmax(rsearch, 1e-300) + 3.0, -20));
     const float2 pfx = bc2((float)(pi.x - cx)), pfy = bc2((float)(pi.y - cy)),
                  pfz = bc2((float)(pi.z - cz));
-    const float2 ri2f = bc2((float)ri2 * 1.0001f), hif = bc2((float)pi.w);
+    const float2 ri2f = bc2((float)ri2 * (1.f + mrg)), hif = bc2((float)pi.w);
     // FP32 h iteration: a candidate whose FP32 distance is below the
-    // threshold narrowed by 1e-4 is inside in FP64 too and skips the FP64
-    // test; its kernel terms use the FP32 relative coordinates and are summed
-    // plainly over the chunk (at most 32 terms), then added to the Kahan sums
+    // threshold narrowed by the same margin is inside in FP64 too and skips
+    // the FP64 test; its kernel terms use the FP32 relative coordinates and
+    // are summed plainly over the chunk (at most 32 terms), then added to the
+    // Kahan sums
     constexpr bool FAST = MODE == 0 && std::is_same<R, float>::value;
-    const float2 ri2lo = bc2((float)ri2 * 0.9999f);
-    const float2 m1 = bc2(-1.f), widen = bc2(1.0001f);
+    const float2 ri2lo = bc2((float)ri2 * (1.f - mrg));
+    const float2 m1 = bc2(-1.f), widen = bc2(1.f + mrg);
 
     auto process = [&](int m) {
         if (lane < m) {

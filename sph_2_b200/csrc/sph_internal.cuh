@@ -332,7 +332,7 @@ int launch_repack_p2(sph_ctx *ctx);
 int launch_gravity(sph_ctx *ctx, cudaStream_t s, bool pot);
 int launch_gravity_direct(sph_ctx *ctx, int nt, const int *targets_dev, double *out_dev);
 int launch_gravity_direct_spline(sph_ctx *ctx, const double *eps_dev, int nt,
-                                 const int *targets_dev, double *out_dev);
+                                 const int *targets_dev, double *out_dev, int nbeg, int nend);
 int launch_kick(sph_ctx *ctx, double fac, bool cfl);
 int launch_drift(sph_ctx *ctx);
 int launch_kick_drift(sph_ctx *ctx);

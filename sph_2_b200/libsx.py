@@ -22,8 +22,6 @@ Differences from the reference, by design:
 * smoothing_length_mpi returns the Newton smoothing length started from a
   uniform-density guess instead of half the 50th-neighbour distance
   (libsx.py:781-803); both are starting values for h_smooth_fast_mpi.
-* getAcc_g_smth_mimj_mpi accepts only the full range (0, N): the reference's
-  partial fields exist for its MPI reduction, which a single GPU does not need.
 * getPressure / getCsound / getKE are elementwise host formulas (no kernel is
   worth a launch there); getPE is the FP64 sum of the tree walk's Plummer
   potential.
@@ -274,18 +272,24 @@ def get_dU_mpi(nbeg, nend, pos, v, rho, P, c, h, m, gama, eta, alpha, beta):
 # ---- gravity -------------------------------------------------------------
 def getAcc_g_smth_mimj_mpi(nbeg, nend, pos, mass, G, epsilon):
     """libsx.py:910-947: spline-softened direct sum with eps_ij = (eps_i +
-    eps_j)/2, as an (N, 3) field (FP64 on the GPU).  Only (0, N)."""
+    eps_j)/2 as an (N, 3) field (FP64 on the GPU).  For rows [nbeg, nend) it
+    is the reference's partial field: each pair (i, j), i < j, with i in the
+    rows adds to both i and j, so the fields of the MPI ranks' row ranges sum
+    to the full field."""
     n = int(pos.shape[0])
-    if (nbeg, nend) != (0, n):
-        raise ValueError("the GPU computes the whole field: call with nbeg=0, nend=N")
+    if not 0 <= nbeg <= nend <= n:
+        raise ValueError("rows [nbeg, nend) must lie in [0, N)")
     ctx = _ctx(n)
     ctx.set_params(G=float(G))
     ones = np.ones(n) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + 1.0
     ctx = _load_state(pos, mass, ones)
     eps = _host(epsilon)
-    inv = np.empty(n, np.int32)
-    inv[ctx.ids()] = np.arange(n, dtype=np.int32)      # storage slot of each particle
-    acc = ctx.gravity_direct_spline(eps, inv)
+    if (nbeg, nend) == (0, n):
+        inv = np.empty(n, np.int32)
+        inv[ctx.ids()] = np.arange(n, dtype=np.int32)  # storage slot of each particle
+        acc = ctx.gravity_direct_spline(eps, inv)
+    else:
+        acc = ctx.gravity_direct_spline_rows(eps, nbeg, nend)
     if _is_cuda_tensor(pos):
         import torch
         return torch.from_numpy(acc).to(pos.device)

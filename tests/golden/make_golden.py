@@ -19,7 +19,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/11_Dec_2022/MPI_sph/sph_code"
+# the reference's 11_Dec_2022 directory ($SPH2_REFERENCE, else its place here)
+REF = os.path.join(os.environ.get("SPH2_REFERENCE", "/root/reference/11_Dec_2022"),
+                   "MPI_sph", "sph_code")
 
 
 def evrard_positions(n, seed):

@@ -64,8 +64,12 @@ def test_gravity_and_energies(g):
     n = len(g["m"])
     acc = X.getAcc_g_smth_mimj_mpi(0, n, g["pos"], g["m"], 1.0, g["eps"])
     assert rel(acc, g["acc_g"]) < 1e-12
-    with pytest.raises(ValueError):
-        X.getAcc_g_smth_mimj_mpi(0, n // 2, g["pos"], g["m"], 1.0, g["eps"])
+    # the reference's partial field of a row range (its MPI decomposition),
+    # and the sum over a partition of the rows is the whole field
+    half = X.getAcc_g_smth_mimj_mpi(0, n // 2, g["pos"], g["m"], 1.0, g["eps"])
+    assert rel(half, g["acc_g_half"]) < 1e-12
+    rest = X.getAcc_g_smth_mimj_mpi(n // 2, n, g["pos"], g["m"], 1.0, g["eps"])
+    assert rel(half + rest, g["acc_g"]) < 1e-12
     assert abs(X.getKE(g["v"], g["m"]) / float(g["ke"]) - 1) < 1e-13
     pe = X.getPE(g["pos"], g["m"], 1.0, np.full(n, 1e-2))
     x, y, z = (g["pos"][:, k].copy() for k in range(3))

@@ -289,3 +289,32 @@ def test_individual_dt_vs_oracle(precision, tol):
     ref = r["dt"].max()
     assert b.min() >= 0 and np.all(ref / 2.0 ** b <= r["dt"] * (1 + 1e-15))
     assert np.all((b == 0) | (ref / 2.0 ** (b - 1) > r["dt"]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_h_and_lists_with_sparse_outskirts(precision):
+    """A dense ball with a sparse log-uniform halo out to 50 radii: groups in
+    the halo are wide compared with their search radius, which widens the
+    FP32 prefilter's margin; the Newton h still matches the oracle and the
+    lists stay exact."""
+    rng = np.random.default_rng(31)
+    core = rng.normal(size=(5000, 3))
+    core *= (rng.random(5000) ** (1 / 3) / np.linalg.norm(core, axis=1))[:, None]
+    halo = rng.normal(size=(600, 3))
+    halo *= (10 ** rng.uniform(0.7, 1.7, 600) / np.linalg.norm(halo, axis=1))[:, None]
+    pos = np.ascontiguousarray(np.concatenate([core, halo]))
+    n = len(pos)
+    h0 = 1.1 * O.ref_smoothing_length(0, n, pos)
+    ctx = Context(Config(n_max=n, precision=precision, max_ngb=512))
+    ctx.load(pos, np.zeros((n, 3)), np.full(n, 1.0 / n), h0, np.full(n, 0.05))
+    ctx.sort(); ctx.build_tree()
+    ctx.smoothing_h()
+    st = ctx.status()
+    assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0 and st["stack_overflow"] == 0, st
+    x, y, z, m, h = storage(ctx)
+    hh, _, _ = O.newton_h(x, y, z, m, h, max_iter=1)
+    assert np.max(np.abs(hh / h - 1)) < 2e-3
+    ctx.neighbours()
+    off, lst = ctx.neighbour_lists()
+    oo, ol = O.neighbours(x, y, z, h)
+    assert np.array_equal(off, oo) and np.array_equal(lst, ol)
