@@ -60,6 +60,8 @@ def parse():
                     help="run the autotuner before timing the headline (the ensemble is always tuned)")
     ap.add_argument("--no-tune", action="store_true", help="do not tune the ensemble either")
     ap.add_argument("--no-theta-table", action="store_true")
+    ap.add_argument("--arm", default="mixed", choices=["mixed", "fp64"],
+                    help="precision of the timed headline arm (fp64: profile the plain step)")
     ap.add_argument("--static-grid", action="store_true",
                     help="group kernels on a grid over the groups instead of the work queue")
     ap.add_argument("--no-ensemble", action="store_true")
@@ -364,7 +366,7 @@ def main():
         return max_over_ranks(e0.elapsed_time(e1))
 
     # ---- mixed precision arm (the headline) ----
-    ctx = make("mixed", L.FLAG_TIMING)
+    ctx = make(a.arm, L.FLAG_TIMING)
     sampler = ClockSampler(local)
     ctx.step(a.warmup)
     ctx.sync()

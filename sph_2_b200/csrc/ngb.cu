@@ -518,9 +518,18 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
             else if (lo == 0.0) hn = h / 1.25;
             else hn = 0.5 * (lo + hi);
         }
+        // an iterate beyond the candidate radius first tries the radius
+        // itself, where the row still holds every term: only a root beyond
+        // it sends the particle to another search (an overshooting Newton
+        // step alone used to)
+        bool clamped = false;
+        if (hn > cap && h < cap) {
+            hn = cap;
+            clamped = true;
+        }
         const double dh = hn - h;
         h = hn;
-        if (fabs(dh) < B.tol * fabs(h - dh)) {
+        if (!clamped && fabs(dh) < B.tol * fabs(h - dh)) {
             ok = true;
             break;
         }

@@ -293,15 +293,15 @@ def test_individual_dt_vs_oracle(precision, tol):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_h_and_lists_with_sparse_outskirts(precision):
-    """A dense ball with a sparse log-uniform halo out to 50 radii: groups in
-    the halo are wide compared with their search radius, which widens the
-    FP32 prefilter's margin; the Newton h still matches the oracle and the
-    lists stay exact."""
+    """A dense unit ball inside a halo that thins out to 5 radii (h grows
+    20-fold outwards): the wide groups of the halo widen the FP32
+    prefilter's margin; the Newton h still matches the oracle and the lists
+    stay exact."""
     rng = np.random.default_rng(31)
     core = rng.normal(size=(5000, 3))
     core *= (rng.random(5000) ** (1 / 3) / np.linalg.norm(core, axis=1))[:, None]
-    halo = rng.normal(size=(600, 3))
-    halo *= (10 ** rng.uniform(0.7, 1.7, 600) / np.linalg.norm(halo, axis=1))[:, None]
+    halo = rng.normal(size=(1500, 3))
+    halo *= ((1.0 + 4.0 * rng.random(1500) ** 2) / np.linalg.norm(halo, axis=1))[:, None]
     pos = np.ascontiguousarray(np.concatenate([core, halo]))
     n = len(pos)
     h0 = 1.1 * O.ref_smoothing_length(0, n, pos)
