@@ -92,7 +92,9 @@ extern "C" {
 #define SPH_S_MLP_FALLBACK 5  /* surrogate rows sent back to the exact solver    */
 #define SPH_S_NONFINITE 6     /* non-finite inputs seen                          */
 #define SPH_S_WALK_STACK_MAX 7/* deepest traversal stack seen in the gravity walk */
-#define SPH_NSTATUS 8
+#define SPH_S_WAIT_TIMEOUT 8  /* bounded device waits that gave up (tensor-core MLP
+                                 tiles; their rows go to the exact solver)        */
+#define SPH_NSTATUS 9
 
 #define SPH_FLAG_DUDT_FUSED 1  /* du/dt in the force pass (one pass) instead of the
                                   reference order (after the closing kick)          */
@@ -103,6 +105,8 @@ extern "C" {
 #define SPH_FLAG_TIMING 32     /* record CUDA events between the phases of sph_step */
 #define SPH_FLAG_COOLING_TABLE 64 /* with SPH_FLAG_COOLING: the grid-file backend
                                   (sph_cooling_table) instead of the implicit solve */
+#define SPH_FLAG_MLP_WARP_MMA 256 /* MLP inference on the warp-level mma.sync path
+                                  instead of tcgen05.mma with a TMEM accumulator  */
 #define SPH_FLAG_STATIC_GRID 128 /* launch the group kernels (walk, searches, h
                                   iteration) with a grid over the groups instead of
                                   a persistent grid draining a work queue        */

@@ -27,7 +27,7 @@ FIELDS = ["x", "y", "z", "vx", "vy", "vz", "m", "h", "u", "rho", "P", "c", "divV
           "dudt_prev", "u_prev"]
 FIELD = {name: k for k, name in enumerate(FIELDS)}
 STATUS = ["h_noconv", "ngb_overflow", "stack_overflow", "h_retry", "cool_noconv", "mlp_fallback",
-          "nonfinite", "walk_stack_max"]
+          "nonfinite", "walk_stack_max", "wait_timeout"]
 FLAG_DUDT_FUSED = 1
 FLAG_COOLING = 2
 FLAG_COOLING_MLP = 4
@@ -36,6 +36,7 @@ FLAG_POTENTIAL = 16
 FLAG_TIMING = 32
 FLAG_COOLING_TABLE = 64
 FLAG_STATIC_GRID = 128
+FLAG_MLP_WARP_MMA = 256
 PHASES = ["kick_drift", "sort", "tree", "smoothing_h", "neighbours", "density", "divcurl",
           "forces", "wait_kick", "dudt", "update_dt", "gravity"]
 MLP_NPARAM = 3 * 64 + 64 + 64 * 64 + 64 + 64 + 1

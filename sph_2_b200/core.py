@@ -202,7 +202,7 @@ class Context:
         return out
 
     def status(self, reset=False) -> dict:
-        out = np.zeros(8, np.int64)
+        out = np.zeros(len(L.STATUS), np.int64)
         self._chk(self._L.sph_get_status(self._h, _ptr(out), int(reset)), "status")
         return dict(zip(L.STATUS, out.tolist()))
 

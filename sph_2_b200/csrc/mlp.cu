@@ -1,7 +1,11 @@
 // mlp.cu -- the cooling surrogate: a 3 -> 64 -> 64 -> 1 MLP (tanh-GELU),
-// BF16 operands with FP32 accumulation on the tensor cores
-// (mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32), forward, backward and
-// Adam kernels written here, and the in-step use: predict
+// BF16 operands with FP32 accumulation on the tensor cores.  Inference (the
+// in-step surrogate, the standalone solves and sph_mlp_forward) runs its 64 x 64
+// layer on tcgen05.mma with a TMEM accumulator, 128 rows per CTA (namespace
+// tc below); training (forward + backward of minibatches, weight gradients from
+// transposed activations) uses the warp-level mma.sync.aligned.m16n8k16 bf16
+// fragments, and SPH_FLAG_MLP_WARP_MMA selects them for inference too.  All
+// kernels are written here, with Adam, and the in-step use: predict
 // dlog10(u) = log10(u_new/u_old) from (log10 rho, log10 u, log10 dt) [cgs],
 // estimate the error of the prediction with the Newton residual of the
 // implicit equation after up to four Newton steps from it, and fall back
@@ -520,6 +524,315 @@ __global__ void k_cool_list_arrays(CoolDev c, const int *__restrict__ list, int 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05): 128 rows per CTA.
+// Layer 1 (3 -> 64) runs on the CUDA cores, one thread per row, from the BF16
+// weights, and writes its BF16 activations into shared memory as operand A of
+// layer 2 (128 x 64, K-major, no swizzle: 8-row x 16-byte core matrices, the
+// K-adjacent ones 128 B apart, the M-adjacent ones 1024 B apart).  W2t is
+// operand B in the same layout (64 x 64).  One thread issues the four K = 16
+// steps of tcgen05.mma kind::f16 (BF16 x BF16 -> FP32, M = 128, N = 64) into a
+// 64-column TMEM accumulator and commits them to an mbarrier; every thread
+// then reads its row (TMEM lane = row) with tcgen05.ld, adds b2, applies GELU
+// and the layer-3 dot product in FP32.  The waits are bounded: a wait that
+// gives up counts in SPH_S_WAIT_TIMEOUT and the CTA sends its remaining rows
+// to the exact solver.
+namespace tc {
+
+constexpr int ROWS = 128;
+constexpr int COLS = 64;          // TMEM columns of the accumulator
+constexpr int SPIN = 1 << 22;     // try_wait polls before a wait gives up
+
+struct alignas(128) Smem {
+    __nv_bfloat16 a[ROWS * H];    // layer-2 operand A, core-matrix layout
+    __nv_bfloat16 b[H * H];       // W2t, core-matrix layout
+    float w1[3][H], b1[H], b2[H], w3[H], b3;
+    unsigned long long mbar;
+    unsigned tmem;
+};
+// dynamic shared memory per CTA: at most 7 CTAs share an SM, 7 x 64 TMEM
+// columns of the 512
+constexpr int SMEM_BYTES = 32 * 1024;
+static_assert(sizeof(Smem) <= SMEM_BYTES, "tcgen05 MLP tile does not fit");
+
+__device__ __forceinline__ unsigned saddr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+// byte offset of element (row, k) in the core-matrix layout of a K = 64 operand
+__device__ __forceinline__ unsigned cm_off(int row, int k) {
+    return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+// shared-memory matrix descriptor (no swizzle, K-major): start, leading
+// (K-direction) and stride (M/N-direction) byte offsets in 16-byte units,
+// descriptor version 1
+__device__ __forceinline__ unsigned long long sdesc(unsigned addr) {
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)(128 >> 4) << 16) |
+           ((unsigned long long)(1024 >> 4) << 32) | (1ull << 46);
+}
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
+// N = 64, M = 128
+constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(H >> 3) << 17) |
+                           ((unsigned)(ROWS >> 4) << 24);
+
+__device__ __forceinline__ void mma(unsigned d, unsigned long long a, unsigned long long b, int acc) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc));
+}
+__device__ __forceinline__ void commit(unsigned mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ bool try_wait(unsigned mbar, unsigned phase) {
+    unsigned ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void ld16(unsigned taddr, float *v) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// weights into shared memory, TMEM allocation (warp 0), mbarrier set-up
+__device__ __forceinline__ void setup(Smem &S, const __nv_bfloat16 *pk, const float *P) {
+    const int t = threadIdx.x;
+    for (int e = t; e < H * H; e += blockDim.x) {
+        const int nn = e / H, k = e % H;  // W2t[n][k]
+        *reinterpret_cast<__nv_bfloat16 *>(reinterpret_cast<char *>(S.b) + cm_off(nn, k)) =
+            pk[PK_W2T + e];
+    }
+    for (int e = t; e < 3 * H; e += blockDim.x) {
+        const int c = e / H, j = e % H;
+        S.w1[c][j] = __bfloat162float(pk[PK_W1T + j * 16 + c]);
+    }
+    for (int j = t; j < H; j += blockDim.x) {
+        S.b1[j] = P[OFF_B1 + j];
+        S.b2[j] = P[OFF_B2 + j];
+        S.w3[j] = P[OFF_W3 + j];
+    }
+    if (t == 0) {
+        S.b3 = P[OFF_B3];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(&S.mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (t < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         saddr(&S.tmem)),
+                     "r"(COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_smem_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+}
+
+__device__ __forceinline__ void teardown(Smem &S) {
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(COLS));
+}
+
+// One tile: x = this thread's normalised features (rounded to BF16 like the
+// warp-level path), returns y; ok = false when the wait gave up (then the
+// caller treats the row as unanswered).  All threads of the CTA call it.
+template <bool FAST>
+__device__ __forceinline__ float predict(Smem &S, const float x[3], unsigned &phase, bool &ok,
+                                         long long *status) {
+    const int r = threadIdx.x;
+    float xb[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xb[c] = __bfloat162float(__float2bfloat16_rn(x[c]));
+    char *arow = reinterpret_cast<char *>(S.a);
+#pragma unroll
+    for (int k8 = 0; k8 < H / 8; k8++) {
+        unsigned pkd[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int j = 8 * k8 + 2 * q;
+            const float z0 = S.b1[j] + xb[0] * S.w1[0][j] + xb[1] * S.w1[1][j] + xb[2] * S.w1[2][j];
+            const float z1 = S.b1[j + 1] + xb[0] * S.w1[0][j + 1] + xb[1] * S.w1[1][j + 1] +
+                             xb[2] * S.w1[2][j + 1];
+            pkd[q] = pack2(act<FAST>(z0), act<FAST>(z1));
+        }
+        *reinterpret_cast<uint4 *>(arow + cm_off(r, 8 * k8)) = make_uint4(pkd[0], pkd[1], pkd[2], pkd[3]);
+    }
+    fence_smem_async();
+    __syncthreads();
+    const unsigned mbar = saddr(&S.mbar);
+    if (r == 0 && ok) {
+        fence_after();
+        const unsigned a0 = saddr(S.a), b0 = saddr(S.b);
+#pragma unroll
+        for (int ks = 0; ks < H / 16; ks++) mma(S.tmem, sdesc(a0 + 256 * ks), sdesc(b0 + 256 * ks), ks > 0);
+        commit(mbar);
+    }
+    bool done = !ok;
+    for (int it = 0; it < SPIN && !done; it++) done = try_wait(mbar, phase);
+    const bool timed_out = !__syncthreads_and(done) || !ok;
+    float y = 0.f;
+    if (!timed_out) {
+        phase ^= 1u;
+        fence_after();
+        const unsigned tl = S.tmem + ((unsigned)(32 * (r >> 5)) << 16);
+        float acc = S.b3;
+#pragma unroll
+        for (int c16 = 0; c16 < H / 16; c16++) {
+            float v[16];
+            ld16(tl + 16 * c16, v);
+            wait_ld();
+#pragma unroll
+            for (int q = 0; q < 16; q++) acc += act<FAST>(v[q] + S.b2[16 * c16 + q]) * S.w3[16 * c16 + q];
+        }
+        y = acc;
+    } else if (ok) {
+        ok = false;  // this CTA stops using the tensor cores
+        if (r == 0) status_add(status, SPH_S_WAIT_TIMEOUT, 1);
+    }
+    fence_before();
+    __syncthreads();  // TMEM and operand A are free for the next tile
+    return y;
+}
+
+}  // namespace tc
+
+__global__ void __launch_bounds__(tc::ROWS)
+    k_mlp_forward_tc(int n, const float *__restrict__ X, float *__restrict__ y,
+                     const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
+                     long long *status) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    tc::Smem &S = *reinterpret_cast<tc::Smem *>(tc_smem);
+    tc::setup(S, pk, P);
+    unsigned phase = 0;
+    bool ok = true;
+    const int ntile = (n + tc::ROWS - 1) / tc::ROWS;
+    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int i = tile * tc::ROWS + threadIdx.x;
+        float x[3] = {0.f, 0.f, 0.f};
+        if (i < n) x[0] = X[3 * i], x[1] = X[3 * i + 1], x[2] = X[3 * i + 2];
+        const float v = tc::predict<false>(S, x, phase, ok, status);
+        if (i < n) y[i] = ok ? v : NAN;
+    }
+    tc::teardown(S);
+}
+
+// in-step cooling with the tensor-core surrogate, 128 rows per CTA
+__global__ void __launch_bounds__(tc::ROWS)
+    k_cool_mlp_tc(CoolDev c, int n, const double *__restrict__ rho, double *__restrict__ u,
+                  const int *__restrict__ cloud, const double *__restrict__ dt, double ur,
+                  double uu, double ut, const __nv_bfloat16 *__restrict__ pk,
+                  const float *__restrict__ P, double err_tol, int *__restrict__ list, int cap,
+                  long long *status) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    tc::Smem &S = *reinterpret_cast<tc::Smem *>(tc_smem);
+    tc::setup(S, pk, P);
+    const float *norm = P + NP;
+    unsigned phase = 0;
+    bool ok = true;
+    const int ntile = (n + tc::ROWS - 1) / tc::ROWS;
+    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int i = tile * tc::ROWS + threadIdx.x;
+        const bool own = i < n;
+        double rho_c = 1.0, u0 = 1.0, dt_c = 1.0;
+        if (own) {
+            rho_c = rho[i] * ur;
+            u0 = u[i] * uu;
+            dt_c = dt[cloud[i]] * ut;
+        }
+        const float x[3] = {(log10f((float)rho_c) - norm[0]) / norm[3],
+                            (log10f((float)u0) - norm[1]) / norm[4],
+                            (log10f((float)dt_c) - norm[2]) / norm[5]};
+        const float y = tc::predict<true>(S, x, phase, ok, status);
+        if (own) {
+            double un = u0, est = INFINITY;
+            if (ok) {
+                un = u0 * exp10((double)y * norm[7] + norm[6]);
+                cool_newton_polish(c, rho_c, u0, dt_c, &un, &est, err_tol);
+            }
+            if (ok && cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+                u[i] = un / uu;
+            } else {
+                status_add(status, SPH_S_MLP_FALLBACK, 1);
+                if (!to_list(list, cap, i)) {
+                    if (cool_solve(c, rho_c, u0, dt_c, &un) < 0) status_add(status, SPH_S_COOL_NOCONV, 1);
+                    u[i] = un / uu;
+                }
+            }
+        }
+    }
+    tc::teardown(S);
+}
+
+// the same for standalone arrays (cgs), with the per-row fallback flag
+__global__ void __launch_bounds__(tc::ROWS)
+    k_cool_mlp_arrays_tc(CoolDev c, int n, const double *__restrict__ rho,
+                         const double *__restrict__ u_old, const double *__restrict__ dtv,
+                         double *__restrict__ u_new, int *__restrict__ fell_back,
+                         const __nv_bfloat16 *__restrict__ pk, const float *__restrict__ P,
+                         double err_tol, int *__restrict__ list, int cap, long long *status) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    tc::Smem &S = *reinterpret_cast<tc::Smem *>(tc_smem);
+    tc::setup(S, pk, P);
+    const float *norm = P + NP;
+    unsigned phase = 0;
+    bool ok = true;
+    const int ntile = (n + tc::ROWS - 1) / tc::ROWS;
+    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int i = tile * tc::ROWS + threadIdx.x;
+        const bool own = i < n;
+        const double r = own ? rho[i] : 1.0, u0 = own ? u_old[i] : 1.0, d = own ? dtv[i] : 1.0;
+        const float x[3] = {(log10f((float)r) - norm[0]) / norm[3],
+                            (log10f((float)u0) - norm[1]) / norm[4],
+                            (log10f((float)d) - norm[2]) / norm[5]};
+        const float y = tc::predict<true>(S, x, phase, ok, status);
+        if (own) {
+            double un = u0, est = INFINITY;
+            if (ok) {
+                un = u0 * exp10((double)y * norm[7] + norm[6]);
+                cool_newton_polish(c, r, u0, d, &un, &est, err_tol);
+            }
+            int fb = 0;
+            if (ok && cool_accept(c, r, u0, d, un, est, err_tol)) {
+                u_new[i] = un;
+            } else {
+                fb = 1;
+                if (!to_list(list, cap, i)) {
+                    cool_solve(c, r, u0, d, &un);
+                    u_new[i] = un;
+                }
+            }
+            if (fell_back) fell_back[i] = fb;
+        }
+    }
+    tc::teardown(S);
+}
+
+// grid of a tensor-core MLP kernel: at most 7 CTAs per SM (TMEM columns)
+int tc_grid(sph_ctx *ctx, int n) {
+    return max(1, min(div_up(n, tc::ROWS), ctx->num_sms * 7));
+}
+bool use_tc(const sph_ctx *ctx) { return !(ctx->cfg.flags & SPH_FLAG_MLP_WARP_MMA); }
+
 int grid_for(sph_ctx *ctx, int n) { return max(1, min(div_up(div_up(n, 16), 4), ctx->num_sms * 8)); }
 int grid32_for(sph_ctx *ctx, int n) { return max(1, min(div_up(div_up(n, 32), 4), ctx->num_sms * 8)); }
 
@@ -560,8 +873,12 @@ int mlp_pack(sph_ctx *ctx) {
 
 int mlp_forward_dev(sph_ctx *ctx, int n, const float *X, float *y) {
     if (n <= 0) return SPH_OK;
-    k_mlp_forward<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
-        n, X, y, (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp);
+    if (use_tc(ctx))
+        k_mlp_forward_tc<<<tc_grid(ctx, n), tc::ROWS, tc::SMEM_BYTES, ctx->stream>>>(
+            n, X, y, (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->status);
+    else
+        k_mlp_forward<<<grid_for(ctx, n), 128, 0, ctx->stream>>>(
+            n, X, y, (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp);
     return ctx_check_launch(ctx, "mlp_forward");
 }
 
@@ -623,11 +940,18 @@ int launch_cooling_mlp(sph_ctx *ctx) {
     if (n <= 0) return SPH_OK;
     const int cap = ctx->cfg.n_max;
     CK(cudaMemsetAsync(ctx->cool_list + cap, 0, sizeof(int), ctx->stream));
-    k_cool_mlp<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
-        cool_dev_of(ctx), n, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
-        ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t,
-        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list, cap,
-        ctx->status);
+    if (use_tc(ctx))
+        k_cool_mlp_tc<<<tc_grid(ctx, n), tc::ROWS, tc::SMEM_BYTES, ctx->stream>>>(
+            cool_dev_of(ctx), n, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
+            ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t,
+            (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list,
+            cap, ctx->status);
+    else
+        k_cool_mlp<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
+            cool_dev_of(ctx), n, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
+            ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t,
+            (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list,
+            cap, ctx->status);
     k_cool_list<<<ctx->num_sms * 4, 128, 0, ctx->stream>>>(
         cool_dev_of(ctx), ctx->cool_list, cap, ctx->rho, ctx->st[c][ST_U], ctx->cloud[c], ctx->dt,
         ctx->cool.unit_rho, ctx->cool.unit_u, ctx->cool.unit_t, ctx->status);
@@ -735,9 +1059,16 @@ int sph_cool_solve_mlp(sph_ctx *ctx, int32_t n, const double *rho, const double 
     cudaSetDevice(ctx->device);
     const int cap = ctx->cfg.n_max;
     CK(cudaMemsetAsync(ctx->cool_list + cap, 0, sizeof(int), ctx->stream));
-    k_cool_mlp_arrays<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
-        cool_dev_of(ctx), n, rho, u_old, dt, u_new, fell_back,
-        (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list, cap);
+    if (use_tc(ctx))
+        k_cool_mlp_arrays_tc<<<tc_grid(ctx, n), tc::ROWS, tc::SMEM_BYTES, ctx->stream>>>(
+            cool_dev_of(ctx), n, rho, u_old, dt, u_new, fell_back,
+            (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list,
+            cap, ctx->status);
+    else
+        k_cool_mlp_arrays<<<grid32_for(ctx, n), 128, 0, ctx->stream>>>(
+            cool_dev_of(ctx), n, rho, u_old, dt, u_new, fell_back,
+            (const __nv_bfloat16 *)ctx->mlp_bf16, ctx->mlp, ctx->cool.mlp_err_tol, ctx->cool_list,
+            cap);
     k_cool_list_arrays<<<ctx->num_sms * 4, 128, 0, ctx->stream>>>(cool_dev_of(ctx), ctx->cool_list,
                                                                  cap, rho, u_old, dt, u_new);
     return ctx_check_launch(ctx, "cool_solve_mlp");

@@ -224,3 +224,28 @@ def test_table_cooling_matches_oracle(tmp_path):
     assert np.isfinite(ctx.get("u")).all() and np.all(ctx.get("u") > 0)
     f = ctx.ion_frac(tab["frac"].shape[4])
     assert np.allclose(f.sum(axis=1), 1.0, atol=1e-5)
+
+
+def test_tcgen05_inference_matches_warp_mma(ctx):
+    """The surrogate's inference on tcgen05.mma with a TMEM accumulator (128
+    rows per CTA) against the warp-level mma.sync path: the same BF16 products
+    with FP32 accumulation, so the outputs agree to FP32 rounding, over a
+    ragged row count (partial last tile), and no wait gave up."""
+    from sph_2_b200 import _lib as L
+    P = cooling.init_params(seed=5)
+    P[192:256] = np.linspace(-0.2, 0.2, 64)
+    ctx.mlp_set(P, np.array([0, 0, 0, 1, 1, 1, 0, 1], np.float32))
+    X = np.random.default_rng(6).normal(size=(1000, 3)).astype(np.float32)
+    ctx.status(reset=True)
+    y_tc = ctx.mlp_forward(X)
+    base = ctx.config.flags
+    ctx.set_params(flags=base | L.FLAG_MLP_WARP_MMA)
+    try:
+        y_w = ctx.mlp_forward(X)
+    finally:
+        ctx.set_params(flags=base)
+    assert np.isfinite(y_tc).all()
+    assert np.max(np.abs(y_tc - y_w)) < 1e-4 * (np.max(np.abs(y_w)) + 1e-6)
+    yo, _ = O.mlp_forward_bf16(X, *cooling.unpack(P))
+    assert np.max(np.abs(y_tc - yo)) < 2e-3 * (np.max(np.abs(yo)) + 1e-6)
+    assert ctx.status()["wait_timeout"] == 0
