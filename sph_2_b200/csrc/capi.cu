@@ -348,7 +348,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->cand_idx, K * N);
     DAF(ctx->cand_cnt, N);
     DAF(ctx->lflag, N + 2);
-    DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N);
+    DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N); DAF(ctx->hover, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C); DAF(ctx->dtmax_bits, C);
     DAF(ctx->dt_part, N); DAF(ctx->dhdt, N); DAF(ctx->dbin, N);
     DAF(ctx->status, SPH_NSTATUS);

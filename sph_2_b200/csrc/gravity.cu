@@ -41,12 +41,7 @@ constexpr int NLOC = 35;
 #define SPH_WALK_STACK 512
 #endif
 constexpr int WSTK = SPH_WALK_STACK;
-#ifndef SPH_WALK_PARTS_V
-#define SPH_WALK_PARTS_V 0
-#endif
-#ifndef SPH_WALK_ACC2
-#define SPH_WALK_ACC2 0
-#endif
+
 constexpr unsigned FULL = 0xffffffffu;
 
 template <class R> __device__ __forceinline__ R rsq(R x);
@@ -67,7 +62,7 @@ struct WalkSmemF {
     int clist[64];
     int plist[96];
     // cells: com x y z, -mass, Qxx Qyy Qzz Qxy Qxz Qyz, trace
-    __align__(16) float f[11][32];
+    __align__(8) float f[11][32];
     // far cells of the group's local expansion: their node ids, per-lane
     // partial sums of the coefficients (one column per lane) and the totals
     int flist[64];
@@ -434,67 +429,32 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
         auto flush_parts = [&](int m) {
           if constexpr (PACKED) {
             const int m2 = (m + 1) & ~1;
-#if SPH_WALK_PARTS_V == 1
-            // pairs of sources as two 16-byte records (x0 x1 y0 y1), (z0 z1 -m0 -m1)
-            float4 *q4 = reinterpret_cast<float4 *>(&S.f[0][0]);
-            if (lane < m2) {
-                float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (lane < m) a = pw[S.plist[lane]];
-                float *r = reinterpret_cast<float *>(q4 + 2 * (lane >> 1));
-                const int o = lane & 1;
-                r[o] = a.x; r[2 + o] = a.y; r[4 + o] = a.z; r[6 + o] = -a.w;
-            }
-#else
             if (lane < m2) {
                 float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (lane < m) a = pw[S.plist[lane]];
                 S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -a.w;
             }
-#endif
             __syncwarp();
             const float2 px = f2(pi.x), py = f2(pi.y), pz = f2(pi.z), e2 = f2(eps2);
             const float2 m1 = f2(-1.f);
             float2 sx = f2(0.f), sy = f2(0.f), sz = f2(0.f), spp = f2(0.f);
-#if SPH_WALK_ACC2
-            float2 tx = f2(0.f), ty = f2(0.f), tz = f2(0.f);
-#endif
 #pragma unroll 4
             for (int k = 0; k < m2; k += 2) {
-#if SPH_WALK_PARTS_V == 1
-                const float4 qa = q4[k], qb = q4[k + 1];
-                const float2 dx = __ffma2_rn(make_float2(qa.x, qa.y), m1, px);
-                const float2 dy = __ffma2_rn(make_float2(qa.z, qa.w), m1, py);
-                const float2 dz = __ffma2_rn(make_float2(qb.x, qb.y), m1, pz);
-                const float2 nm = make_float2(qb.z, qb.w);  // -m
-#else
                 const float2 dx = __ffma2_rn(ld2(&S.f[0][k]), m1, px);
                 const float2 dy = __ffma2_rn(ld2(&S.f[1][k]), m1, py);
                 const float2 dz = __ffma2_rn(ld2(&S.f[2][k]), m1, pz);
                 const float2 nm = ld2(&S.f[3][k]);  // -m
-#endif
                 float2 r2 = __ffma2_rn(dx, dx, e2);
                 r2 = __ffma2_rn(dy, dy, r2);
                 r2 = __ffma2_rn(dz, dz, r2);
                 const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                 const float2 nmr = __fmul2_rn(nm, rinv);
                 const float2 g = __fmul2_rn(nmr, __fmul2_rn(rinv, rinv));  // -m / r^3
-#if SPH_WALK_ACC2
-                if (k & 2) {
-                    tx = __ffma2_rn(g, dx, tx);
-                    ty = __ffma2_rn(g, dy, ty);
-                    tz = __ffma2_rn(g, dz, tz);
-                } else
-#endif
-                {
-                    sx = __ffma2_rn(g, dx, sx);
-                    sy = __ffma2_rn(g, dy, sy);
-                    sz = __ffma2_rn(g, dz, sz);
-                }
+                sx = __ffma2_rn(g, dx, sx);
+                sy = __ffma2_rn(g, dy, sy);
+                sz = __ffma2_rn(g, dz, sz);
                 if (POT) spp = __fadd2_rn(spp, nmr);
             }
-#if SPH_WALK_ACC2
-            sx = __fadd2_rn(sx, tx); sy = __fadd2_rn(sy, ty); sz = __fadd2_rn(sz, tz);
-#endif
             ax.add(sx.x + sx.y); ay.add(sy.x + sy.y); az.add(sz.x + sz.y);
             if (POT) ph.add(spp.x + spp.y);
             nP += m;

@@ -423,17 +423,20 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 6)
 // that the next list is complete from the particle's own candidates, at most
 // to 2 (1.5 h)
 __global__ void k_h_init(int n, const double *__restrict__ h, const double *__restrict__ hnb,
-                         double *__restrict__ hc, int *__restrict__ retry, double grow) {
+                         double *__restrict__ hc, int *__restrict__ retry, double grow,
+                         double *__restrict__ hover) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double hi = h[i];
     hc[i] = fmax(hi * grow, fmin(0.5 * (hi + 1.05 * hnb[i]), 1.5 * hi));
     retry[i] = 1;
+    if (hover) hover[i] = INFINITY;
 }
 
 struct NewtonArgs {
     const void *p1;  // Real4 (v, m)
     double *h_out, *hc;
+    double *hover;   // per particle: the smallest candidate radius / 2 whose row overflowed
     int *retry;
     double n_ngb, tol, grow;
     int max_iter, last_round;
@@ -455,14 +458,17 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
     const int craw = A.cnt[i];
     if (craw > A.K) {
         // more candidates inside 2 hc than the row holds: the sums would miss
-        // some, so shrink hc towards a half-full row and search again; h
-        // restarts just below the new radius
+        // some, so remember that radius, shrink hc towards a three-quarter
+        // full row and search again; h restarts at most just below the new
+        // radius
         if (!B.last_round) {
-            const double hc = B.hc[i] * fmax(0.5, cbrt(0.5 * A.K / (double)craw));
+            B.hover[i] = fmin(B.hover[i], B.hc[i]);
+            const double hc = B.hc[i] * fmax(0.5, cbrt(0.75 * A.K / (double)craw));
+            const double h0 = fmin(pi.w, hc / B.grow);
             B.hc[i] = hc;
             B.retry[i] = 1;
-            B.h_out[i] = hc / B.grow;
-            A.p0[i].w = hc / B.grow;
+            B.h_out[i] = h0;
+            A.p0[i].w = h0;
             status_add(A.status, SPH_S_H_RETRY, 1);
         } else {
             B.retry[i] = 0;
@@ -504,10 +510,12 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
         if (f < 0.0) lo = h; else hi = h;
         double hn = fp > 0.0 ? h - f / fp : -1.0;
         // a Newton step below the tolerance is accepted before any bracket
-        // test: in FP64 it can round to exactly h (= a bracket end)
+        // test: in FP64 it can round to exactly h (= a bracket end); one that
+        // ends beyond the candidate radius needs the wider search first
         if (fp > 0.0 && fabs(f / fp) < B.tol * h) {
             h = hn;
-            ok = true;
+            if (h > cap) need = true;
+            else ok = true;
             break;
         }
         // at most a factor 1.25 per iteration (keeps retries inside the rows)
@@ -530,12 +538,15 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
         const double dh = hn - h;
         h = hn;
         if (!clamped && fabs(dh) < B.tol * fabs(h - dh)) {
-            ok = true;
+            if (h > cap) need = true;
+            else ok = true;
             break;
         }
     }
     if (need && !B.last_round) {
-        B.hc[i] = h * B.grow;
+        // a wider search, kept below a radius whose row already overflowed
+        const double ov = B.hover[i];
+        B.hc[i] = h < ov ? fmin(h * B.grow, h + 0.5 * (ov - h)) : h * B.grow;
         B.retry[i] = 1;
     } else {
         B.retry[i] = 0;
@@ -735,7 +746,7 @@ int launch_smoothing_h(sph_ctx *ctx) {
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW);
+                                            ctx->retry, H_GROW, ctx->hover);
     const int rounds = ctx->prologue_done ? 4 : 8;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
@@ -743,6 +754,7 @@ int launch_smoothing_h(sph_ctx *ctx) {
     B.p1 = ctx->p1;
     B.h_out = ctx->st[c][ST_H];
     B.hc = ctx->hcand;
+    B.hover = ctx->hover;
     B.retry = ctx->retry;
     B.n_ngb = ctx->cfg.n_ngb;
     B.tol = ctx->cfg.h_tol;
@@ -772,7 +784,7 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW);
+                                            ctx->retry, H_GROW, nullptr);
     k_zero_int<<<div_up(n, 256), 256, 0, s>>>(n, ctx->hiter);
     // each round widens the radius by H_GROW; 0.3 % steps need about 26
     // iterations for that, so 16 rounds cover a 3.4x change of h

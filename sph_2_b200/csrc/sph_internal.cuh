@@ -116,6 +116,7 @@ struct sph_ctx {
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
     int *hiter = nullptr;        // per particle: iterations of the count iteration so far
     double *hcand = nullptr;     // candidate radius / 2 used per particle
+    double *hover = nullptr;     // smallest candidate radius / 2 whose row overflowed this call
     bool lists_ok = false, rho_ok = false, divcurl_ok = false;
 
     // time step, status, counters
