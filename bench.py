@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--static-grid", action="store_true",
                     help="group kernels on a grid over the groups instead of the work queue")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-cooling", action="store_true", help="skip the 2M cooling-cloud key")
+    ap.add_argument("--no-large", action="store_true", help="skip the 16M Evrard key")
+    ap.add_argument("--large-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -514,6 +517,16 @@ def main():
     if not a.no_ensemble:
         ens = ensemble_run(a, stream, timed_steps)
 
+    # ---- the cooling cloud (N = 2M) and the large Evrard run (N = 16M,
+    # learned cooling, 50 steps beside the FP64 plain path) ----
+    cool = large = None
+    if not a.no_cooling:
+        cool = cooling_run(a, stream, timed_steps)
+    if not a.no_large:
+        from types import SimpleNamespace
+        big = SimpleNamespace(**{**vars(a), "steps": a.large_steps, "warmup": 3})
+        large = large_evrard(big, stream, timed_steps)
+
     # ---- energy and momentum drift over 100 steps, N = 10,000 Evrard (the
     # plain FP64 method's own configuration: theta 0.5, Courant 0.25) ----
     conservation = {}
@@ -603,6 +616,8 @@ def main():
         "mixed_over_fp64_tuned_walk": (value / fp64["value"]) if fp64 else None,
         "theta_table_1M": theta_rows,
         "ensemble": ens,
+        "cooling_cloud_2M": cool,
+        "large_16M": large,
         "accel_err": err,
         "conservation_100_steps_n10k": conservation,
         "phases_ms": phases,
@@ -709,6 +724,44 @@ def large_evrard(a, stream, timed):
             "arms": res}
 
 
+def cooling_run(a, stream, timed, n=2_000_000):
+    """The cooling cloud collapse: N = 2M uniform sphere at n = 100 cm^-3, T =
+    1e4 K, Mach 2 turbulence (k^-4), the synthetic 128-bin Lambda(T) table;
+    the step with the exact implicit solve, then with the MLP surrogate
+    (trained on the GPU on 5M exact-solver samples) and its exact fallback.
+    The cooling phase is the u update + cooling solve + dt commit of a step."""
+    from sph_2_b200 import Config, Context, cooling, ic
+    from sph_2_b200 import _lib as L
+    d = ic.cooling_cloud(n, seed=42)
+    res = {}
+    for mode in ("exact", "mlp"):
+        flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
+        ctx = Context(Config(n_max=n, precision="mixed", leaf_size=a.leaf,
+                             flags=flags, **walk_kw(a, "mixed")))
+        ctx.set_stream(stream.cuda_stream)
+        cooling.setup(ctx, d["units"])
+        if mode == "mlp":
+            Xn, yn, norm, _ = cooling.training_set(ctx, n=5_000_000, seed=7)
+            ctx.mlp_set(cooling.init_params(seed=0), norm)
+            cooling.train(ctx, Xn, yn, steps=4000, batch=4096, lr=2e-3)
+        ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+        ctx.prologue()
+        k = max(2, a.steps // 2)
+        ms = timed(ctx, k, a.warmup)
+        ph = ctx.phase_times()
+        res[mode] = {"value": n * k / (ms * 1e-3), "ms_per_step": ms / k, "steps": k,
+                     "cooling_phase_ms": ph["update_dt"], "status": ctx.status()}
+        ctx.close()
+    return {"value": res["mlp"]["value"], "ms_per_step": res["mlp"]["ms_per_step"],
+            "config": {"workload": f"cooling_cloud_{n}", "n": n, "theta": a.theta, "mach": 2,
+                       "n_cgs": 100, "T": 1e4, "training_samples": 5_000_000,
+                       "cooling_phase": "u update + cooling solve + dt commit of the last step",
+                       "mlp_inference": "tcgen05.mma, TMEM accumulator, 128-row tiles"},
+            "exact": res["exact"], "mlp": res["mlp"],
+            "cooling_phase_mlp_over_exact": res["mlp"]["cooling_phase_ms"] /
+            res["exact"]["cooling_phase_ms"]}
+
+
 def extra_workload(a, world, rank, local):
     """The batched 64-cloud ensemble (clouds sharded over the ranks) or the
     2M-particle turbulent cooling cloud (exact implicit cooling vs the MLP
@@ -760,32 +813,7 @@ def extra_workload(a, world, rank, local):
     elif a.workload == "large":
         out.update(large_evrard(a, stream, timed))
     else:
-        n = a.n if a.n != 1_000_000 else 2_000_000
-        d = ic.cooling_cloud(n, seed=42)
-        res = {}
-        for mode in ("exact", "mlp"):
-            flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
-            ctx = Context(Config(n_max=n, precision="mixed", leaf_size=a.leaf,
-                                 flags=flags, **walk_kw(a, "mixed")))
-            ctx.set_stream(stream.cuda_stream)
-            cooling.setup(ctx, d["units"])
-            if mode == "mlp":
-                Xn, yn, norm, _ = cooling.training_set(ctx, n=1_000_000, seed=7)
-                ctx.mlp_set(cooling.init_params(seed=0), norm)
-                cooling.train(ctx, Xn, yn, steps=3000, batch=4096, lr=2e-3)
-            ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
-            ctx.prologue()
-            ms = timed(ctx, a.steps, a.warmup)
-            ph = ctx.phase_times()
-            res[mode] = {"value": n * a.steps / (ms * 1e-3), "ms_per_step": ms / a.steps,
-                         "cooling_phase_ms": ph["update_dt"],
-                         "cooling_phase": "u update + cooling solve + dt commit of the last step",
-                         "status": ctx.status()}
-            ctx.close()
-        out.update(value=res["mlp"]["value"], ms_per_step=res["mlp"]["ms_per_step"],
-                   config={"workload": f"cooling_cloud_{n}", "n": n, "theta": a.theta,
-                           "mach": 2, "n_cgs": 100, "T": 1e4},
-                   exact=res["exact"], mlp=res["mlp"])
+        out.update(cooling_run(a, stream, timed, a.n if a.n != 1_000_000 else 2_000_000))
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
