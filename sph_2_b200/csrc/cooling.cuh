@@ -160,6 +160,87 @@ __device__ __forceinline__ bool cool_accept(const CoolDev &c, double rho, double
     return cool_monotone(c, rho, dt, lo, hi);
 }
 
+// ---- the surrogate's side in FP32 -------------------------------------------
+// The surrogate is accepted to a relative error of mlp_err_tol (1e-3 by
+// default), far above FP32 rounding, so its Newton polish, error estimate and
+// monotonicity test run in FP32, where the logarithm and exponential are
+// single SFU instructions (the FP64 ones are long FMA-pipe sequences and made
+// the FP64 polish as slow as the exact bisection it should replace).  The
+// residual u - u_old - ratefact * net * dt is formed in FP32 from FP32 u and
+// u_old: its rounding (~1e-7 u) is four orders below the tolerance.  The
+// exact solver and the fallback stay in FP64.
+__device__ __forceinline__ float cool_lambda_f(const CoolDev &c, float T, float *slope) {
+    const float lt = __log10f(T);
+    const float lT0 = (float)c.logT0;
+    const float dl = (float)((c.logT1 - c.logT0) / c.nb);
+    int k = (int)floorf((lt - lT0) / dl);
+    k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
+    const float L0 = (float)c.logL[k], L1 = (float)c.logL[k + 1];
+    const float s = (L1 - L0) / dl;
+    if (slope) *slope = s;
+    return __exp10f(L0 + s * (lt - (lT0 + k * dl)));
+}
+
+__device__ __forceinline__ void cool_newton_polish_f(const CoolDev &c, double rho, double u_old,
+                                                     double dt, double *u, double *est, double tol) {
+    const float nH = (float)(c.XH * rho / MH_CGS);
+    const float ratefact = (float)((c.XH * rho / MH_CGS) * (c.XH * rho / MH_CGS) / rho);
+    const float kT = (float)((c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS);
+    const float gn = (float)(c.gheat / (c.XH * rho / MH_CGS));
+    const float uo = (float)u_old, fdt = (float)dt, ftol = (float)tol;
+    float uu = (float)*u;
+    *est = INFINITY;
+    for (int it = 0; it < 5; it++) {
+        float s;
+        const float lam = cool_lambda_f(c, kT * uu, &s);
+        const float r = uu - uo - ratefact * (gn - lam) * fdt;
+        const float rp = 1.f + ratefact * fdt * s * lam / uu;
+        if (!(rp > 0.f) || !(uu > 0.f)) break;  // the estimate is void here
+        const float e = fabsf(r / rp) / uu;
+        *u = (double)uu;
+        *est = (double)e;
+        if (e <= 0.25f * ftol || it == 4) break;
+        const float u1 = uu - r / rp;
+        if (!(u1 > 0.f)) break;
+        uu = u1;
+    }
+    (void)nH;
+}
+
+__device__ __forceinline__ bool cool_monotone_f(const CoolDev &c, double rho, double dt, double u_lo,
+                                                double u_hi) {
+    const float A = (float)((c.XH * rho / MH_CGS) * (c.XH * rho / MH_CGS) / rho * dt);
+    const float kT = (float)((c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS);
+    const float lT0 = (float)c.logT0;
+    const float dl = (float)((c.logT1 - c.logT0) / c.nb);
+    const float T0 = kT * (float)u_lo, T1 = kT * (float)u_hi;
+    if (!(T0 > 0.f) || !(T1 >= T0)) return false;
+    const float l0 = __log10f(T0), l1 = __log10f(T1);
+    int k = (int)floorf((l0 - lT0) / dl);
+    k = k < 0 ? 0 : (k > c.nb - 1 ? c.nb - 1 : k);
+    float s = (float)(c.logL[k + 1] - c.logL[k]) / dl;
+    if (s < 0.f) {
+        const float lam = __exp10f((float)c.logL[k] + s * (l0 - (lT0 + k * dl)));
+        if (!(1.f + A * s * lam * kT / T0 > 0.f)) return false;
+    }
+    int kend = (int)floorf((l1 - lT0) / dl);
+    kend = kend > c.nb - 1 ? c.nb - 1 : kend;
+    for (int e = k + 1; e <= kend; e++) {
+        s = (float)(c.logL[e + 1] - c.logL[e]) / dl;
+        if (s < 0.f) {
+            if (!(1.f + A * s * (float)c.lamT[e] * kT > 0.f)) return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool cool_accept_f(const CoolDev &c, double rho, double u_old, double dt,
+                                              double un, double est, double tol) {
+    if (!(est <= tol) || !(un > 0.0)) return false;
+    const double lo = fmin(u_old, un / 1.1), hi = fmax(u_old, un * 1.1);
+    return cool_monotone_f(c, rho, dt, lo, hi);
+}
+
 static inline CoolDev cool_dev_of(const sph_ctx *ctx) {
     const sph_cooling_params &p = ctx->cool;
     CoolDev c;

@@ -444,9 +444,9 @@ __global__ void __launch_bounds__(128)
         const float y = predict32(S, xs[w], ys[w], norm, own, rho_c, u0, dt_c);
         if (own) {
             const double dl = (double)y * norm[7] + norm[6];
-            double un = u0 * exp10(dl), est;
-            cool_newton_polish(c, rho_c, u0, dt_c, &un, &est, err_tol);
-            if (cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+            double un = u0 * (double)__exp10f((float)dl), est;
+            cool_newton_polish_f(c, rho_c, u0, dt_c, &un, &est, err_tol);
+            if (cool_accept_f(c, rho_c, u0, dt_c, un, est, err_tol)) {
                 u[i] = un / uu;
             } else {
                 status_add(status, SPH_S_MLP_FALLBACK, 1);
@@ -495,10 +495,10 @@ __global__ void __launch_bounds__(128)
         const float y = predict32(S, xs[w], ys[w], norm, own, r, u0, d);
         if (own) {
             const double dl = (double)y * norm[7] + norm[6];
-            double un = u0 * exp10(dl), est;
-            cool_newton_polish(c, r, u0, d, &un, &est, err_tol);
+            double un = u0 * (double)__exp10f((float)dl), est;
+            cool_newton_polish_f(c, r, u0, d, &un, &est, err_tol);
             int fb = 0;
-            if (cool_accept(c, r, u0, d, un, est, err_tol)) {
+            if (cool_accept_f(c, r, u0, d, un, est, err_tol)) {
                 u_new[i] = un;
             } else {
                 fb = 1;
@@ -766,10 +766,10 @@ __global__ void __launch_bounds__(tc::ROWS)
         if (own) {
             double un = u0, est = INFINITY;
             if (ok) {
-                un = u0 * exp10((double)y * norm[7] + norm[6]);
-                cool_newton_polish(c, rho_c, u0, dt_c, &un, &est, err_tol);
+                un = u0 * (double)__exp10f(y * norm[7] + norm[6]);
+                cool_newton_polish_f(c, rho_c, u0, dt_c, &un, &est, err_tol);
             }
-            if (ok && cool_accept(c, rho_c, u0, dt_c, un, est, err_tol)) {
+            if (ok && cool_accept_f(c, rho_c, u0, dt_c, un, est, err_tol)) {
                 u[i] = un / uu;
             } else {
                 status_add(status, SPH_S_MLP_FALLBACK, 1);
@@ -808,11 +808,11 @@ __global__ void __launch_bounds__(tc::ROWS)
         if (own) {
             double un = u0, est = INFINITY;
             if (ok) {
-                un = u0 * exp10((double)y * norm[7] + norm[6]);
-                cool_newton_polish(c, r, u0, d, &un, &est, err_tol);
+                un = u0 * (double)__exp10f(y * norm[7] + norm[6]);
+                cool_newton_polish_f(c, r, u0, d, &un, &est, err_tol);
             }
             int fb = 0;
-            if (ok && cool_accept(c, r, u0, d, un, est, err_tol)) {
+            if (ok && cool_accept_f(c, r, u0, d, un, est, err_tol)) {
                 u_new[i] = un;
             } else {
                 fb = 1;
