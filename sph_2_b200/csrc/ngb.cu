@@ -738,7 +738,12 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
 
 }  // namespace
 
-static const double H_GROW = 1.08;
+// margin of the candidate radius over h: h may grow by this factor inside one
+// search round before the particle is searched again
+#ifndef SPH_H_GROW
+#define SPH_H_GROW 1.08
+#endif
+static const double H_GROW = SPH_H_GROW;
 
 int launch_smoothing_h(sph_ctx *ctx) {
     const int n = ctx->n;
