@@ -461,6 +461,17 @@ typedef struct sph_outflow_params {
 int sph_outflow_inject(sph_ctx *ctx, const sph_outflow_params *p, double *leftover_mass,
                        int32_t *n_added);
 
+/* ---- FP64 restart (replaces the float text dumps the reference restarts
+ * from, GPU_sph/With_metal_cooling/Check_Restart_version/hfv_sph_gpu_v5.cu) ----
+ * The file holds the particle state in FP64 and in the context's storage
+ * order (ids and clouds, x y z vx vy vz m h u du/dt_prev and the largest
+ * neighbour h), the last step's accelerations and every cloud's dt.  A context
+ * that reads it (capacity permitting) continues exactly as the writing context
+ * would have: the next sph_step repeats it bit for bit in the same precision.
+ * Cooling tables and surrogate parameters are not part of it. */
+int sph_write_restart(sph_ctx *ctx, const char *path);
+int sph_read_restart(sph_ctx *ctx, const char *path);
+
 /* ---- the reference's binary files (host I/O) ---- */
 /* IC file of IC_evrard4.cu:245-260 / readVectorsFromFile
  * (hfvCLibs_v7_hfv_v2.h:59-101): int32 N, int32 Typ[N], then float32 x, y, z,

@@ -158,6 +158,8 @@ SIGNATURES = [
     ("sph_load_ic", C.c_int, [_P, C.c_char_p, _P]),
     ("sph_write_ic", C.c_int, [_P, C.c_char_p, _P]),
     ("sph_write_snapshot", C.c_int, [_P, C.c_char_p, _P, _I]),
+    ("sph_write_restart", C.c_int, [_P, C.c_char_p]),
+    ("sph_read_restart", C.c_int, [_P, C.c_char_p]),
     ("sph_prologue", C.c_int, [_P]),
     ("sph_step", C.c_int, [_P, _I]),
 ]

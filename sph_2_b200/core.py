@@ -171,6 +171,15 @@ class Context:
         self._chk(self._L.sph_write_snapshot(self._h, str(path).encode(), _ptr(ion), nion),
                   "sph_write_snapshot")
 
+    def write_restart(self, path):
+        """FP64 restart file of the whole state (storage order kept)."""
+        self._chk(self._L.sph_write_restart(self._h, str(path).encode()), "sph_write_restart")
+
+    def read_restart(self, path):
+        """Replace the particles with a restart file's; the next step
+        continues exactly where the writing context would have."""
+        self._chk(self._L.sph_read_restart(self._h, str(path).encode()), "sph_read_restart")
+
     def get(self, name: str, storage_order=False, out=None) -> np.ndarray:
         """Field in original (or storage) order.  `out`: an existing C-contiguous
         float64 array of n values (e.g. pinned host memory) to copy into."""

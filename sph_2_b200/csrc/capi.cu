@@ -39,6 +39,15 @@ int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem) {
     return ctx->num_sms * per_sm;
 }
 
+void drop_graphs(sph_ctx *ctx) {
+    for (int k = 0; k < 2; k++)
+        if (ctx->graph[k]) {
+            cudaGraphExecDestroy(ctx->graph[k]);
+            ctx->graph[k] = nullptr;
+        }
+    ctx->graph_valid = false;
+}
+
 int queue_launch(sph_ctx *ctx, cudaStream_t s, int slot, const void *kernel, int block,
                  int static_grid, int *grid, unsigned **queue) {
     if (ctx->cfg.flags & SPH_FLAG_STATIC_GRID) {
@@ -149,14 +158,6 @@ double *field_ptr(sph_ctx *ctx, int f) {
     }
 }
 
-void drop_graphs(sph_ctx *ctx) {
-    for (int k = 0; k < 2; k++)
-        if (ctx->graph[k]) {
-            cudaGraphExecDestroy(ctx->graph[k]);
-            ctx->graph[k] = nullptr;
-        }
-    ctx->graph_valid = false;
-}
 
 int enter(sph_ctx *ctx) {
     if (!ctx) return SPH_ERR_ARG;

@@ -14,6 +14,7 @@
 // outflow particle types are outside it, so an IC holding them is rejected.
 // The snapshot's per-particle int32 debug slot carries the neighbour count.
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "sph_internal.cuh"
@@ -145,4 +146,128 @@ int sph_write_snapshot(sph_ctx *ctx, const char *path, const float *ion_frac, in
     ok = ok && F.write(ion_frac, sizeof(float) * n_ion_frac) &&
          F.write(ngb.data(), sizeof(int32_t) * n);
     return ok ? SPH_OK : SPH_ERR_IO;
+}
+
+// ---- FP64 restart -----------------------------------------------------------
+// The reference restarts from text dumps of its float arrays
+// (GPU_sph/With_metal_cooling/Check_Restart_version/hfv_sph_gpu_v5.cu); a run
+// resumed from those differs from the run that continued.  The restart file
+// here holds what the next step reads, in FP64 and in storage order: the
+// state fields (x y z vx vy vz m h u du/dt_prev and the largest neighbour h,
+// which sets the next candidate radius), the original ids and clouds, the
+// accelerations of the last step (the next step's first kick uses them) and
+// every cloud's time step.  Reading it restores the storage order as well, so
+// the next sort sees the same input order and the resumed run repeats the
+// continuing one bit for bit.  Cooling tables and MLP parameters are set up
+// separately.
+//   char magic[8] "SPHB200R"; int32 version (1), n, ncloud, prologue_done,
+//   last_injected_id, pad; int64 step_count;
+//   int32 cloud_start[ncloud + 1]; double dt[ncloud];
+//   int32 id[n], cloud[n]; double state[ST_N][n]; double a_sph[3n], a_grav[3n]
+namespace {
+const char RESTART_MAGIC[8] = {'S', 'P', 'H', 'B', '2', '0', '0', 'R'};
+struct RestartHeader {
+    char magic[8];
+    int32_t version, n, ncloud, prologue_done, last_injected_id, pad;
+    int64_t step_count;
+};
+}  // namespace
+
+int sph_write_restart(sph_ctx *ctx, const char *path) {
+    if (!ctx || !path) return SPH_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int n = ctx->n, nc = ctx->ncloud, c = ctx->cur;
+    RestartHeader h{};
+    memcpy(h.magic, RESTART_MAGIC, 8);
+    h.version = 1;
+    h.n = n;
+    h.ncloud = nc;
+    h.prologue_done = ctx->prologue_done ? 1 : 0;
+    h.last_injected_id = ctx->last_injected_id;
+    h.step_count = ctx->step_count;
+    std::vector<double> dt(nc > 0 ? nc : 1);
+    std::vector<int32_t> ids(n > 0 ? n : 1), cl(n > 0 ? n : 1);
+    std::vector<double> buf((size_t)(n > 0 ? n : 1) * 3);
+    if (nc > 0) CK(cudaMemcpy(dt.data(), ctx->dt, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+    if (n > 0) {
+        CK(cudaMemcpy(ids.data(), ctx->id[c], sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(cl.data(), ctx->cloud[c], sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    }
+    HostFile F(path, "wb");
+    if (!F.f) return SPH_ERR_IO;
+    bool ok = F.write(&h, sizeof h) &&
+              F.write(ctx->cloud_start_h.data(), sizeof(int32_t) * (nc + 1)) &&
+              F.write(dt.data(), sizeof(double) * nc) && F.write(ids.data(), sizeof(int32_t) * n) &&
+              F.write(cl.data(), sizeof(int32_t) * n);
+    for (int k = 0; k < ST_N && ok; k++) {
+        if (n > 0) CK(cudaMemcpy(buf.data(), ctx->st[c][k], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        ok = F.write(buf.data(), sizeof(double) * n);
+    }
+    for (double *a : {ctx->asph, ctx->agrav}) {
+        if (!ok) break;
+        if (n > 0) CK(cudaMemcpy(buf.data(), a, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+        ok = F.write(buf.data(), sizeof(double) * 3 * n);
+    }
+    return ok ? SPH_OK : SPH_ERR_IO;
+}
+
+int sph_read_restart(sph_ctx *ctx, const char *path) {
+    if (!ctx || !path) return SPH_ERR_ARG;
+    HostFile F(path, "rb");
+    if (!F.f) return SPH_ERR_IO;
+    const long long sz = file_bytes(F.f);
+    RestartHeader h{};
+    if (sz < (long long)sizeof h || !F.read(&h, sizeof h) || memcmp(h.magic, RESTART_MAGIC, 8) != 0 ||
+        h.version != 1 || h.n < 0 || h.ncloud < 1)
+        return SPH_ERR_IO;
+    const long long n = h.n, nc = h.ncloud;
+    const long long want = (long long)sizeof h + 4 * (nc + 1) + 8 * nc + 8 * n + 8 * n * (ST_N + 6);
+    if (sz != want) return SPH_ERR_IO;
+    if (n > ctx->cfg.n_max || nc > ctx->cfg.n_cloud_max) return SPH_ERR_CAPACITY;
+    std::vector<int32_t> cs(nc + 1), ids(n > 0 ? n : 1), cl(n > 0 ? n : 1);
+    std::vector<double> dt(nc), buf((size_t)(n > 0 ? n : 1) * 3);
+    if (!F.read(cs.data(), 4 * (nc + 1)) || !F.read(dt.data(), 8 * nc) || !F.read(ids.data(), 4 * n) ||
+        !F.read(cl.data(), 4 * n))
+        return SPH_ERR_IO;
+    if (cs[0] != 0 || cs[nc] != n) return SPH_ERR_IO;
+    CK(cudaSetDevice(ctx->device));
+    drop_graphs(ctx);
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaStream_t s = ctx->stream;
+    ctx->cur = 0;
+    for (int k = 0; k < ST_N; k++) {
+        if (!F.read(buf.data(), 8 * n)) return SPH_ERR_IO;
+        if (n > 0) CK(cudaMemcpy(ctx->st[0][k], buf.data(), 8 * n, cudaMemcpyHostToDevice));
+    }
+    for (double *a : {ctx->asph, ctx->agrav}) {
+        if (!F.read(buf.data(), 8 * 3 * n)) return SPH_ERR_IO;
+        if (n > 0) CK(cudaMemcpy(a, buf.data(), 8 * 3 * n, cudaMemcpyHostToDevice));
+    }
+    if (n > 0) {
+        CK(cudaMemcpy(ctx->id[0], ids.data(), 4 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->cloud[0], cl.data(), 4 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemset(ctx->divV, 0, 8 * n));
+        CK(cudaMemset(ctx->curlV, 0, 8 * n));
+        CK(cudaMemset(ctx->pot, 0, 8 * n));
+    }
+    ctx->n = (int)n;
+    ctx->ncloud = (int)nc;
+    ctx->ngroup = (int)(n + nc);
+    ctx->cloud_start_h.assign(cs.begin(), cs.end());
+    CK(cudaMemcpy(ctx->cloud_start, cs.data(), 4 * (nc + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->dt, dt.data(), 8 * nc, cudaMemcpyHostToDevice));
+    CK(cudaMemset(ctx->dt_bits, 0xff, 8 * nc));
+    CK(cudaMemset(ctx->d_ngroup, 0, sizeof(int)));
+    int rc = launch_pack_p1(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s));
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = ctx->cand_ok = false;
+    ctx->p2_dirty = true;
+    ctx->prologue_done = h.prologue_done != 0;
+    ctx->step_count = h.step_count;
+    ctx->last_injected_id = h.last_injected_id;
+    return ctx_check_launch(ctx, "read_restart");
 }

@@ -162,6 +162,7 @@ struct sph_ctx {
 };
 
 int ctx_fail(sph_ctx *ctx, cudaError_t e, const char *what, int line);
+void drop_graphs(sph_ctx *ctx);  // the step graphs are re-captured at the next sph_step
 int ctx_check_launch(sph_ctx *ctx, const char *what);
 
 // ----------------------------------------------------------------------------
