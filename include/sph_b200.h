@@ -238,6 +238,13 @@ int sph_smoothing_h(sph_ctx *ctx);
  * Needs sph_build_tree. */
 int sph_smoothing_h_count(sph_ctx *ctx, int32_t n_target, int32_t n_tol, double step_frac,
                           int32_t max_iter);
+/* The reference's starting smoothing length (smoothing_length_mpi,
+ * MPI_sph/sph_code/libsx.py:777-800 with k = 50): h = half the k-th smallest
+ * distance to the particles of its cloud, the particle itself counted at
+ * distance 0, the distance rounded as the reference computes it; the
+ * candidate search starts from the current h.  k + 1 must not exceed max_ngb.
+ * Needs sph_build_tree. */
+int sph_smoothing_length_kth(sph_ctx *ctx, int32_t k);
 /* Exact neighbour lists |r_ij|^2 <= (h_i+h_j)^2 (replaces ngbDB_new_v2,
  * ngb_v3.h:124-238).  Needs sph_build_tree (h_max is refitted here). */
 int sph_neighbours(sph_ctx *ctx);

@@ -114,6 +114,7 @@ SIGNATURES = [
     ("sph_get_groups", C.c_int, [_P, _P, _P, _P, _I]),
     ("sph_smoothing_h", C.c_int, [_P]),
     ("sph_smoothing_h_count", C.c_int, [_P, _I, _I, _D, _I]),
+    ("sph_smoothing_length_kth", C.c_int, [_P, _I]),
     ("sph_neighbours", C.c_int, [_P]),
     ("sph_get_neighbours", C.c_int, [_P, _P, _P, C.c_int64, _I]),
     ("sph_density", C.c_int, [_P]),

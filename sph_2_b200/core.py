@@ -271,6 +271,11 @@ class Context:
                                                 float(step_frac), int(max_iter)),
                   "sph_smoothing_h_count")
 
+    def smoothing_length_kth(self, k=50):
+        """h = half the k-th smallest distance (self at 0), the reference's
+        smoothing_length_mpi (libsx.py:777-800) for k = 50."""
+        self._chk(self._L.sph_smoothing_length_kth(self._h, int(k)), "sph_smoothing_length_kth")
+
     def neighbours(self):
         self._chk(self._L.sph_neighbours(self._h), "sph_neighbours")
 

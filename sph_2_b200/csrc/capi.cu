@@ -679,6 +679,15 @@ int sph_smoothing_h_count(sph_ctx *ctx, int32_t n_target, int32_t n_tol, double 
     return launch_smoothing_h_count(ctx, n_target, n_tol, step_frac, max_iter);
 }
 
+int sph_smoothing_length_kth(sph_ctx *ctx, int32_t k) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!ctx->tree_ok) return SPH_ERR_STATE;
+    if (k < 0 || k + 1 > ctx->cfg.max_ngb) return SPH_ERR_ARG;
+    drop_graphs(ctx);
+    return launch_smoothing_kth(ctx, k);
+}
+
 int sph_neighbours(sph_ctx *ctx) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -687,6 +687,74 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
     }
 }
 
+// Half the k-th smallest distance (self at index 0) of the particle of one
+// lane (smoothing_length_mpi, MPI_sph/sph_code/libsx.py:777-800: np.sort(dist)
+// [50] / 2).  With a complete row (every j with d_j <= 2 hc) holding at least
+// k + 1 entries, the k-th smallest distance overall is the row's; it is found
+// by bisection over the bit patterns of the row's distances (non-negative
+// doubles order like their patterns), so the value is one of the distances,
+// rounded as the reference computes them.  A row with too few entries widens
+// the radius, one that overflows narrows it, and the particle searches again.
+__device__ __forceinline__ void kth_lane(const SearchArgs &A, const CountArgs &B, int i,
+                                         const double4 &pi, const int *row, int k) {
+    const int craw = A.cnt[i];
+    const double cap = B.hc[i];
+    bool again = false;
+    if (craw > A.K) {
+        B.hc[i] = cap * fmax(0.5, cbrt(0.75 * A.K / (double)craw));
+        again = true;
+    } else if (craw < k + 1) {
+        B.hc[i] = cap * (craw > 0 ? fmin(2.0, fmax(1.1, cbrt(1.5 * (k + 1) / (double)craw))) : 2.0);
+        again = true;
+    } else {
+        // every row entry lies within 2 cap up to the rounding of the
+        // search's r^2 test; hi bounds them all
+        unsigned long long lo = 0,
+                           hi = (unsigned long long)__double_as_longlong(2.0 * cap * (1.0 + 1e-9));
+        for (int it = 0; it < 64 && lo < hi; it++) {
+            const unsigned long long mid = lo + (hi - lo) / 2;
+            const double v = __longlong_as_double((long long)mid);
+            int c = 0;
+            for (int q = 0; q < craw; q++) c += ref_dist(pi, A.p0[row[q]]) <= v;
+            if (c >= k + 1) hi = mid;
+            else lo = mid + 1;
+        }
+        const double d = __longlong_as_double((long long)lo);
+        if (d > 2.0 * cap * (1.0 - 1e-12)) {
+            // at the radius itself a particle outside the row could be nearer
+            // by a rounding: search again, wider
+            B.hc[i] = cap * 1.1;
+            again = true;
+        } else {
+            B.h_out[i] = 0.5 * d;
+            A.p0[i].w = 0.5 * d;
+        }
+    }
+    if (again) status_add(A.status, SPH_S_H_RETRY, 1);
+    const bool retry = again && !B.last_round;
+    B.retry[i] = retry ? 1 : 0;
+    if (again && !retry) status_add(A.status, SPH_S_H_NOCONV, 1);
+}
+
+__global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
+    k_cand_kth(const int *__restrict__ ngroup_p, SearchArgs A, CountArgs B, int k, unsigned *queue) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
+         g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
+        const int s0 = A.gstart[g], gc = A.gcount[g];
+        bool act = lane < gc;
+        const int i = s0 + (act ? lane : 0);
+        act = act && B.retry[i];
+        if (!__ballot_sync(FULL, act)) continue;
+        const double4 pi = A.p0[i];
+        group_search<2, double>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i]);
+        if (act) kth_lane(A, B, i, pi, A.cidx + (size_t)i * A.K, k);
+        __syncwarp();
+    }
+}
+
 __global__ void k_zero_int(int n, int *__restrict__ a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = 0;
@@ -819,6 +887,38 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     ctx->cand_ok = true;
     ctx->p2_dirty = true;
     return ctx_check_launch(ctx, "smoothing_h_count");
+}
+
+// h = half the k-th neighbour distance, the search radius started from the
+// current h
+int launch_smoothing_kth(sph_ctx *ctx, int k) {
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int c = ctx->cur;
+    k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
+                                            ctx->retry, H_GROW, nullptr);
+    const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
+    SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
+    CountArgs B{};
+    B.h_out = ctx->st[c][ST_H];
+    B.hc = ctx->hcand;
+    B.retry = ctx->retry;
+    B.iters = ctx->hiter;
+    B.grow = H_GROW;
+    const int rounds = 24;
+    for (int r = 0; r < rounds; r++) {
+        B.last_round = r == rounds - 1;
+        int g;
+        unsigned *q;
+        int rc = queue_launch(ctx, s, WQ_SEARCH, (const void *)k_cand_kth, SEARCH_WARPS * 32, grid, &g, &q);
+        if (rc) return rc;
+        k_cand_kth<<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, k, q);
+    }
+    ctx->lists_ok = false;
+    ctx->cand_ok = false;  // the rows are candidate sets of the search radius, not of h
+    ctx->p2_dirty = true;
+    return ctx_check_launch(ctx, "smoothing_kth");
 }
 
 int launch_neighbours(sph_ctx *ctx) {

@@ -323,6 +323,7 @@ int launch_tree(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);
 int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac, int max_iter);
+int launch_smoothing_kth(sph_ctx *ctx, int k);
 int launch_neighbours(sph_ctx *ctx);
 int launch_density(sph_ctx *ctx);
 int launch_divcurl(sph_ctx *ctx);

@@ -18,10 +18,10 @@ iteration (libsx.py:806-902) on the GPU and return the same h bit for bit.
 The project's Newton smoothing length, which solves (4 pi / 3)(2h)^3 rho(h) =
 N_ngb m, is offered under its own name, h_newton_mpi.
 
+smoothing_length_mpi (half the 50th-neighbour distance, libsx.py:777-800) is
+the reference's too, bit for bit.
+
 Differences from the reference, by design:
-* smoothing_length_mpi returns the Newton smoothing length started from a
-  uniform-density guess instead of half the 50th-neighbour distance
-  (libsx.py:781-803); both are starting values for h_smooth_fast_mpi.
 * getPressure / getCsound / getKE are elementwise host formulas (no kernel is
   worth a launch there); getPE is the FP64 sum of the tree walk's Plummer
   potential.
@@ -358,15 +358,22 @@ def h_newton_mpi(nbeg, nend, pos, h, m=None, n_ngb=50.0):
     return _rows(_out(ctx, "h", pos), nbeg, nend)
 
 
-def smoothing_length_mpi(nbeg, nend, pos, m=None, n_ngb=50.0):
-    """Initial smoothing lengths (replaces libsx.py:781-803): the Newton
-    solution started from a uniform-density guess."""
+def smoothing_length_mpi(nbeg, nend, pos):
+    """libsx.py:777-800: half the distance to the 50th neighbour (the sorted
+    distances' entry 50, the particle itself at entry 0), rows nbeg..nend-1,
+    bit-exact with the reference."""
     n = int(pos.shape[0])
     p = _host(pos)
     ext = np.ptp(p, axis=0).prod() if n > 1 else 1.0
-    h0 = 0.5 * (max(ext, 1e-300) * n_ngb / max(n, 1)) ** (1.0 / 3.0)
+    h0 = 0.5 * (max(ext, 1e-300) * 50.0 / max(n, 1)) ** (1.0 / 3.0)   # search start
     h = np.full(n, h0) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + h0
-    return h_newton_mpi(nbeg, nend, pos, h, m, n_ngb)
+    mm = np.full(n, 1.0 / n) if not _is_cuda_tensor(pos) else _zeros_like_dev(n) + 1.0 / n
+    ctx = _load_state(pos, mm, h)
+    ctx.smoothing_length_kth(50)
+    st = ctx.status(reset=True)
+    if st["h_noconv"]:
+        raise L.SphError(-4, "smoothing_length_mpi", f"({st['h_noconv']} rows did not converge)")
+    return _rows(_out(ctx, "h", pos), nbeg, nend)
 
 
 # ---- elementwise formulas and energies -----------------------------------

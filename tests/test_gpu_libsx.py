@@ -88,8 +88,9 @@ def test_smoothing_length(g):
     x, y, z = (g["pos"][:, k].copy() for k in range(3))
     ho, _, bad = O.newton_h(x, y, z, g["m"], g["h"], n_ngb=50.0)
     assert bad == 0 and np.max(np.abs(hn / ho - 1)) < 2e-3
-    h0 = X.smoothing_length_mpi(0, n, g["pos"], m=g["m"])
-    assert np.max(np.abs(h0 / ho - 1)) < 2e-3
+    # the reference's starting h: half the 50th-neighbour distance
+    assert np.array_equal(X.smoothing_length_mpi(0, n, g["pos"]), g["h0"])
+    assert np.array_equal(X.smoothing_length_mpi(17, 99, g["pos"]), g["h0"][17:99])
 
 
 def test_torch_cuda_tensors(g):

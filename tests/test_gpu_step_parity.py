@@ -318,3 +318,31 @@ def test_h_and_lists_with_sparse_outskirts(precision):
     off, lst = ctx.neighbour_lists()
     oo, ol = O.neighbours(x, y, z, h)
     assert np.array_equal(off, oo) and np.array_equal(lst, ol)
+
+
+# ------------------------------------------- the reference's starting h ---
+@pytest.mark.parametrize("fixture", ["ref_sph_evrard_n600.npz", "ref_sph_ragged_n64.npz"])
+def test_kth_neighbour_h_equals_reference_golden(fixture):
+    """smoothing_length_mpi's half 50th-neighbour distance, from a search
+    radius that starts 30 % short, equals the reference's h0 bit for bit."""
+    g = dict(np.load(os.path.join(GOLD, fixture)))
+    n = len(g["m"])
+    ctx = Context(Config(n_max=n, precision="fp64", max_ngb=256))
+    ctx.load(g["pos"], g["v"], g["m"], 0.7 * g["h0"], g["u"])
+    ctx.sort(); ctx.build_tree()
+    ctx.smoothing_length_kth(50)
+    assert ctx.status()["h_noconv"] == 0
+    assert np.array_equal(ctx.get("h"), g["h0"])
+
+
+def test_kth_neighbour_h_equals_oracle_on_evrard():
+    n = 5_000
+    d = ic.evrard(n, seed=6)
+    h0 = d["h"] * np.random.default_rng(4).uniform(0.3, 2.0, n)
+    ctx = Context(Config(n_max=n, precision="mixed"))
+    ctx.load(d["pos"], d["vel"], d["m"], h0, d["u"])
+    ctx.sort(); ctx.build_tree()
+    ctx.smoothing_length_kth(50)
+    assert ctx.status()["h_noconv"] == 0
+    ho = O.ref_smoothing_length(0, n, np.ascontiguousarray(d["pos"]))
+    assert np.array_equal(ctx.get("h"), ho)
