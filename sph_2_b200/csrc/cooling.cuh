@@ -183,10 +183,10 @@ __device__ __forceinline__ float cool_lambda_f(const CoolDev &c, float T, float 
 
 __device__ __forceinline__ void cool_newton_polish_f(const CoolDev &c, double rho, double u_old,
                                                      double dt, double *u, double *est, double tol) {
-    const float nH = (float)(c.XH * rho / MH_CGS);
-    const float ratefact = (float)((c.XH * rho / MH_CGS) * (c.XH * rho / MH_CGS) / rho);
+    const double nHd = c.XH * rho / MH_CGS;
+    const float ratefact = (float)(nHd * nHd / rho);
     const float kT = (float)((c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS);
-    const float gn = (float)(c.gheat / (c.XH * rho / MH_CGS));
+    const float gn = (float)(c.gheat / nHd);
     const float uo = (float)u_old, fdt = (float)dt, ftol = (float)tol;
     float uu = (float)*u;
     *est = INFINITY;
@@ -204,7 +204,6 @@ __device__ __forceinline__ void cool_newton_polish_f(const CoolDev &c, double rh
         if (!(u1 > 0.f)) break;
         uu = u1;
     }
-    (void)nH;
 }
 
 __device__ __forceinline__ bool cool_monotone_f(const CoolDev &c, double rho, double dt, double u_lo,

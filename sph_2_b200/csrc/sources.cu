@@ -38,14 +38,14 @@ __device__ __forceinline__ double pair_uniform(unsigned long long seed, long lon
     return (double)((z >> 11) + 1) * 0x1.0p-53;
 }
 
-__global__ void k_inject_pairs(int npairs, long long pair0, unsigned long long seed, int n0,
-                               int id0, int cloud, double r_max, double v_in, double m,
+__global__ void k_inject_pairs(int npairs, unsigned long long seed, int n0, int id0, int cloud,
+                               double r_max, double v_in, double m,
                                double u, const double *__restrict__ h_src, double *const *st,
                                int *__restrict__ id, int *__restrict__ cl,
                                double *__restrict__ dudt) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
-    const long long j = pair0 + p;
+    const long long j = p;
     const double rt = pair_uniform(seed, j, 0) * r_max;
     const double th = pair_uniform(seed, j, 1) * 2.0 * SPH_PI;
     const double ph = acos(2.0 * pair_uniform(seed, j, 2) - 1.0);
@@ -124,8 +124,8 @@ int launch_inject_pairs(sph_ctx *ctx, int npairs, unsigned long long seed, int c
         k_h_of_id<<<div_up(max(n0, 1), 256), 256, 0, s>>>(n0, ctx->id[c], ctx->st[c][ST_H], h_id,
                                                           hbuf);
     CK(cudaMemcpyAsync(ctx->st_table, ctx->st[c], sizeof(double *) * ST_N, cudaMemcpyHostToDevice, s));
-    k_inject_pairs<<<div_up(npairs, 128), 128, 0, s>>>(npairs, 0, seed, n0, n0, cloud, r_max, v_in,
-                                                       m, u, hbuf, ctx->st_table, ctx->id[c],
+    k_inject_pairs<<<div_up(npairs, 128), 128, 0, s>>>(npairs, seed, n0, n0, cloud, r_max, v_in, m,
+                                                       u, hbuf, ctx->st_table, ctx->id[c],
                                                        ctx->cloud[c], ctx->dudt);
     // relayout of a_sph and a_grav through the scratch buffer (2 N doubles)
     double *tmp = ctx->red + 8;
