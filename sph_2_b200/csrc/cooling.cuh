@@ -168,7 +168,10 @@ __device__ __forceinline__ bool cool_accept(const CoolDev &c, double rho, double
 // the FP64 polish as slow as the exact bisection it should replace).  The
 // residual u - u_old - ratefact * net * dt is formed in FP32 from FP32 u and
 // u_old: its rounding (~1e-7 u) is four orders below the tolerance.  The
-// exact solver and the fallback stay in FP64.
+// products are ordered so that no intermediate leaves the FP32 range:
+// ratefact = nH^2 / rho reaches 1e29 and ratefact * dt 1e42, but ratefact *
+// Lambda stays below 1e10 and its product with dt below 1e25.  The exact
+// solver and the fallback stay in FP64.
 __device__ __forceinline__ float cool_lambda_f(const CoolDev &c, float T, float *slope) {
     const float lt = __log10f(T);
     const float lT0 = (float)c.logT0;
@@ -193,8 +196,8 @@ __device__ __forceinline__ void cool_newton_polish_f(const CoolDev &c, double rh
     for (int it = 0; it < 5; it++) {
         float s;
         const float lam = cool_lambda_f(c, kT * uu, &s);
-        const float r = uu - uo - ratefact * (gn - lam) * fdt;
-        const float rp = 1.f + ratefact * fdt * s * lam / uu;
+        const float r = uu - uo - (ratefact * (gn - lam)) * fdt;
+        const float rp = 1.f + (ratefact * lam) * fdt * s / uu;
         if (!(rp > 0.f) || !(uu > 0.f)) break;  // the estimate is void here
         const float e = fabsf(r / rp) / uu;
         *u = (double)uu;
@@ -208,7 +211,9 @@ __device__ __forceinline__ void cool_newton_polish_f(const CoolDev &c, double rh
 
 __device__ __forceinline__ bool cool_monotone_f(const CoolDev &c, double rho, double dt, double u_lo,
                                                 double u_hi) {
-    const float A = (float)((c.XH * rho / MH_CGS) * (c.XH * rho / MH_CGS) / rho * dt);
+    // A = ratefact * dt can pass the FP32 range: it is applied in FP64 to
+    // the Lambda / T values (two multiplies, no transcendental)
+    const double A = (c.XH * rho / MH_CGS) * (c.XH * rho / MH_CGS) / rho * dt;
     const float kT = (float)((c.gamma - 1.0) * c.mu * MH_CGS / KB_CGS);
     const float lT0 = (float)c.logT0;
     const float dl = (float)((c.logT1 - c.logT0) / c.nb);
@@ -220,14 +225,14 @@ __device__ __forceinline__ bool cool_monotone_f(const CoolDev &c, double rho, do
     float s = (float)(c.logL[k + 1] - c.logL[k]) / dl;
     if (s < 0.f) {
         const float lam = __exp10f((float)c.logL[k] + s * (l0 - (lT0 + k * dl)));
-        if (!(1.f + A * s * lam * kT / T0 > 0.f)) return false;
+        if (!(1.0 + A * (double)(s * (lam / T0) * kT) > 0.0)) return false;
     }
     int kend = (int)floorf((l1 - lT0) / dl);
     kend = kend > c.nb - 1 ? c.nb - 1 : kend;
     for (int e = k + 1; e <= kend; e++) {
         s = (float)(c.logL[e + 1] - c.logL[e]) / dl;
         if (s < 0.f) {
-            if (!(1.f + A * s * (float)c.lamT[e] * kT > 0.f)) return false;
+            if (!(1.0 + A * (double)s * c.lamT[e] * (double)kT > 0.0)) return false;
         }
     }
     return true;

@@ -27,13 +27,6 @@
 namespace {
 
 constexpr int SEARCH_WARPS = 4;
-#ifndef SPH_H_PACKED_TERMS
-#define SPH_H_PACKED_TERMS 0
-#endif
-#ifndef SPH_H_UNROLL
-#define SPH_H_UNROLL 4
-#endif
-constexpr int H_UNROLL = SPH_H_UNROLL;
 constexpr int SSTK = 512;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -200,15 +193,8 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         }
         __syncwarp();
         unsigned hit = 0, sure = 0;
-#if SPH_H_PACKED_TERMS
-        // FP32 h iteration: the kernel terms of the certain candidates summed
-        // in the prefilter itself, branch-free and two at a time; the hit loop
-        // below then only writes their row entries
-        float2 ps = bc2(0.f), pd = bc2(0.f);
-        const float2 ihf = bc2(FAST ? (float)hs->inv_h : 0.f);
-#endif
         if (act) {
-#pragma unroll H_UNROLL
+#pragma unroll 4
             for (int k = 0; k < m; k += 2) {
                 const float2 dx = __ffma2_rn(ldf2(&S.fx[k]), m1, pfx);
                 const float2 dy = __ffma2_rn(ldf2(&S.fy[k]), m1, pfy);
@@ -222,38 +208,12 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                 hit |= (r2.x <= lim.x ? 1u : 0u) << k;
                 hit |= (r2.y <= lim.y ? 2u : 0u) << k;
                 if (FAST) {
-                    const bool sx = r2.x <= ri2lo.x, sy = r2.y <= ri2lo.y;
-                    sure |= (sx ? 1u : 0u) << k;
-                    sure |= (sy ? 2u : 0u) << k;
-#if SPH_H_PACKED_TERMS
-                    const float2 rr = make_float2(r2.x > 0.f ? r2.x * rsqrtf(r2.x) : 0.f,
-                                                  r2.y > 0.f ? r2.y * rsqrtf(r2.y) : 0.f);
-                    const float2 q = __fmul2_rn(rr, ihf);
-                    const float2 q2 = __fmul2_rn(q, q), q3 = __fmul2_rn(q2, q);
-                    const float2 w1 = __ffma2_rn(q3, bc2(0.75f), __ffma2_rn(q2, bc2(-1.5f), bc2(1.f)));
-                    const float2 d1 = __ffma2_rn(q3, bc2(4.5f), __ffma2_rn(q2, bc2(-7.5f), bc2(3.f)));
-                    const float2 t = __ffma2_rn(q, m1, bc2(2.f));
-                    const float2 t2 = __fmul2_rn(t, t);
-                    const float2 w2 = __fmul2_rn(__fmul2_rn(t2, t), bc2(0.25f));
-                    const float2 d2 = __fmul2_rn(__fmul2_rn(t2, bc2(1.5f)), __ffma2_rn(q, m1, bc2(1.f)));
-                    const float2 mk = ldf2(&S.fh[k]);
-                    const float wx = (sx && q.x < 2.f) ? (q.x <= 1.f ? w1.x : w2.x) : 0.f;
-                    const float wy = (sy && q.y < 2.f) ? (q.y <= 1.f ? w1.y : w2.y) : 0.f;
-                    const float dxw = (sx && q.x < 2.f) ? (q.x <= 1.f ? d1.x : d2.x) : 0.f;
-                    const float dyw = (sy && q.y < 2.f) ? (q.y <= 1.f ? d1.y : d2.y) : 0.f;
-                    ps = __ffma2_rn(mk, make_float2(wx, wy), ps);
-                    pd = __ffma2_rn(mk, make_float2(dxw, dyw), pd);
-#endif
+                    sure |= (r2.x <= ri2lo.x ? 1u : 0u) << k;
+                    sure |= (r2.y <= ri2lo.y ? 2u : 0u) << k;
                 }
             }
         }
         R cs = R(0), cd = R(0);
-#if SPH_H_PACKED_TERMS
-        if (FAST) {
-            cs = ps.x + ps.y;
-            cd = pd.x + pd.y;
-        }
-#endif
         while (hit) {
             const int k = __ffs(hit) - 1;
             hit &= hit - 1;
@@ -267,16 +227,11 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                     in = dx * dx + dy * dy + dz * dz <= ri2;
                 }
                 if (in) {
-#if SPH_H_PACKED_TERMS
-                    if (!((sure >> k) & 1u))  // a certain one is summed already
-#endif
-                    {
-                        const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
-                        R w, dw;
-                        if (hs->terms(qsqrt<float>(rx * rx + ry * ry + rz * rz), w, dw)) {
-                            cs += S.fh[k] * w;
-                            cd += S.fh[k] * dw;
-                        }
+                    const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
+                    R w, dw;
+                    if (hs->terms(qsqrt<float>(rx * rx + ry * ry + rz * rz), w, dw)) {
+                        cs += S.fh[k] * w;
+                        cd += S.fh[k] * dw;
                     }
                     if (count < K) A.cidx[cbase + count] = S.flat[k];
                     count++;
