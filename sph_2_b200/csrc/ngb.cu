@@ -438,7 +438,7 @@ struct NewtonArgs {
     double *h_out, *hc;
     double *hover;   // per particle: the smallest candidate radius / 2 whose row overflowed
     int *retry;
-    double n_ngb, tol, grow;
+    double n_ngb, tol, grow, regrow;
     int max_iter, last_round;
 };
 
@@ -546,7 +546,7 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
     if (need && !B.last_round) {
         // a wider search, kept below a radius whose row already overflowed
         const double ov = B.hover[i];
-        B.hc[i] = h < ov ? fmin(h * B.grow, h + 0.5 * (ov - h)) : h * B.grow;
+        B.hc[i] = h < ov ? fmin(h * B.regrow, h + 0.5 * (ov - h)) : h * B.regrow;
         B.retry[i] = 1;
     } else {
         B.retry[i] = 0;
@@ -806,12 +806,18 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
 
 }  // namespace
 
-// margin of the candidate radius over h: h may grow by this factor inside one
-// search round before the particle is searched again
+// margin of the step's first candidate radius over h: h may grow by this
+// factor inside the first search round before the particle is searched again
 #ifndef SPH_H_GROW
-#define SPH_H_GROW 1.08
+#define SPH_H_GROW 1.05
 #endif
 static const double H_GROW = SPH_H_GROW;
+// the wider margin of a repeated search (a few particles per step), so that
+// the step's four rounds follow a growth of h by 1.05 x 1.25^3 = 2.05
+static const double H_REGROW = 1.25;
+// the margin of the count and k-th iterations, whose round counts are sized
+// for it
+static const double H_GROW_COUNT = 1.08;
 
 int launch_smoothing_h(sph_ctx *ctx) {
     const int n = ctx->n;
@@ -832,6 +838,7 @@ int launch_smoothing_h(sph_ctx *ctx) {
     B.n_ngb = ctx->cfg.n_ngb;
     B.tol = ctx->cfg.h_tol;
     B.grow = H_GROW;
+    B.regrow = H_REGROW;
     B.max_iter = ctx->cfg.h_max_iter;
     const bool mixed = ctx->cfg.precision == SPH_PREC_MIXED;
     const void *kern = mixed ? (const void *)k_cand_newton<float> : (const void *)k_cand_newton<double>;
@@ -857,9 +864,9 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW, nullptr);
+                                            ctx->retry, H_GROW_COUNT, nullptr);
     k_zero_int<<<div_up(n, 256), 256, 0, s>>>(n, ctx->hiter);
-    // each round widens the radius by H_GROW; 0.3 % steps need about 26
+    // each round widens the radius by H_GROW_COUNT; 0.3 % steps need about 26
     // iterations for that, so 16 rounds cover a 3.4x change of h
     const int rounds = 16;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
@@ -873,7 +880,7 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     B.hi_n = n_target + n_tol;
     B.max_iter = max_iter;
     B.frac = frac;
-    B.grow = H_GROW;
+    B.grow = H_GROW_COUNT;
     for (int r = 0; r < rounds; r++) {
         B.last_round = r == rounds - 1;
         int g;
@@ -897,7 +904,7 @@ int launch_smoothing_kth(sph_ctx *ctx, int k) {
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW, nullptr);
+                                            ctx->retry, H_GROW_COUNT, nullptr);
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
     CountArgs B{};
@@ -905,7 +912,7 @@ int launch_smoothing_kth(sph_ctx *ctx, int k) {
     B.hc = ctx->hcand;
     B.retry = ctx->retry;
     B.iters = ctx->hiter;
-    B.grow = H_GROW;
+    B.grow = H_GROW_COUNT;
     const int rounds = 24;
     for (int r = 0; r < rounds; r++) {
         B.last_round = r == rounds - 1;
