@@ -192,8 +192,12 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             S.fh[lane] = 0.f;
         }
         __syncwarp();
-        unsigned hit = 0, sure = 0;
+        unsigned hit = 0;
         if (act) {
+            // r2 <= lim exactly when lim - r2 (rounded: the sign survives,
+            // an exact tie gives +0) has a clear sign bit; the sign bits are
+            // shifted into acc one per candidate, the newest at bit 0
+            unsigned acc = 0;
 #pragma unroll 4
             for (int k = 0; k < m; k += 2) {
                 const float2 dx = __ffma2_rn(ldf2(&S.fx[k]), m1, pfx);
@@ -205,13 +209,14 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                     const float2 sh = __fadd2_rn(hif, ldf2(&S.fh[k]));
                     lim = __fmul2_rn(__fmul2_rn(sh, sh), widen);
                 }
-                hit |= (r2.x <= lim.x ? 1u : 0u) << k;
-                hit |= (r2.y <= lim.y ? 2u : 0u) << k;
-                if (FAST) {
-                    sure |= (r2.x <= ri2lo.x ? 1u : 0u) << k;
-                    sure |= (r2.y <= ri2lo.y ? 2u : 0u) << k;
-                }
+                const float2 d = __ffma2_rn(r2, m1, lim);
+                acc = __funnelshift_l(__float_as_uint(d.x), acc, 1);
+                acc = __funnelshift_l(__float_as_uint(d.y), acc, 1);
             }
+            // candidate k's sign bit is at bit m2 - 1 - k (m2 = m rounded up
+            // to even, 2..32; the padding entry of an odd chunk never passes)
+            const int m2 = (m + 1) & ~1;
+            hit = ~(__brev(acc) >> (32 - m2)) & (0xffffffffu >> (32 - m2));
         }
         R cs = R(0), cd = R(0);
         while (hit) {
@@ -220,16 +225,19 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             double4 pj;
             if (!FAST) pj = S.stage[k];
             if (FAST) {
-                bool in = (sure >> k) & 1u;
+                // the prefilter's FP32 r^2, rounded the same way: below the
+                // narrowed threshold the candidate is inside in FP64 too
+                const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
+                const float r2s = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
+                bool in = r2s <= ri2lo.x;
                 if (!in) {
                     pj = S.stage[k];
                     const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     in = dx * dx + dy * dy + dz * dz <= ri2;
                 }
                 if (in) {
-                    const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
                     R w, dw;
-                    if (hs->terms(qsqrt<float>(rx * rx + ry * ry + rz * rz), w, dw)) {
+                    if (hs->terms(qsqrt<float>(r2s), w, dw)) {
                         cs += S.fh[k] * w;
                         cd += S.fh[k] * dw;
                     }
