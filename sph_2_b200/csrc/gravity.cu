@@ -48,10 +48,15 @@ template <class R> __device__ __forceinline__ R rsq(R x);
 template <> __device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
 template <> __device__ __forceinline__ double rsq<double>(double x) { return rsqrt(x); }
 
+// pending bucket particles: ranges of consecutive slots, range r starting at
+// slot rf[r] and at offset rs[r] of the pending stream (rs ascending; at most
+// 31 carried ranges + 32 appended by one round)
+constexpr int NRANGE = 64;
+
 template <class R> struct WalkSmem {
     int stk[WSTK];
     int clist[64];
-    int plist[96];
+    int rf[NRANGE], rs[NRANGE];
     typename R4<R>::T sa[32], sb[32], sc[32];
 };
 
@@ -60,7 +65,7 @@ template <class R> struct WalkSmem {
 struct WalkSmemF {
     int stk[WSTK];
     int clist[64];
-    int plist[96];
+    int rf[NRANGE], rs[NRANGE];
     // cells: com x y z, -mass, Qxx Qyy Qzz Qxy Qxz Qyz, trace
     __align__(8) float f[11][32];
     // far cells of the group's local expansion: their node ids, per-lane
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
                 bz1 = wmax<R>(act ? pi.z : R(-INFINITY));
         KSum<R> ax, ay, az, ph;
         long long nC = 0, nP = 0, nF = 0;
-        int sp = 1, nc = 0, np = 0, nfar = 0;
+        int sp = 1, nc = 0, np = 0, nr = 0, nfar = 0;
         bool overflow = false;
         // the super-group's node list replaces the root when it has one
         int rpos = 0, nrem = 0, sgi = -1;
@@ -426,12 +431,24 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
             __syncwarp();
           }
         };
-        auto flush_parts = [&](int m) {
+        // slot of the particle at offset t of the pending stream: the last
+        // range starting at or before t (nr <= NRANGE)
+        auto part_slot = [&](int t) {
+            int r = 0;
+#pragma unroll
+            for (int step = NRANGE / 2; step; step >>= 1) {
+                const int c = r + step;
+                if (c < nr && S.rs[c] <= t) r = c;
+            }
+            return S.rf[r] + (t - S.rs[r]);
+        };
+        // the m pending particles from stream offset h
+        auto flush_parts = [&](int m, int h) {
           if constexpr (PACKED) {
             const int m2 = (m + 1) & ~1;
             if (lane < m2) {
                 float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (lane < m) a = pw[S.plist[lane]];
+                if (lane < m) a = pw[part_slot(h + lane)];
                 S.f[0][lane] = a.x; S.f[1][lane] = a.y; S.f[2][lane] = a.z; S.f[3][lane] = -a.w;
             }
             __syncwarp();
@@ -460,7 +477,7 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
             nP += m;
             __syncwarp();
           } else {
-            if (lane < m) S.sa[lane] = pw[S.plist[lane]];
+            if (lane < m) S.sa[lane] = pw[part_slot(h + lane)];
             __syncwarp();
             R sx = 0, sy = 0, sz = 0, sp_ = 0;
 #pragma unroll 8
@@ -562,28 +579,63 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
                     nc -= 32;
                     __syncwarp();
                 }
-                while (bm) {
-                    const int src = __ffs(bm) - 1;
-                    bm &= bm - 1;
-                    const int ff = __shfl_sync(FULL, f, src), cc = __shfl_sync(FULL, cn, src);
-                    for (int b0 = 0; b0 < cc; b0 += 32)
-                        if (b0 + lane < cc) S.plist[np + b0 + lane] = ff + b0 + lane;
-                    np += cc;
+                if (bm) {
+                    // opened buckets join the pending stream in lane order:
+                    // one range per bucket at the scanned offset
+                    const int cnt = bucket ? cn : 0;
+                    int incl = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(FULL, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    if (bucket) {
+                        const int r = nr + __popc(bm & lt);
+                        S.rf[r] = f;
+                        S.rs[r] = np + incl - cnt;
+                    }
+                    nr += __popc(bm);
+                    np += __shfl_sync(FULL, incl, 31);
                     __syncwarp();
-                    while (np >= 32) {
-                        flush_parts(32);
-                        int v0 = S.plist[32 + lane], v1 = S.plist[64 + lane];
+                    if (np >= 32) {
+                        int h = 0;
+                        do {
+                            flush_parts(32, h);
+                            h += 32;
+                        } while (np - h >= 32);
+                        np -= h;
+                        // keep the ranges from the one holding offset h on,
+                        // their offsets taken from h (<= 31 of them: each
+                        // keeps at least one of the < 32 pending particles)
+                        int r0 = 0;
+                        if (np > 0) {
+#pragma unroll
+                            for (int step = NRANGE / 2; step; step >>= 1) {
+                                const int c = r0 + step;
+                                if (c < nr && S.rs[c] <= h) r0 = c;
+                            }
+                        } else {
+                            r0 = nr;
+                        }
+                        const int keep = nr - r0;
+                        int vf = 0, vs = 0;
+                        if (lane < keep) {
+                            vf = S.rf[r0 + lane];
+                            vs = S.rs[r0 + lane] - h;
+                        }
                         __syncwarp();
-                        if (lane + 32 < np) S.plist[lane] = v0;
-                        if (lane + 64 < np) S.plist[32 + lane] = v1;
-                        np -= 32;
+                        if (lane < keep) {
+                            S.rf[lane] = vf;
+                            S.rs[lane] = vs;
+                        }
+                        nr = keep;
                         __syncwarp();
                     }
                 }
             }
             if (sp == 0 && rpos >= nrem) {
                 if (nc > 0) { flush_cells(nc); nc = 0; }
-                if (np > 0) { flush_parts(np); np = 0; }
+                if (np > 0) { flush_parts(np, 0); np = 0; nr = 0; }
                 if (nfar > 0) { flush_far(nfar); nfar = 0; }
             }
         }
