@@ -29,10 +29,15 @@ namespace {
 constexpr int SEARCH_WARPS = 4;
 constexpr int SSTK = 512;
 constexpr unsigned FULL = 0xffffffffu;
+// pending bucket particles: ranges of consecutive slots, range r starting at
+// slot rf[r] and at offset rs[r] of the pending stream (rs ascending; at most
+// 31 carried ranges + 32 appended by one round)
+constexpr int NRANGE = 64;
 
 struct SearchSmem {
     int stk[SSTK];
-    int flat[96];
+    int flat[32];  // slots of the chunk being processed
+    int rf[NRANGE], rs[NRANGE];
     double4 stage[32];
     double smass[32];
     // FP32 copies of the staged positions relative to the group's centre and
@@ -145,7 +150,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const size_t cbase = MODE != 1 ? (size_t)i * K : 0;
     int count = 0;
     double hnb = 0.0;
-    int sp = 1, nflat = 0;
+    int sp = 1, nflat = 0, nr = 0;
     bool overflow = false;
     if (lane == 0) S.stk[0] = A.croot[A.gcloud[g]];
     __syncwarp();
@@ -175,9 +180,22 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const float2 ri2lo = bc2((float)ri2 * (1.f - mrg));
     const float2 m1 = bc2(-1.f), widen = bc2(1.f + mrg);
 
-    auto process = [&](int m) {
+    // slot of the particle at offset t of the pending stream: the last range
+    // starting at or before t
+    auto part_slot = [&](int t) {
+        int r = 0;
+#pragma unroll
+        for (int step = NRANGE / 2; step; step >>= 1) {
+            const int c = r + step;
+            if (c < nr && S.rs[c] <= t) r = c;
+        }
+        return S.rf[r] + (t - S.rs[r]);
+    };
+    // the m pending candidates from stream offset h
+    auto process = [&](int m, int h) {
         if (lane < m) {
-            const int j = S.flat[lane];
+            const int j = part_slot(h + lane);
+            S.flat[lane] = j;
             const double4 q = A.p0[j];
             S.stage[lane] = q;
             S.fx[lane] = (float)(q.x - cx);
@@ -300,30 +318,66 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             } else {
                 overflow = true;
             }
-            unsigned lm = __ballot_sync(FULL, open && leafy);
+            const bool bucket = open && leafy;
+            const unsigned lm = __ballot_sync(FULL, bucket);
             __syncwarp();
-            while (lm) {
-                const int src = __ffs(lm) - 1;
-                lm &= lm - 1;
-                const int ff = __shfl_sync(FULL, f, src), cc = __shfl_sync(FULL, cn, src);
-                for (int b0 = 0; b0 < cc; b0 += 32)
-                    if (b0 + lane < cc) S.flat[nflat + b0 + lane] = ff + b0 + lane;
-                nflat += cc;
+            if (lm) {
+                // opened buckets join the pending stream in lane order: one
+                // range per bucket at the scanned offset
+                const int cnt = bucket ? cn : 0;
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (bucket) {
+                    const int r = nr + __popc(lm & lt);
+                    S.rf[r] = f;
+                    S.rs[r] = nflat + incl - cnt;
+                }
+                nr += __popc(lm);
+                nflat += __shfl_sync(FULL, incl, 31);
                 __syncwarp();
-                while (nflat >= 32) {
-                    process(32);
-                    int v0 = S.flat[32 + lane], v1 = S.flat[64 + lane];
+                if (nflat >= 32) {
+                    int h = 0;
+                    do {
+                        process(32, h);
+                        h += 32;
+                    } while (nflat - h >= 32);
+                    nflat -= h;
+                    // keep the ranges from the one holding offset h on, their
+                    // offsets taken from h (<= 31 of them: each keeps at
+                    // least one of the < 32 pending candidates)
+                    int r0 = nr;
+                    if (nflat > 0) {
+                        r0 = 0;
+#pragma unroll
+                        for (int step = NRANGE / 2; step; step >>= 1) {
+                            const int c = r0 + step;
+                            if (c < nr && S.rs[c] <= h) r0 = c;
+                        }
+                    }
+                    const int keep = nr - r0;
+                    int vf = 0, vs = 0;
+                    if (lane < keep) {
+                        vf = S.rf[r0 + lane];
+                        vs = S.rs[r0 + lane] - h;
+                    }
                     __syncwarp();
-                    if (lane + 32 < nflat) S.flat[lane] = v0;
-                    if (lane + 64 < nflat) S.flat[32 + lane] = v1;
-                    nflat -= 32;
+                    if (lane < keep) {
+                        S.rf[lane] = vf;
+                        S.rs[lane] = vs;
+                    }
+                    nr = keep;
                     __syncwarp();
                 }
             }
         }
         if (sp == 0 && nflat > 0) {
-            process(nflat);
+            process(nflat, 0);
             nflat = 0;
+            nr = 0;
         }
     }
     if (act) {
