@@ -41,7 +41,7 @@ struct SearchSmem {
     double4 stage[32];
     double smass[32];
     // FP32 copies of the staged positions relative to the group's centre and
-    // of their h, one array per field (two entries per 64-bit load)
+    // of their h, one array per field (four entries per 128-bit load)
     __align__(8) float fx[32];
     __align__(8) float fy[32];
     __align__(8) float fz[32];
@@ -49,6 +49,9 @@ struct SearchSmem {
 };
 
 __device__ __forceinline__ float2 ldf2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ float4 ldf4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
 
 template <class R> struct R2;
@@ -204,37 +207,53 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             if (FAST) S.fh[lane] = (float)((const V4 *)A.p1)[j].w;  // the mass
             else S.fh[lane] = (float)q.w;
             if (MODE == 0 && !FAST) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
-        } else if (lane < ((m + 1) & ~1)) {
-            // the odd tail of a chunk: an entry that never passes
+        } else if (lane < ((m + 3) & ~3)) {
+            // the tail of a chunk up to a multiple of four: entries that
+            // never pass
             S.fx[lane] = S.fy[lane] = S.fz[lane] = INFINITY;
             S.fh[lane] = 0.f;
         }
         __syncwarp();
+        const int m4 = (m + 3) & ~3;
         unsigned hit = 0;
         if (act) {
             // r2 <= lim exactly when lim - r2 (rounded: the sign survives,
             // an exact tie gives +0) has a clear sign bit; the sign bits are
             // shifted into acc one per candidate, the newest at bit 0
             unsigned acc = 0;
-#pragma unroll 4
-            for (int k = 0; k < m; k += 2) {
-                const float2 dx = __ffma2_rn(ldf2(&S.fx[k]), m1, pfx);
-                const float2 dy = __ffma2_rn(ldf2(&S.fy[k]), m1, pfy);
-                const float2 dz = __ffma2_rn(ldf2(&S.fz[k]), m1, pfz);
+            auto pair = [&](float2 qx, float2 qy, float2 qz, float2 qh) {
+                const float2 dx = __ffma2_rn(qx, m1, pfx);
+                const float2 dy = __ffma2_rn(qy, m1, pfy);
+                const float2 dz = __ffma2_rn(qz, m1, pfz);
                 const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                 float2 lim = ri2f;
                 if (MODE == 1) {
-                    const float2 sh = __fadd2_rn(hif, ldf2(&S.fh[k]));
+                    const float2 sh = __fadd2_rn(hif, qh);
                     lim = __fmul2_rn(__fmul2_rn(sh, sh), widen);
                 }
                 const float2 d = __ffma2_rn(r2, m1, lim);
                 acc = __funnelshift_l(__float_as_uint(d.x), acc, 1);
                 acc = __funnelshift_l(__float_as_uint(d.y), acc, 1);
+            };
+            if ((reinterpret_cast<uintptr_t>(S.fx) & 15u) == 0) {
+                // four candidates per 128-bit shared load
+#pragma unroll 2
+                for (int k = 0; k < m4; k += 4) {
+                    const float4 X = ldf4(&S.fx[k]), Y = ldf4(&S.fy[k]), Z = ldf4(&S.fz[k]);
+                    const float4 H = MODE == 1 ? ldf4(&S.fh[k]) : X;
+                    pair(lo2(X), lo2(Y), lo2(Z), lo2(H));
+                    pair(hi2(X), hi2(Y), hi2(Z), hi2(H));
+                }
+            } else {
+                // (a shared array placed on an 8-byte boundary only)
+#pragma unroll 4
+                for (int k = 0; k < m4; k += 2)
+                    pair(ldf2(&S.fx[k]), ldf2(&S.fy[k]), ldf2(&S.fz[k]),
+                         MODE == 1 ? ldf2(&S.fh[k]) : bc2(0.f));
             }
-            // candidate k's sign bit is at bit m2 - 1 - k (m2 = m rounded up
-            // to even, 2..32; the padding entry of an odd chunk never passes)
-            const int m2 = (m + 1) & ~1;
-            hit = ~(__brev(acc) >> (32 - m2)) & (0xffffffffu >> (32 - m2));
+            // candidate k's sign bit is at bit m4 - 1 - k (m4 = m rounded up
+            // to a multiple of four, 4..32; the padding entries never pass)
+            hit = ~(__brev(acc) >> (32 - m4)) & (0xffffffffu >> (32 - m4));
         }
         R cs = R(0), cd = R(0);
         while (hit) {
