@@ -46,6 +46,8 @@ struct SearchSmem {
     __align__(8) float fy[32];
     __align__(8) float fz[32];
     __align__(8) float fh[32];
+    // the same per candidate (x, y, z, m) for the hit loop of the h iteration
+    float4 fq[32];
 };
 
 __device__ __forceinline__ float2 ldf2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
@@ -63,19 +65,18 @@ template <> struct R2<double> { typedef double2 T; };
 template <class R> struct HSums {
     KSum<R> S, D;
     R inv_h;
-    // kernel terms at distance r: false outside the support
-    __device__ __forceinline__ bool terms(R r, R &w, R &dw) const {
+    // kernel terms at distance r, branch-free (Horner forms of both pieces,
+    // then a select; zero outside the support)
+    __device__ __forceinline__ void terms(R r, R &w, R &dw) const {
         const R q = r * inv_h;
-        if (!(q < R(2))) return false;
-        if (q <= R(1)) {
-            w = R(1) - R(1.5) * q * q + R(0.75) * q * q * q;
-            dw = R(3) - R(7.5) * q * q + R(4.5) * q * q * q;
-        } else {
-            const R t = R(2) - q;
-            w = R(0.25) * t * t * t;
-            dw = R(1.5) * t * t * (R(1) - q);
-        }
-        return true;
+        const R q2 = q * q, t = R(2) - q;
+        const R t2 = t * t;
+        const R w_in = fma(q2, fma(R(0.75), q, R(-1.5)), R(1));
+        const R dw_in = fma(q2, fma(R(4.5), q, R(-7.5)), R(3));
+        const R w_out = R(0.25) * t2 * t, dw_out = R(1.5) * t2 * (R(1) - q);
+        const bool inner = q <= R(1), inside = q < R(2);
+        w = inside ? (inner ? w_in : w_out) : R(0);
+        dw = inside ? (inner ? dw_in : dw_out) : R(0);
     }
     __device__ __forceinline__ void add(R r, R m) {
         const R q = r * inv_h;
@@ -201,11 +202,17 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             S.flat[lane] = j;
             const double4 q = A.p0[j];
             S.stage[lane] = q;
-            S.fx[lane] = (float)(q.x - cx);
-            S.fy[lane] = (float)(q.y - cy);
-            S.fz[lane] = (float)(q.z - cz);
-            if (FAST) S.fh[lane] = (float)((const V4 *)A.p1)[j].w;  // the mass
-            else S.fh[lane] = (float)q.w;
+            const float qx = (float)(q.x - cx), qy = (float)(q.y - cy), qz = (float)(q.z - cz);
+            S.fx[lane] = qx;
+            S.fy[lane] = qy;
+            S.fz[lane] = qz;
+            if (FAST) {
+                const float mj = (float)((const V4 *)A.p1)[j].w;
+                S.fh[lane] = mj;
+                S.fq[lane] = make_float4(qx, qy, qz, mj);
+            } else {
+                S.fh[lane] = (float)q.w;
+            }
             if (MODE == 0 && !FAST) S.smass[lane] = (double)((const V4 *)A.p1)[j].w;
         } else if (lane < ((m + 3) & ~3)) {
             // the tail of a chunk up to a multiple of four: entries that
@@ -264,7 +271,8 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             if (FAST) {
                 // the prefilter's FP32 r^2, rounded the same way: below the
                 // narrowed threshold the candidate is inside in FP64 too
-                const float rx = pfx.x - S.fx[k], ry = pfy.x - S.fy[k], rz = pfz.x - S.fz[k];
+                const float4 cj = S.fq[k];
+                const float rx = pfx.x - cj.x, ry = pfy.x - cj.y, rz = pfz.x - cj.z;
                 const float r2s = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
                 bool in = r2s <= ri2lo.x;
                 if (!in) {
@@ -274,10 +282,9 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                 }
                 if (in) {
                     R w, dw;
-                    if (hs->terms(qsqrt<float>(r2s), w, dw)) {
-                        cs += S.fh[k] * w;
-                        cd += S.fh[k] * dw;
-                    }
+                    hs->terms(qsqrt<float>(r2s), w, dw);
+                    cs = fmaf(cj.w, w, cs);
+                    cd = fmaf(cj.w, dw, cd);
                     if (count < K) A.cidx[cbase + count] = S.flat[k];
                     count++;
                 }
