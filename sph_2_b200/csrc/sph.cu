@@ -14,7 +14,20 @@
 // spatially local in Morton order so the gathers mostly hit L1/L2.  Partial
 // sums are Kahan-compensated in FP32 (mixed) and reduced across the lanes in
 // FP64.  Coordinate differences are always taken in FP64.
+#include <type_traits>
+
 #include "sph_internal.cuh"
+
+// resident 256-thread blocks per SM asked of the FP32 list + density and
+// force passes (register budget: 65536 / (256 x this)).  The force pass is
+// gather-latency bound: 48 registers (5) run it 3 % faster than 58, 40 (6)
+// spill; the list pass spills at 48
+#ifndef SPH_LISTS_MINB
+#define SPH_LISTS_MINB 1
+#endif
+#ifndef SPH_FORCE_MINB
+#define SPH_FORCE_MINB 5
+#endif
 
 namespace {
 
@@ -193,7 +206,7 @@ __global__ void __launch_bounds__(256)
 // from that list; a row that is not a complete candidate set (overflow, or h
 // above the candidate radius) marks every particle.
 template <class R, int LANES>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, std::is_same<R, float>::value ? SPH_LISTS_MINB : 1)
     k_cand_density_divcurl(int n, const double4 *__restrict__ p0,
                            const typename R4<R>::T *__restrict__ p1,
                            typename R4<R>::T *__restrict__ p2, const int *__restrict__ crows,
@@ -309,7 +322,7 @@ __global__ void __launch_bounds__(256)
 // du_i  =  sum m_j (P_i/rho_i^2 + PI_ij/2) v_ij . gradW_ij,
 // vsig_i = max_j (c_i + c_j - 3 w_ij), w_ij = v_ij.r_ij/(r_ij + 1e-5).
 template <class R, int LANES>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, std::is_same<R, float>::value ? SPH_FORCE_MINB : 1)
     k_force(int n, const double4 *__restrict__ p0, const typename R4<R>::T *__restrict__ p1,
             const typename R4<R>::T *__restrict__ p2, const int *__restrict__ rows,
             const int *__restrict__ cnt, int K, int av_mode, int balsara, R alpha, R beta, R eta,
