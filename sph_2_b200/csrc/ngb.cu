@@ -263,32 +263,52 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             hit = ~(__brev(acc) >> (32 - m4)) & (0xffffffffu >> (32 - m4));
         }
         R cs = R(0), cd = R(0);
-        while (hit) {
-            const int k = __ffs(hit) - 1;
-            hit &= hit - 1;
-            double4 pj;
-            if (!FAST) pj = S.stage[k];
-            if (FAST) {
+        if (FAST) {
+            // two hits per trip (independent chains for the scheduler), the
+            // sums and the row entries in the same order as one per trip
+            auto exact_in = [&](int k) {
+                const double4 pj = S.stage[k];
+                const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                return dx * dx + dy * dy + dz * dz <= ri2;
+            };
+            while (hit) {
+                const int k1 = __ffs(hit) - 1;
+                hit &= hit - 1;
+                const bool two = hit != 0;
+                const int k2 = two ? __ffs(hit) - 1 : k1;
+                hit &= hit - 1;
                 // the prefilter's FP32 r^2, rounded the same way: below the
                 // narrowed threshold the candidate is inside in FP64 too
-                const float4 cj = S.fq[k];
-                const float rx = pfx.x - cj.x, ry = pfy.x - cj.y, rz = pfz.x - cj.z;
-                const float r2s = fmaf(rz, rz, fmaf(ry, ry, rx * rx));
-                bool in = r2s <= ri2lo.x;
-                if (!in) {
-                    pj = S.stage[k];
-                    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    in = dx * dx + dy * dy + dz * dz <= ri2;
-                }
-                if (in) {
-                    R w, dw;
-                    hs->terms(qsqrt<float>(r2s), w, dw);
-                    cs = fmaf(cj.w, w, cs);
-                    cd = fmaf(cj.w, dw, cd);
-                    if (count < K) A.cidx[cbase + count] = S.flat[k];
+                const float4 c1 = S.fq[k1], c2 = S.fq[k2];
+                const float ax = pfx.x - c1.x, ay = pfy.x - c1.y, az = pfz.x - c1.z;
+                const float bx = pfx.x - c2.x, by = pfy.x - c2.y, bz = pfz.x - c2.z;
+                const float r2a = fmaf(az, az, fmaf(ay, ay, ax * ax));
+                const float r2b = fmaf(bz, bz, fmaf(by, by, bx * bx));
+                bool in1 = r2a <= ri2lo.x, in2 = two && r2b <= ri2lo.x;
+                if (!in1) in1 = exact_in(k1);
+                if (two && !in2) in2 = exact_in(k2);
+                R w1, dw1, w2, dw2;
+                hs->terms(qsqrt<float>(r2a), w1, dw1);
+                hs->terms(qsqrt<float>(r2b), w2, dw2);
+                if (in1) {
+                    cs = fmaf(c1.w, w1, cs);
+                    cd = fmaf(c1.w, dw1, cd);
+                    if (count < K) A.cidx[cbase + count] = S.flat[k1];
                     count++;
                 }
-            } else if (MODE != 1) {
+                if (in2) {
+                    cs = fmaf(c2.w, w2, cs);
+                    cd = fmaf(c2.w, dw2, cd);
+                    if (count < K) A.cidx[cbase + count] = S.flat[k2];
+                    count++;
+                }
+            }
+        }
+        while (!FAST && hit) {
+            const int k = __ffs(hit) - 1;
+            hit &= hit - 1;
+            const double4 pj = S.stage[k];
+            if (MODE != 1) {
                 const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                 if (dx * dx + dy * dy + dz * dz <= ri2) {
                     // the first Newton evaluation (at h = pi.w) rides on the
