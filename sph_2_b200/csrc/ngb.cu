@@ -116,7 +116,7 @@ struct SearchArgs {
     const int *gstart, *gcount, *gcloud, *croot;
     double4 *p0;
     const double4 *sA, *sB;  // node box min (+h_max), box max
-    const int *first, *last, *child;
+    const int4 *wL;  // per node: first particle, count, left and right child
     int leaf_size, K;
     int *rows, *cnt;
     int *ngb_cnt;  // list counts written by k_lists_cand (cnt holds candidate counts)
@@ -336,13 +336,16 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         if (sp > 0) {
             const int take = min(sp, 32);
             sp -= take;
-            int nd = 0, f = 0, cn = 0;
+            int nd = 0, f = 0, cn = 0, cl = 0, cr = 0;
             bool open = false;
             if (lane < take) {
                 nd = S.stk[sp + lane];
                 const double4 a = A.sA[nd], b = A.sB[nd];
-                f = A.first[nd];
-                cn = A.last[nd] - f + 1;
+                const int4 L = A.wL[nd];
+                f = L.x;
+                cn = L.y;
+                cl = L.z;
+                cr = L.w;
                 double ex = fmax(fmax(a.x - gx1, gx0 - b.x), 0.0);
                 double ey = fmax(fmax(a.y - gy1, gy0 - b.y), 0.0);
                 double ez = fmax(fmax(a.z - gz1, gz0 - b.z), 0.0);
@@ -357,8 +360,8 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             if (sp + npush <= SSTK) {
                 if (open && !leafy) {
                     int pos = sp + 2 * __popc(pm & lt);
-                    S.stk[pos] = A.child[2 * nd + 1];
-                    S.stk[pos + 1] = A.child[2 * nd];
+                    S.stk[pos] = cr;
+                    S.stk[pos + 1] = cl;
                 }
                 sp += npush;
             } else {
@@ -895,9 +898,7 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.p0 = ctx->p0;
     A.sA = (const double4 *)ctx->node_box;
     A.sB = A.sA + 2 * (size_t)ctx->cfg.n_max;
-    A.first = ctx->first;
-    A.last = ctx->last;
-    A.child = ctx->child;
+    A.wL = ctx->wL;
     A.leaf_size = ctx->cfg.leaf_size;
     A.K = ctx->cfg.max_ngb;
     A.rows = rows;
