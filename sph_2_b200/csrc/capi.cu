@@ -333,7 +333,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->child, 2 * NN); DAF(ctx->parent, NN); DAF(ctx->first, NN); DAF(ctx->last, NN);
     DAF(ctx->flag, NN);
     DAF(ctx->node, 16 * NN); DAF(ctx->hmax, NN); DAF(ctx->ropen2, NN);
-    double4 *nb4;
+    float4 *nb4;
     DAF(nb4, 2 * NN); ctx->node_box = nb4;
     DAF(tmpb, rs * NN); ctx->wA = tmpb;
     DAF(tmpb, rs * NN); ctx->wB = tmpb;

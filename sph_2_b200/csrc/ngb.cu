@@ -115,7 +115,9 @@ __device__ __forceinline__ double wmax(double v) {
 struct SearchArgs {
     const int *gstart, *gcount, *gcloud, *croot;
     double4 *p0;
-    const double4 *sA, *sB;  // node box min (+h_max), box max
+    // node boxes in FP32 rounded outward: (min rounded down, h_max rounded
+    // up), (max rounded up, 0)
+    const float4 *sA, *sB;
     const int4 *wL;  // per node: first particle, count, left and right child
     int leaf_size, K;
     int *rows, *cnt;
@@ -150,6 +152,14 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     const double rmax = wmax(act ? ri : 0.0);
     const double ri2 = ri * ri;
     const int K = A.K;
+    // the traversal's box test in FP32 with directed rounding: the group box
+    // rounded outward, the gap between the boxes rounded down and the reach
+    // rounded up, so a node is opened whenever the FP64 test would open it
+    const float fgx0 = __double2float_rd(gx0), fgy0 = __double2float_rd(gy0),
+                fgz0 = __double2float_rd(gz0);
+    const float fgx1 = __double2float_ru(gx1), fgy1 = __double2float_ru(gy1),
+                fgz1 = __double2float_ru(gz1);
+    const float frmax = fmaxf(__double2float_ru(rmax), 1e-18f);
     // candidate row of particle i: entries [i K, i K + K)
     const size_t cbase = MODE != 1 ? (size_t)i * K : 0;
     int count = 0;
@@ -340,18 +350,18 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             bool open = false;
             if (lane < take) {
                 nd = S.stk[sp + lane];
-                const double4 a = A.sA[nd], b = A.sB[nd];
+                const float4 a = A.sA[nd], b = A.sB[nd];
                 const int4 L = A.wL[nd];
                 f = L.x;
                 cn = L.y;
                 cl = L.z;
                 cr = L.w;
-                double ex = fmax(fmax(a.x - gx1, gx0 - b.x), 0.0);
-                double ey = fmax(fmax(a.y - gy1, gy0 - b.y), 0.0);
-                double ez = fmax(fmax(a.z - gz1, gz0 - b.z), 0.0);
-                double d2 = ex * ex + ey * ey + ez * ez;
-                double reach = MODE != 1 ? rmax : (a.w + rmax);
-                open = d2 <= reach * reach * (1.0 + 1e-12);
+                const float ex = fmaxf(fmaxf(__fsub_rd(a.x, fgx1), __fsub_rd(fgx0, b.x)), 0.f);
+                const float ey = fmaxf(fmaxf(__fsub_rd(a.y, fgy1), __fsub_rd(fgy0, b.y)), 0.f);
+                const float ez = fmaxf(fmaxf(__fsub_rd(a.z, fgz1), __fsub_rd(fgz0, b.z)), 0.f);
+                const float d2 = __fmaf_rd(ez, ez, __fmaf_rd(ey, ey, __fmul_rd(ex, ex)));
+                const float reach = MODE != 1 ? frmax : __fadd_ru(a.w, frmax);
+                open = d2 <= __fmul_ru(__fmul_ru(reach, reach), 1.000001f);
             }
             __syncwarp();
             const bool leafy = cn <= A.leaf_size;
@@ -896,7 +906,7 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.gcloud = ctx->groot_g;
     A.croot = ctx->croot;
     A.p0 = ctx->p0;
-    A.sA = (const double4 *)ctx->node_box;
+    A.sA = (const float4 *)ctx->node_box;
     A.sB = A.sA + 2 * (size_t)ctx->cfg.n_max;
     A.wL = ctx->wL;
     A.leaf_size = ctx->cfg.leaf_size;

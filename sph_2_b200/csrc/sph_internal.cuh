@@ -84,7 +84,7 @@ struct sph_ctx {
     // tree
     int *child = nullptr, *parent = nullptr, *first = nullptr, *last = nullptr, *flag = nullptr;
     double *node = nullptr, *hmax = nullptr, *ropen2 = nullptr;
-    void *node_box = nullptr;  // double4 [2][2*n_max]: (box min, h_max), (box max, 0)
+    void *node_box = nullptr;  // float4 [2][2*n_max], rounded outward: (box min, h_max), (box max, 0)
     // Real4 walk records per node: wA (com, r_open^2), wB (Qxx, Qyy, Qzz, M),
     // wC (Qxy, Qxz, Qyz, trace); wL (first, count, left, right child)
     void *wA = nullptr, *wB = nullptr, *wC = nullptr;

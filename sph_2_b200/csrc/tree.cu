@@ -95,11 +95,20 @@ __device__ __forceinline__ double open_r2(const double *o, double theta) {
     return xmul(r, r);
 }
 
+// search-box records in FP32, rounded outward: (min down, h_max up), (max up)
+__device__ __forceinline__ float4 box_lo(double x, double y, double z, double hm) {
+    return make_float4(__double2float_rd(x), __double2float_rd(y), __double2float_rd(z),
+                       __double2float_ru(hm));
+}
+__device__ __forceinline__ float4 box_hi(double x, double y, double z) {
+    return make_float4(__double2float_ru(x), __double2float_ru(y), __double2float_ru(z), 0.f);
+}
+
 template <class R>
 __global__ void k_leaves(int n, const double *__restrict__ x, const double *__restrict__ y,
                          const double *__restrict__ z, const double *__restrict__ h,
                          double *__restrict__ hmax, double *__restrict__ ropen2,
-                         double4 *__restrict__ sA, double4 *__restrict__ sB, int *__restrict__ flag,
+                         float4 *__restrict__ sA, float4 *__restrict__ sB, int *__restrict__ flag,
                          int *__restrict__ first, int *__restrict__ last, int *__restrict__ child,
                          typename R4<R>::T *wA, int4 *__restrict__ wL) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -111,8 +120,8 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
     const double xp = x[p], yp = y[p], zp = z[p];
     hmax[nd] = h[p];
     ropen2[nd] = 0.0;
-    sA[nd] = make_double4(xp, yp, zp, h[p]);
-    sB[nd] = make_double4(xp, yp, zp, 0.0);
+    sA[nd] = box_lo(xp, yp, zp, h[p]);
+    sB[nd] = box_hi(xp, yp, zp);
     first[nd] = p;
     last[nd] = p;
     child[2 * nd] = -1;
@@ -182,15 +191,15 @@ struct Opening {
 template <class R>
 __device__ __forceinline__ void store_node(int nd, const double *o, double hm, double theta,
                                            double *node, double *hmax, double *ropen2,
-                                           double4 *sA, double4 *sB, typename R4<R>::T *wA,
+                                           float4 *sA, float4 *sB, typename R4<R>::T *wA,
                                            typename R4<R>::T *wB, typename R4<R>::T *wC) {
     const double r2 = open_r2(o, theta);
     double *dst = node + (size_t)16 * nd;
     for (int q = 0; q < 16; q++) dst[q] = o[q];
     hmax[nd] = hm;
     ropen2[nd] = r2;
-    sA[nd] = make_double4(o[10], o[11], o[12], hm);
-    sB[nd] = make_double4(o[13], o[14], o[15], 0.0);
+    sA[nd] = box_lo(o[10], o[11], o[12], hm);
+    sB[nd] = box_hi(o[13], o[14], o[15]);
     write_walk<R>(nd, o, r2, hm, wA, wB, wC);
 }
 
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
                const double *__restrict__ x, const double *__restrict__ y,
                const double *__restrict__ z, const double *__restrict__ m,
                const double *__restrict__ h, double *node, double *hmax, double *ropen2,
-               double4 *sA, double4 *sB, Opening op, typename R4<R>::T *wA,
+               float4 *sA, float4 *sB, Opening op, typename R4<R>::T *wA,
                typename R4<R>::T *wB, typename R4<R>::T *wC) {
     __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
         pm[GUP_WARPS][32], ph[GUP_WARPS][32];
@@ -274,7 +283,7 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
                             const int *__restrict__ child, const double *__restrict__ x,
                             const double *__restrict__ y, const double *__restrict__ z,
                             const double *__restrict__ m, double *node, double *hmax,
-                            double *ropen2, double4 *sA, double4 *sB, int *flag, Opening op,
+                            double *ropen2, float4 *sA, float4 *sB, int *flag, Opening op,
                             const int4 *__restrict__ wL, typename R4<R>::T *wA,
                             typename R4<R>::T *wB, typename R4<R>::T *wC) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -316,7 +325,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
     k_refit_groups(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
                    const int *__restrict__ gcount, const int *__restrict__ gnode,
                    const int *__restrict__ first, const int *__restrict__ last,
-                   const double *__restrict__ h, double *hmax, double4 *sA,
+                   const double *__restrict__ h, double *hmax, float4 *sA,
                    const int *__restrict__ need) {
     __shared__ double sh[GUP_WARPS][32];
     if (need && !*need) return;
@@ -328,7 +337,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             const double hp = h[s0 + lane];
             sh[w][lane] = hp;
             hmax[n - 1 + s0 + lane] = hp;
-            sA[n - 1 + s0 + lane].w = hp;
+            sA[n - 1 + s0 + lane].w = __double2float_ru(hp);
         }
         __syncwarp();
         if (c >= 2 && lane < c - 1) {
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             double hm = sh[w][f];
             for (int k = f + 1; k <= l; k++) hm = fmax(hm, sh[w][k]);
             hmax[nd] = hm;
-            sA[nd].w = hm;
+            sA[nd].w = __double2float_ru(hm);
         }
         __syncwarp();
     }
@@ -347,7 +356,7 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
 // second arrival combines and clears the counter for the next pass
 __global__ void k_refit_up(int n, const int *__restrict__ ngroup_p, const int *__restrict__ gnode,
                            const int *__restrict__ parent, const int *__restrict__ child,
-                           double *hmax, double4 *sA, int *flag, const int *__restrict__ need) {
+                           double *hmax, float4 *sA, int *flag, const int *__restrict__ need) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= *ngroup_p || n < 2 || (need && !*need)) return;
     int nd = parent[gnode[g]];
@@ -357,7 +366,7 @@ __global__ void k_refit_up(int n, const int *__restrict__ ngroup_p, const int *_
         arrived.store(0, cuda::memory_order_relaxed);
         double hm = fmax(__ldcg(hmax + child[2 * nd]), __ldcg(hmax + child[2 * nd + 1]));
         hmax[nd] = hm;
-        sA[nd].w = hm;
+        sA[nd].w = __double2float_ru(hm);
         nd = parent[nd];
     }
 }
@@ -381,8 +390,8 @@ int launch_tree(sph_ctx *ctx) {
     CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
     // leaf records (they complete the leaves' first / last the groups read),
     // the groups, the nodes inside the groups, then the climb above them
-    double4 *boxA = (double4 *)ctx->node_box;
-    double4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
+    float4 *boxA = (float4 *)ctx->node_box;
+    float4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
     const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
     const Opening op{ctx->cfg.theta, ctx->cfg.theta_small, ctx->cfg.small_cell};
     int rc;
@@ -435,7 +444,7 @@ int launch_refit_hmax(sph_ctx *ctx, const int *need) {
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
-    double4 *boxA = (double4 *)ctx->node_box;
+    float4 *boxA = (float4 *)ctx->node_box;
     const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
     k_refit_groups<<<ggrid, GUP_WARPS * 32, 0, s>>>(n, ctx->d_ngroup, ctx->gstart, ctx->gcount,
                                                     ctx->gnode, ctx->first, ctx->last,
