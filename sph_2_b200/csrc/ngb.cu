@@ -65,18 +65,17 @@ template <> struct R2<double> { typedef double2 T; };
 template <class R> struct HSums {
     KSum<R> S, D;
     R inv_h;
-    // kernel terms at distance r, branch-free (Horner forms of both pieces,
-    // then a select; zero outside the support)
+    // kernel terms at distance r, branch-free in the B-spline form of the
+    // two pieces: with a = (2 - q)+ and b = (1 - q)+,
+    //   w  = a^3 / 4 - b^3                    (1 - 1.5 q^2 + 0.75 q^3 up to q = 1)
+    //   dw = 1.5 a^2 (1 - q) - 3 b^2 (1 - 2q)  (3 - 7.5 q^2 + 4.5 q^3 up to q = 1)
+    // both zero from q = 2 on
     __device__ __forceinline__ void terms(R r, R &w, R &dw) const {
         const R q = r * inv_h;
-        const R q2 = q * q, t = R(2) - q;
-        const R t2 = t * t;
-        const R w_in = fma(q2, fma(R(0.75), q, R(-1.5)), R(1));
-        const R dw_in = fma(q2, fma(R(4.5), q, R(-7.5)), R(3));
-        const R w_out = R(0.25) * t2 * t, dw_out = R(1.5) * t2 * (R(1) - q);
-        const bool inner = q <= R(1), inside = q < R(2);
-        w = inside ? (inner ? w_in : w_out) : R(0);
-        dw = inside ? (inner ? dw_in : dw_out) : R(0);
+        const R a = fmax(R(2) - q, R(0)), b = fmax(R(1) - q, R(0));
+        const R a2 = a * a, b2 = b * b;
+        w = fma(R(0.25) * a2, a, -(b2 * b));
+        dw = fma(R(1.5) * a2, R(1) - q, R(-3) * b2 * fma(R(-2), q, R(1)));
     }
     __device__ __forceinline__ void add(R r, R m) {
         const R q = r * inv_h;
@@ -192,7 +191,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
     // Kahan sums
     constexpr bool FAST = MODE == 0 && std::is_same<R, float>::value;
     const float2 ri2lo = bc2((float)ri2 * (1.f - mrg));
-    const float2 m1 = bc2(-1.f), widen = bc2(1.f + mrg);
+    const float2 m1 = bc2(-1.f), nwiden = bc2(-(1.f + mrg)), nri2f = bc2(-ri2f.x);
 
     // slot of the particle at offset t of the pending stream: the last range
     // starting at or before t
@@ -234,21 +233,21 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
         const int m4 = (m + 3) & ~3;
         unsigned hit = 0;
         if (act) {
-            // r2 <= lim exactly when lim - r2 (rounded: the sign survives,
-            // an exact tie gives +0) has a clear sign bit; the sign bits are
-            // shifted into acc one per candidate, the newest at bit 0
+            // d = r^2 - lim accumulated from -lim: a set sign bit is a hit
+            // (within a few ulps of the widened threshold, which lies outside
+            // the true radius, a candidate may count either way); the sign
+            // bits are shifted into acc one per candidate, the newest at bit 0
             unsigned acc = 0;
             auto pair = [&](float2 qx, float2 qy, float2 qz, float2 qh) {
                 const float2 dx = __ffma2_rn(qx, m1, pfx);
                 const float2 dy = __ffma2_rn(qy, m1, pfy);
                 const float2 dz = __ffma2_rn(qz, m1, pfz);
-                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                float2 lim = ri2f;
+                float2 nlim = nri2f;
                 if (MODE == 1) {
                     const float2 sh = __fadd2_rn(hif, qh);
-                    lim = __fmul2_rn(__fmul2_rn(sh, sh), widen);
+                    nlim = __fmul2_rn(__fmul2_rn(sh, sh), nwiden);
                 }
-                const float2 d = __ffma2_rn(r2, m1, lim);
+                const float2 d = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, nlim)));
                 acc = __funnelshift_l(__float_as_uint(d.x), acc, 1);
                 acc = __funnelshift_l(__float_as_uint(d.y), acc, 1);
             };
@@ -270,7 +269,7 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
             }
             // candidate k's sign bit is at bit m4 - 1 - k (m4 = m rounded up
             // to a multiple of four, 4..32; the padding entries never pass)
-            hit = ~(__brev(acc) >> (32 - m4)) & (0xffffffffu >> (32 - m4));
+            hit = (__brev(acc) >> (32 - m4)) & (0xffffffffu >> (32 - m4));
         }
         R cs = R(0), cd = R(0);
         if (FAST) {
