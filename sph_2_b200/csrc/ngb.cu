@@ -296,9 +296,11 @@ __device__ __forceinline__ void group_search(SearchSmem &S, const SearchArgs &A,
                 bool in1 = r2a <= ri2lo.x, in2 = two && r2b <= ri2lo.x;
                 if (!in1) in1 = exact_in(k1);
                 if (two && !in2) in2 = exact_in(k2);
+                // r = r^2 rsqrt(r^2 + 1e-30): the same r for the candidates'
+                // r^2 (far above 1e-30), 0 for the particle itself
                 R w1, dw1, w2, dw2;
-                hs->terms(qsqrt<float>(r2a), w1, dw1);
-                hs->terms(qsqrt<float>(r2b), w2, dw2);
+                hs->terms(r2a * rsqrtf(r2a + 1e-30f), w1, dw1);
+                hs->terms(r2b * rsqrtf(r2b + 1e-30f), w2, dw2);
                 if (in1) {
                     cs = fmaf(c1.w, w1, cs);
                     cd = fmaf(c1.w, dw1, cd);
