@@ -126,6 +126,27 @@ def test_step_lists_with_steep_h_contrast(precision):
     check_step_state(ctx, dt, precision)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_lists_far_from_origin(precision):
+    """A sphere centred at (2e4, -3e4, 1e4): the search boxes are FP32
+    rounded outward, a few 1e-3 wide there, and the prefilter works in
+    coordinates relative to each group's centre.  The step's lists stay
+    exact and its sums match the oracle (gravity plays no part in the check:
+    the dynamics only move the particles the lists are taken on)."""
+    n, dt = 6000, 1e-4
+    d = ic.evrard(n, seed=8)
+    pos = d["pos"] + np.array([2e4, -3e4, 1e4])
+    ctx = Context(Config(n_max=n, precision=precision, dt_fixed=dt, av_mode="gadget",
+                         balsara=True))
+    ctx.load(pos, infall(d), d["m"], d["h"], d["u"])
+    ctx.prologue()
+    ctx.step(2)
+    ctx.sync()
+    st = ctx.status()
+    assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0 and st["stack_overflow"] == 0, st
+    check_step_state(ctx, dt, precision)
+
+
 def test_step_lists_and_density_at_1M():
     """N = 1,000,000 Evrard in mixed precision with the headline's walk
     settings: every list of the step is bit-exact with the oracle, rho
