@@ -567,16 +567,15 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(a.steps):
-            for f in fields:
-                ctx.set(f, pinned[f])
+            ctx.set_fields(pinned)
             ctx.step(1)
-            for f in fields:
-                ctx.get(f, out=pinned[f])
+            ctx.get_fields(fields, out=pinned)
         torch.cuda.synchronize()
         t_e2e = max_over_ranks(time.perf_counter() - t0)
         e2e = {"value": world * n * a.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": 8 * n * len(fields), "d2h_bytes_per_step": 8 * n * len(fields),
-               "api": "sph_set_field x8 (pinned host) + sph_step + sph_get_field x8 per step"}
+               "api": "sph_set_fields (8 fields from pinned host memory) + sph_step + "
+                      "sph_get_fields (the same 8 fields back) per step"}
 
     # ---- CPU baseline (rank 0, one GPU only) ----
     cpu = None

@@ -191,6 +191,13 @@ int32_t sph_count(sph_ctx *ctx);
 int32_t sph_cloud_count(sph_ctx *ctx);
 int sph_get_field(sph_ctx *ctx, int32_t field, double *out, int32_t host, int32_t storage_order);
 int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host, int32_t storage_order);
+/* nfield fields at once (fields[k] from in[k] / into out[k]): one
+ * synchronisation and one rebuild of the particle records per call instead
+ * of one per field; same arguments and order conventions as above */
+int sph_set_fields(sph_ctx *ctx, int32_t nfield, const int32_t *fields, const double *const *in,
+                   int32_t host, int32_t storage_order);
+int sph_get_fields(sph_ctx *ctx, int32_t nfield, const int32_t *fields, double *const *out,
+                   int32_t host, int32_t storage_order);
 /* original id of each stored particle (storage order) */
 int sph_get_ids(sph_ctx *ctx, int32_t *out, int32_t host);
 int sph_get_status(sph_ctx *ctx, int64_t *out /* SPH_NSTATUS */, int32_t reset);

@@ -196,6 +196,33 @@ class Context:
         self._chk(self._L.sph_set_field(self._h, L.FIELD[name], _ptr(a), 1, int(storage_order)),
                   f"set {name}")
 
+    def set_fields(self, arrays: dict, storage_order=False):
+        """Several fields in one library call ({name: array of n values})."""
+        names = list(arrays)
+        arrs = [_f64(arrays[k]) for k in names]
+        ids = np.array([L.FIELD[k] for k in names], np.int32)
+        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        self._chk(self._L.sph_set_fields(self._h, len(arrs), _ptr(ids), ptrs, 1,
+                                         int(storage_order)), "set_fields")
+
+    def get_fields(self, names, storage_order=False, out=None) -> dict:
+        """Several fields in one library call; `out`: {name: C-contiguous
+        float64 array of n values} to copy into (e.g. pinned host memory)."""
+        names = list(names)
+        res = {}
+        for k in names:
+            a = None if out is None else out.get(k)
+            if a is None:
+                a = np.zeros(self.n)
+            elif a.dtype != np.float64 or a.shape != (self.n,) or not a.flags.c_contiguous:
+                raise ValueError("out arrays must be C-contiguous float64 arrays of n values")
+            res[k] = a
+        ids = np.array([L.FIELD[k] for k in names], np.int32)
+        ptrs = (C.c_void_p * len(names))(*[res[k].ctypes.data for k in names])
+        self._chk(self._L.sph_get_fields(self._h, len(names), _ptr(ids), ptrs, 1,
+                                         int(storage_order)), "get_fields")
+        return res
+
     def get_pos(self, storage_order=False):
         return np.stack([self.get(k, storage_order) for k in "xyz"], 1)
 

@@ -566,6 +566,67 @@ int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host,
     return ctx_check_launch(ctx, "set_field");
 }
 
+// several fields in one call: the copies (and the order permutations) are
+// queued back to back on the context stream through one scratch array, the
+// particle records are rebuilt once, and the call returns after one
+// synchronisation
+int sph_set_fields(sph_ctx *ctx, int32_t nfield, const int32_t *fields, const double *const *in,
+                   int32_t host, int32_t storage_order) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (nfield < 0 || (nfield > 0 && (!fields || !in))) return SPH_ERR_ARG;
+    for (int k = 0; k < nfield; k++)
+        if (!field_ptr(ctx, fields[k]) || !in[k]) return SPH_ERR_ARG;
+    const int n = ctx->n;
+    if (n == 0 || nfield == 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    bool pack = false;
+    for (int k = 0; k < nfield; k++) {
+        const int field = fields[k];
+        double *dst = field_ptr(ctx, field);
+        if (storage_order) {
+            CK(cudaMemcpyAsync(dst, in[k], sizeof(double) * n, kind, s));
+        } else {
+            CK(cudaMemcpyAsync(ctx->red, in[k], sizeof(double) * n, kind, s));
+            k_gather_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur], ctx->red, dst);
+        }
+        if (field <= SPH_F_H) {
+            pack = true;
+            if (field <= SPH_F_Z || field == SPH_F_M) ctx->tree_ok = false;
+            ctx->cand_ok = false;
+        }
+        if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
+    }
+    if (pack && (rc = launch_pack_p1(ctx))) return rc;
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "set_fields");
+}
+
+int sph_get_fields(sph_ctx *ctx, int32_t nfield, const int32_t *fields, double *const *out,
+                   int32_t host, int32_t storage_order) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (nfield < 0 || (nfield > 0 && (!fields || !out))) return SPH_ERR_ARG;
+    for (int k = 0; k < nfield; k++)
+        if (!field_ptr(ctx, fields[k]) || !out[k]) return SPH_ERR_ARG;
+    const int n = ctx->n;
+    if (n == 0 || nfield == 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    const cudaMemcpyKind kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    for (int k = 0; k < nfield; k++) {
+        const double *from = field_ptr(ctx, fields[k]);
+        if (!storage_order) {
+            k_scatter_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur], from, ctx->red);
+            from = ctx->red;
+        }
+        CK(cudaMemcpyAsync(out[k], from, sizeof(double) * n, kind, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "get_fields");
+}
+
 int sph_get_ids(sph_ctx *ctx, int32_t *out, int32_t host) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -436,3 +436,38 @@ def test_fused_density_divcurl_matches_separate_passes(precision, tol):
     for f, v in fused.items():
         assert rel(v, ctx.get(f, True)) < tol, f
     assert rel(acc_fused, ctx.get_acc("sph", True)) < 10 * tol
+
+
+def test_batched_field_transfers_equal_per_field_calls():
+    """sph_set_fields / sph_get_fields (one synchronisation per call) leave
+    the same state and return the same arrays as one sph_set_field /
+    sph_get_field per field, and a step after either gives identical
+    results."""
+    n = 4000
+    d = shuffled_evrard(n, seed=5)
+    rng = np.random.default_rng(2)
+    new = {"x": d["pos"][:, 0] * 1.01, "y": d["pos"][:, 1], "z": d["pos"][:, 2] * 0.99,
+           "vx": rng.normal(size=n) * 0.1, "vy": rng.normal(size=n) * 0.1,
+           "vz": rng.normal(size=n) * 0.1, "u": d["u"] * 1.5, "h": d["h"] * 1.02}
+    out = []
+    for batched in (False, True):
+        ctx = make_ctx(n, "mixed", dt_fixed=1e-4)
+        ctx.load(d["pos"], d["vel"], d["m"], d["h"], d["u"])
+        ctx.prologue()
+        if batched:
+            ctx.set_fields(new)
+        else:
+            for k, a in new.items():
+                ctx.set(k, a)
+        ctx.step(1)
+        names = ["x", "vx", "u", "h", "rho", "ax_grav", "dudt"]
+        if batched:
+            got = ctx.get_fields(names)
+        else:
+            got = {k: ctx.get(k) for k in names}
+        assert np.array_equal(got["rho"], ctx.get("rho"))
+        st = ctx.get_fields(["x", "y"], storage_order=True)
+        assert np.array_equal(st["y"], ctx.get("y", storage_order=True))
+        out.append(got)
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
