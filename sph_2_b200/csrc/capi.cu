@@ -329,6 +329,7 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     ctx->sort_blocks = div_up(N, 2048);
     DAF(ctx->hist, 256 * (size_t)ctx->sort_blocks + 256);
     DAF(ctx->box, 6 * C);
+    DAF(ctx->corg, 3 * C);
     DAF(ctx->cloud_start, C + 1);
     DAF(ctx->child, 2 * NN); DAF(ctx->parent, NN); DAF(ctx->first, NN); DAF(ctx->last, NN);
     DAF(ctx->flag, NN);
@@ -373,7 +374,8 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
         cudaMemsetAsync(ctx->dt_bits, 0xff, C * sizeof(unsigned long long), ctx->stream) ||
         cudaMemsetAsync(ctx->dt, 0, C * sizeof(double), ctx->stream) ||
         cudaMemsetAsync(ctx->divV, 0, N * sizeof(double), ctx->stream) ||
-        cudaMemsetAsync(ctx->curlV, 0, N * sizeof(double), ctx->stream))
+        cudaMemsetAsync(ctx->curlV, 0, N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->corg, 0, 3 * C * sizeof(double), ctx->stream))
         return fail(SPH_ERR_CUDA);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(SPH_ERR_CUDA);
 #undef DAF

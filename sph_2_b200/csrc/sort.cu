@@ -245,6 +245,18 @@ __global__ void __launch_bounds__(SORT_THREADS)
     }
 }
 
+// origin of each cloud's FP32 walk coordinates: the centre of its box (0
+// for a cloud without a finite box)
+__global__ void k_origin(const unsigned long long *__restrict__ box, int ncloud,
+                         double *__restrict__ corg) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncloud) return;
+    for (int d = 0; d < 3; d++) {
+        const double lo = ord_to_dbl(box[6 * c + d]), hi = ord_to_dbl(box[6 * c + 3 + d]);
+        corg[3 * c + d] = lo <= hi ? 0.5 * (lo + hi) : 0.0;
+    }
+}
+
 struct PermTab {
     const double *src[ST_N];
     double *dst[ST_N];
@@ -254,7 +266,8 @@ template <class R>
 __global__ void k_permute(int n, const int *__restrict__ perm, const PermTab tab, const int *__restrict__ id_in,
                           const int *__restrict__ cl_in, int *__restrict__ id_out,
                           int *__restrict__ cl_out, double4 *__restrict__ p0,
-                          typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ pw) {
+                          typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ pw,
+                          const double *__restrict__ corg) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     int o = perm[s];
@@ -263,12 +276,17 @@ __global__ void k_permute(int n, const int *__restrict__ perm, const PermTab tab
     for (int k = 0; k < ST_N; k++) v[k] = tab.src[k][o];
 #pragma unroll
     for (int k = 0; k < ST_N; k++) tab.dst[k][s] = v[k];
+    const int cl = cl_in[o];
     id_out[s] = id_in[o];
-    cl_out[s] = cl_in[o];
+    cl_out[s] = cl;
     p0[s] = make_double4(v[ST_X], v[ST_Y], v[ST_Z], v[ST_H]);
     typename R4<R>::T a, b;
     a.x = (R)v[ST_VX]; a.y = (R)v[ST_VY]; a.z = (R)v[ST_VZ]; a.w = (R)v[ST_M];
-    b.x = (R)v[ST_X]; b.y = (R)v[ST_Y]; b.z = (R)v[ST_Z]; b.w = (R)v[ST_M];
+    const double *org = corg + 3 * cl;
+    b.x = (R)(v[ST_X] - WalkOrigin<R>::off(org, 0));
+    b.y = (R)(v[ST_Y] - WalkOrigin<R>::off(org, 1));
+    b.z = (R)(v[ST_Z] - WalkOrigin<R>::off(org, 2));
+    b.w = (R)v[ST_M];
     p1[s] = a;
     pw[s] = b;
 }
@@ -291,6 +309,7 @@ int launch_sort(sph_ctx *ctx) {
     k_box_reset<<<div_up(6 * ctx->ncloud, 256), 256, 0, s>>>(ctx->box, ctx->ncloud);
     k_box<<<div_up(n, 256), 256, 0, s>>>(st[ST_X], st[ST_Y], st[ST_Z], ctx->cloud[c], n, ctx->box,
                                          ctx->status);
+    k_origin<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->box, ctx->ncloud, ctx->corg);
     const int bits = morton_bits_for(ctx->ncloud);
     k_keys<<<div_up(n, 256), 256, 0, s>>>(st[ST_X], st[ST_Y], st[ST_Z], ctx->cloud[c], n, ctx->box,
                                           bits, ctx->key_in);
@@ -325,12 +344,13 @@ int launch_sort(sph_ctx *ctx) {
     if (ctx->cfg.precision == SPH_PREC_MIXED)
         k_permute<float><<<div_up(n, 256), 256, 0, s>>>(n, ctx->perm, tab, ctx->id[c],
                                                         ctx->cloud[c], ctx->id[d], ctx->cloud[d],
-                                                        ctx->p0, (float4 *)ctx->p1, (float4 *)ctx->pw);
+                                                        ctx->p0, (float4 *)ctx->p1, (float4 *)ctx->pw,
+                                                        ctx->corg);
     else
         k_permute<double><<<div_up(n, 256), 256, 0, s>>>(n, ctx->perm, tab, ctx->id[c],
                                                          ctx->cloud[c], ctx->id[d], ctx->cloud[d],
                                                          ctx->p0, (double4 *)ctx->p1,
-                                                         (double4 *)ctx->pw);
+                                                         (double4 *)ctx->pw, ctx->corg);
     ctx->cur = d;
     return ctx_check_launch(ctx, "sort");
 }

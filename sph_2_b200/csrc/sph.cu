@@ -417,12 +417,17 @@ __global__ void k_pack_p1(int n, const double *__restrict__ vx, const double *__
                           const double *__restrict__ x, const double *__restrict__ y,
                           const double *__restrict__ z, const double *__restrict__ h,
                           typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ pw,
-                          double4 *__restrict__ p0) {
+                          double4 *__restrict__ p0, const int *__restrict__ cloud,
+                          const double *__restrict__ corg) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     typename R4<R>::T a, b;
     a.x = (R)vx[i]; a.y = (R)vy[i]; a.z = (R)vz[i]; a.w = (R)m[i];
-    b.x = (R)x[i]; b.y = (R)y[i]; b.z = (R)z[i]; b.w = (R)m[i];
+    const double *org = corg + 3 * cloud[i];
+    b.x = (R)(x[i] - WalkOrigin<R>::off(org, 0));
+    b.y = (R)(y[i] - WalkOrigin<R>::off(org, 1));
+    b.z = (R)(z[i] - WalkOrigin<R>::off(org, 2));
+    b.w = (R)m[i];
     p1[i] = a;
     pw[i] = b;
     p0[i] = make_double4(x[i], y[i], z[i], h[i]);
@@ -582,11 +587,11 @@ int launch_pack_p1(sph_ctx *ctx) {
     if (ctx->cfg.precision == SPH_PREC_MIXED)
         k_pack_p1<float><<<div_up(n, 256), 256, 0, ctx->stream>>>(
             n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
-            (float4 *)ctx->p1, (float4 *)ctx->pw, ctx->p0);
+            (float4 *)ctx->p1, (float4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg);
     else
         k_pack_p1<double><<<div_up(n, 256), 256, 0, ctx->stream>>>(
             n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
-            (double4 *)ctx->p1, (double4 *)ctx->pw, ctx->p0);
+            (double4 *)ctx->p1, (double4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg);
     return ctx_check_launch(ctx, "pack_p1");
 }
 

@@ -79,6 +79,9 @@ struct sph_ctx {
     unsigned *hist = nullptr;    // radix histograms
     int sort_blocks = 0;
     unsigned long long *box = nullptr;  // per cloud 6 ordered-uint64 (min xyz, max xyz)
+    // per cloud: the origin of the mixed walk's FP32 coordinates (x, y, z; the
+    // centre of the cloud's box at the last sort, 0 before the first)
+    double *corg = nullptr;
     int *cloud_start = nullptr;         // device copy
 
     // tree
@@ -182,6 +185,16 @@ __device__ __forceinline__ unsigned long long dbl_to_ord(double d) {
     unsigned long long b = (unsigned long long)__double_as_longlong(d);
     return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
 }
+// FP32 walk coordinates are taken relative to the cloud's origin, so their
+// rounding scales with the cloud's size, not with its distance from 0; the
+// FP64 walk keeps absolute coordinates
+template <class R> struct WalkOrigin {
+    __device__ __forceinline__ static double off(const double *, int) { return 0.0; }
+};
+template <> struct WalkOrigin<float> {
+    __device__ __forceinline__ static double off(const double *org, int d) { return org[d]; }
+};
+
 __host__ __device__ __forceinline__ double ord_to_dbl(unsigned long long o) {
     unsigned long long b = (o & 0x8000000000000000ULL) ? (o & 0x7fffffffffffffffULL) : ~o;
 #ifdef __CUDA_ARCH__

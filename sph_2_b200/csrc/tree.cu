@@ -71,9 +71,12 @@ __global__ void k_single_roots(const int *__restrict__ cstart, int ncloud, int n
 template <class R>
 __device__ __forceinline__ void write_walk(int nd, const double *o, double r2, double hm,
                                            typename R4<R>::T *wA, typename R4<R>::T *wB,
-                                           typename R4<R>::T *wC) {
+                                           typename R4<R>::T *wC, const double *org) {
     typename R4<R>::T a, b, c;
-    a.x = (R)o[0]; a.y = (R)o[1]; a.z = (R)o[2]; a.w = (R)r2;
+    a.x = (R)(o[0] - WalkOrigin<R>::off(org, 0));
+    a.y = (R)(o[1] - WalkOrigin<R>::off(org, 1));
+    a.z = (R)(o[2] - WalkOrigin<R>::off(org, 2));
+    a.w = (R)r2;
     b.x = (R)o[4]; b.y = (R)o[5]; b.z = (R)o[6]; b.w = (R)o[3];
     c.x = (R)o[7]; c.y = (R)o[8]; c.z = (R)o[9];
     c.w = (R)(o[4] + o[5] + o[6]);  // trace of the second moments
@@ -110,7 +113,8 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
                          double *__restrict__ hmax, double *__restrict__ ropen2,
                          float4 *__restrict__ sA, float4 *__restrict__ sB, int *__restrict__ flag,
                          int *__restrict__ first, int *__restrict__ last, int *__restrict__ child,
-                         typename R4<R>::T *wA, int4 *__restrict__ wL) {
+                         typename R4<R>::T *wA, int4 *__restrict__ wL,
+                         const int *__restrict__ cloud, const double *__restrict__ corg) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     int nd = n - 1 + p;
@@ -128,7 +132,11 @@ __global__ void k_leaves(int n, const double *__restrict__ x, const double *__re
     child[2 * nd + 1] = -1;
     wL[nd] = make_int4(p, 1, -1, -1);
     typename R4<R>::T a;
-    a.x = (R)xp; a.y = (R)yp; a.z = (R)zp; a.w = (R)0;
+    const double *org = corg + 3 * cloud[p];
+    a.x = (R)(xp - WalkOrigin<R>::off(org, 0));
+    a.y = (R)(yp - WalkOrigin<R>::off(org, 1));
+    a.z = (R)(zp - WalkOrigin<R>::off(org, 2));
+    a.w = (R)0;
     wA[nd] = a;
     if (p < n - 1) flag[p] = 0;
 }
@@ -192,7 +200,8 @@ template <class R>
 __device__ __forceinline__ void store_node(int nd, const double *o, double hm, double theta,
                                            double *node, double *hmax, double *ropen2,
                                            float4 *sA, float4 *sB, typename R4<R>::T *wA,
-                                           typename R4<R>::T *wB, typename R4<R>::T *wC) {
+                                           typename R4<R>::T *wB, typename R4<R>::T *wC,
+                                           const double *org) {
     const double r2 = open_r2(o, theta);
     double *dst = node + (size_t)16 * nd;
     for (int q = 0; q < 16; q++) dst[q] = o[q];
@@ -200,7 +209,7 @@ __device__ __forceinline__ void store_node(int nd, const double *o, double hm, d
     ropen2[nd] = r2;
     sA[nd] = box_lo(o[10], o[11], o[12], hm);
     sB[nd] = box_hi(o[13], o[14], o[15]);
-    write_walk<R>(nd, o, r2, hm, wA, wB, wC);
+    write_walk<R>(nd, o, r2, hm, wA, wB, wC, org);
 }
 
 // the internal nodes inside each group (the nodes of at most 32 particles of
@@ -222,7 +231,8 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
                const double *__restrict__ z, const double *__restrict__ m,
                const double *__restrict__ h, double *node, double *hmax, double *ropen2,
                float4 *sA, float4 *sB, Opening op, typename R4<R>::T *wA,
-               typename R4<R>::T *wB, typename R4<R>::T *wC) {
+               typename R4<R>::T *wB, typename R4<R>::T *wC,
+               const int *__restrict__ cloud, const double *__restrict__ corg) {
     __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
         pm[GUP_WARPS][32], ph[GUP_WARPS][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -269,7 +279,8 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             }
             o[0] = cx; o[1] = cy; o[2] = cz; o[3] = M;
             o[4] = qxx; o[5] = qyy; o[6] = qzz; o[7] = qxy; o[8] = qxz; o[9] = qyz;
-            store_node<R>(nd, o, hm, op.at(l - f + 1), node, hmax, ropen2, sA, sB, wA, wB, wC);
+            store_node<R>(nd, o, hm, op.at(l - f + 1), node, hmax, ropen2, sA, sB, wA, wB, wC,
+                          corg + 3 * cloud[s0]);
         }
         __syncwarp();
     }
@@ -285,7 +296,8 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
                             const double *__restrict__ m, double *node, double *hmax,
                             double *ropen2, float4 *sA, float4 *sB, int *flag, Opening op,
                             const int4 *__restrict__ wL, typename R4<R>::T *wA,
-                            typename R4<R>::T *wB, typename R4<R>::T *wC) {
+                            typename R4<R>::T *wB, typename R4<R>::T *wC,
+                            const int *__restrict__ cloud, const double *__restrict__ corg) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= *ngroup_p || n < 2) return;
     int nd = parent[gnode[g]];
@@ -311,7 +323,8 @@ __global__ void k_bottom_up(int n, const int *__restrict__ ngroup_p,
         }
         combine(o, a, b);
         double hm = fmax(__ldcg(hmax + L), __ldcg(hmax + Rr));
-        store_node<R>(nd, o, hm, op.at(wL[nd].y), node, hmax, ropen2, sA, sB, wA, wB, wC);
+        store_node<R>(nd, o, hm, op.at(wL[nd].y), node, hmax, ropen2, sA, sB, wA, wB, wC,
+                      corg + 3 * cloud[wL[nd].x]);
         nd = parent[nd];
     }
 }
@@ -399,34 +412,34 @@ int launch_tree(sph_ctx *ctx) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (float4 *)ctx->wA,
-            ctx->wL);
+            ctx->wL, ctx->cloud[c], ctx->corg);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
-            (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC);
+            (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->cloud[c], ctx->corg);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (float4 *)ctx->wA,
-            (float4 *)ctx->wB, (float4 *)ctx->wC);
+            (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->cloud[c], ctx->corg);
     } else {
         k_leaves<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (double4 *)ctx->wA,
-            ctx->wL);
+            ctx->wL, ctx->cloud[c], ctx->corg);
         if ((rc = launch_groups(ctx))) return rc;
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
-            (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC);
+            (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->cloud[c], ctx->corg);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (double4 *)ctx->wA,
-            (double4 *)ctx->wB, (double4 *)ctx->wC);
+            (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->cloud[c], ctx->corg);
     }
     ctx->tree_ok = true;
     return ctx_check_launch(ctx, "tree");

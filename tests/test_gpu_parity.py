@@ -300,6 +300,30 @@ def test_gravity_walk_mixed_vs_direct(theta, bound):
     assert rms_rel(a, ad) < bound
 
 
+def test_gravity_walk_mixed_far_from_origin():
+    """The mixed walk's FP32 coordinates are relative to each cloud's box
+    centre, so a sphere centred at (2e4, -3e4, 1e4) (FP32 spacing 2e-3 there,
+    against particle separations of 1e-2) keeps the accuracy of the same
+    sphere at the origin against the FP64 direct sum, with the expansions of
+    the headline walk."""
+    n = 40000
+    d = shuffled_evrard(n, seed=4)
+    tg = np.random.default_rng(1).choice(n, 2000, replace=False).astype(np.int32)
+    errs = []
+    for shift in (np.zeros(3), np.array([2e4, -3e4, 1e4])):
+        ctx = make_ctx(n, "mixed", theta=0.35, theta_small=0.45, small_cell=128,
+                       theta_local=0.28)
+        ctx.load(d["pos"] + shift, d["vel"], d["m"], d["h"], d["u"])
+        ctx.sort()
+        ctx.build_tree()
+        ctx.gravity()
+        ad, _ = ctx.gravity_direct(tg)
+        errs.append(rms_rel(ctx.get_acc("grav", True)[tg], ad))
+        ctx.close()
+    assert errs[0] < 3e-4, errs
+    assert errs[1] < 1.05 * errs[0], errs
+
+
 @pytest.mark.parametrize("theta,theta_local,bound", [(0.38, 0.13, 1.6e-4), (0.38, 0.25, 1.6e-4), (0.5, 0.2, 5e-4)])
 def test_gravity_walk_local_expansion_vs_direct(theta, theta_local, bound):
     """Far cells through the groups' Taylor expansions: the error against the
