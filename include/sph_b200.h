@@ -124,8 +124,10 @@ typedef struct sph_config {
     int32_t max_ngb;      /* neighbour-list row capacity                          */
     int32_t h_max_iter;   /* Newton iteration cap                                 */
     int32_t flags;        /* SPH_FLAG_*                                           */
-    int32_t walk_blocks;  /* gravity-walk blocks per SM (0: one group per warp);
-                             fewer leaves room for the SPH passes beside it      */
+    int32_t walk_blocks;  /* gravity-walk blocks per SM; fewer leave room for the
+                             SPH passes running beside the walk in sph_step.
+                             0: 4 per SM for the FP32 walk inside sph_step, the
+                             occupancy limit otherwise                         */
     double n_ngb;         /* target (4pi/3)(2h)^3 rho / m                         */
     double h_tol;         /* |dh/h| convergence of the Newton iteration           */
     double gamma, alpha, beta, eta; /* EOS and viscosity (libsx.py:22-26)         */

@@ -196,7 +196,10 @@ int step_body(sph_ctx *ctx) {
     CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
     CK(cudaStreamWaitEvent(ctx->stream_g, ctx->ev_fork, 0));
     MARK(13, ctx->stream_g);
-    if ((rc = launch_gravity(ctx, ctx->stream_g, pot))) return rc;
+    ctx->in_step = true;
+    rc = launch_gravity(ctx, ctx->stream_g, pot);
+    ctx->in_step = false;
+    if (rc) return rc;
     MARK(14, ctx->stream_g);
     CK(cudaEventRecord(ctx->ev_join, ctx->stream_g));
     if ((rc = launch_smoothing_h(ctx))) return rc;

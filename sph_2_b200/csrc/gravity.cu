@@ -934,7 +934,12 @@ int run_walk(sph_ctx *ctx, cudaStream_t s) {
     // groups hold 1..32 particles (about 20 on average); size the grid for
     // one group per warp at 16 particles per group, the rest by grid stride
     int grid0 = max(1, div_up(div_up(ctx->n, 16) + ctx->ncloud, WALK_WARPS));
-    if (ctx->cfg.walk_blocks > 0) grid0 = min(grid0, ctx->num_sms * ctx->cfg.walk_blocks);
+    // inside the step the walk runs beside the SPH passes of the other
+    // stream: 4 of the FP32 walk's 6 resident blocks per SM leave room for
+    // them (N = 1M: step 6.21 -> 6.15 ms, the walk alone 2.29 -> 2.66 ms)
+    int per_sm = ctx->cfg.walk_blocks;
+    if (per_sm == 0 && ctx->in_step && std::is_same<R, float>::value) per_sm = 4;
+    if (per_sm > 0) grid0 = min(grid0, ctx->num_sms * per_sm);
     const R eps2 = (R)(ctx->cfg.eps * ctx->cfg.eps);
     SgArgs sg{};
     int rc;

@@ -161,6 +161,7 @@ struct sph_ctx {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_valid = false;
     bool prologue_done = false;
+    bool in_step = false;  // the walk being queued is sph_step's (beside the SPH passes)
     int64_t step_count = 0;
 };
 
