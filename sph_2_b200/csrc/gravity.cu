@@ -20,10 +20,10 @@
 // root per interaction.  In FP32 every instruction evaluates two staged
 // entries at once with the packed f32x2 arithmetic of sm_100 (__ffma2_rn /
 // __fmul2_rn), which halves the issued instructions of this issue-bound loop.
-// Each 32-term chunk is summed plainly and folded into a Kahan accumulator
-// (mixed).  The FP32 walk with theta_local > 0 also sends far accepted cells
-// through per-group Taylor expansions, and starts each group from its
-// super-group's node list with the super-group's own expansion (k_sg_walk).
+// Each 32-term chunk is summed plainly and added to a plain accumulator.
+// The FP32 walk with theta_local > 0 also sends far accepted cells through
+// per-group Taylor expansions, and starts each group from its super-group's
+// node list with the super-group's own expansion (k_sg_walk).
 #include <type_traits>
 
 #include "sph_internal.cuh"
@@ -43,6 +43,12 @@ constexpr int NLOC = 35;
 constexpr int WSTK = SPH_WALK_STACK;
 
 constexpr unsigned FULL = 0xffffffffu;
+
+template <class R> struct PlainSum {
+    R s = R(0);
+    __device__ __forceinline__ void add(R x) { s += x; }
+    __device__ __forceinline__ double value() const { return (double)s; }
+};
 
 template <class R> __device__ __forceinline__ R rsq(R x);
 template <> __device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
@@ -278,8 +284,12 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
                 bz0 = wmin<R>(act ? pi.z : R(INFINITY));
         const R bx1 = wmax<R>(act ? pi.x : R(-INFINITY)), by1 = wmax<R>(act ? pi.y : R(-INFINITY)),
                 bz1 = wmax<R>(act ? pi.z : R(-INFINITY));
-        KSum<R> ax, ay, az, ph;
-        long long nC = 0, nP = 0, nF = 0;
+        // each chunk's sum (at most 32 terms) joins a plain accumulator of
+        // the walk's precision: in FP32 the compensated form measured 1.7 %
+        // slower (the registers of its correction terms) for a change of
+        // 1.3e-7 in the acceleration, against the opening angle's 1e-4
+        PlainSum<R> ax, ay, az, ph;
+        int nC = 0, nP = 0, nF = 0;
         int sp = 1, nc = 0, np = 0, nr = 0, nfar = 0;
         bool overflow = false;
         // the super-group's node list replaces the root when it has one
@@ -667,8 +677,8 @@ __global__ void __launch_bounds__(WALK_WARPS * 32, std::is_same<R, float>::value
             if (POT) pot[i] = G * (ph.value() + self);
         }
         if (lane == 0) {
-            atomicAdd(&counters[0], (unsigned long long)(nC * gc));
-            atomicAdd(&counters[1], (unsigned long long)(nP * gc));
+            atomicAdd(&counters[0], (unsigned long long)nC * gc);
+            atomicAdd(&counters[1], (unsigned long long)nP * gc);
             atomicAdd(&counters[2], (unsigned long long)nF);
             if (overflow) status_add(status, SPH_S_STACK_OVERFLOW, 1);
         }
