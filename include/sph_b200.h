@@ -47,8 +47,9 @@ extern "C" {
 
 /* ---- enums ---- */
 #define SPH_PREC_FP64 0   /* every sum and the gravity walk in FP64                  */
-#define SPH_PREC_MIXED 1  /* FP32 walk and SPH sums with Kahan compensation; FP64
-                             positions, integration, h convergence, reductions       */
+#define SPH_PREC_MIXED 1  /* FP32 walk and SPH sums (the SPH sums with Kahan
+                             compensation); FP64 positions, integration, h
+                             convergence, reductions                                */
 #define SPH_AV_MG83 0     /* Monaghan & Gingold 1983 (libsx.py:185-262)              */
 #define SPH_AV_GADGET 1   /* signal-velocity form (shear.py:243-330, hfvCLibs:705)   */
 #define SPH_DT_COURANT 0  /* dt = courant min_i min(h/v_sig, sqrt(h/|a|)) per cloud  */
@@ -404,6 +405,21 @@ int sph_prologue(sph_ctx *ctx);
  * -kick-du/dt-u-[cooling]-dt (sph_mpi4_v4.py:278-442; EVR.cu:1139-1782),
  * replayed from a CUDA graph unless SPH_FLAG_NO_GRAPH. */
 int sph_step(sph_ctx *ctx, int32_t nsteps);
+/* One step with its host transfers, for drivers that exchange particle fields
+ * with the host every step (the reference's GPU loop copies x, y, z and the
+ * masses out and the tree arrays back in every step, EVR.cu:1462-1482): the
+ * nin fields fin[k] are copied in from the host arrays in[k] (as
+ * sph_set_fields, caller order), one step runs (as sph_step), and the nout
+ * fields fout[k] are copied to the host arrays out[k] (as sph_get_fields,
+ * caller order).  The out copies run on a copy stream of the context, each
+ * as soon as the step has written the field's last value (positions and
+ * masses after the sort, h after the neighbour pass, velocities after the
+ * closing kick, the rest at the end), so they overlap the rest of the step.
+ * in[k] and out[j] may be the same array.  The first call allocates a staging
+ * buffer of max(nin, nout) x n_max doubles and the copy stream.  Returns when
+ * the step and every copy are complete. */
+int sph_step_io(sph_ctx *ctx, int32_t nin, const int32_t *fin, const double *const *in,
+                int32_t nout, const int32_t *fout, double *const *out);
 
 /* internal per-particle arrays for diagnostics, storage order:
  * 0 candidate count (int32), 1 list count (int32), 2 retry flag (int32),

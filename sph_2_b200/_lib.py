@@ -105,6 +105,7 @@ SIGNATURES = [
     ("sph_set_field", C.c_int, [_P, _I, _P, _I, _I]),
     ("sph_set_fields", C.c_int, [_P, _I, _P, _P, _I, _I]),
     ("sph_get_fields", C.c_int, [_P, _I, _P, _P, _I, _I]),
+    ("sph_step_io", C.c_int, [_P, _I, _P, _P, _I, _P, _P]),
     ("sph_get_ids", C.c_int, [_P, _P, _I]),
     ("sph_get_status", C.c_int, [_P, _P, _I]),
     ("sph_get_dt", C.c_int, [_P, _P]),

@@ -223,6 +223,27 @@ class Context:
                                          int(storage_order)), "get_fields")
         return res
 
+    def step_io(self, inputs: dict, outputs: dict):
+        """One step with its host transfers (sph_step_io): the fields of
+        `inputs` ({name: array of n values}) are copied in, one step runs, and
+        the fields of `outputs` ({name: C-contiguous float64 array of n
+        values}, e.g. pinned host memory) are filled with the step's results,
+        copied out while the rest of the step runs.  Caller (original) order."""
+        names_in = list(inputs)
+        arrs = [_f64(inputs[k]) for k in names_in]
+        ids_in = np.array([L.FIELD[k] for k in names_in], np.int32)
+        ptr_in = (C.c_void_p * max(len(arrs), 1))(*[a.ctypes.data for a in arrs])
+        names_out = list(outputs)
+        for k in names_out:
+            a = outputs[k]
+            if a.dtype != np.float64 or a.shape != (self.n,) or not a.flags.c_contiguous:
+                raise ValueError("output arrays must be C-contiguous float64 arrays of n values")
+        ids_out = np.array([L.FIELD[k] for k in names_out], np.int32)
+        ptr_out = (C.c_void_p * max(len(names_out), 1))(*[outputs[k].ctypes.data for k in names_out])
+        self._chk(self._L.sph_step_io(self._h, len(arrs), _ptr(ids_in), ptr_in, len(names_out),
+                                      _ptr(ids_out), ptr_out), "step_io")
+        return outputs
+
     def get_pos(self, storage_order=False):
         return np.stack([self.get(k, storage_order) for k in "xyz"], 1)
 

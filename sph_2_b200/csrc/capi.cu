@@ -173,9 +173,20 @@ int ensure_timing(sph_ctx *ctx) {
     return SPH_OK;
 }
 
-#define MARK(k, strm)                                                          \
-    do {                                                                       \
-        if (timing) CK(cudaEventRecordWithFlags(ctx->tev[k], (strm), cudaEventRecordExternal)); \
+// an event visible outside the step: an external event node while the
+// step is captured into a graph, a plain record when it runs eagerly (the
+// external flag is refused outside a capture)
+cudaError_t record_ext(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaError_t r = cudaStreamIsCapturing(s, &st);
+    if (r != cudaSuccess) return r;
+    return st == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, s);
+}
+
+#define MARK(k, strm)                                         \
+    do {                                                      \
+        if (timing) CK(record_ext(ctx->tev[k], (strm)));      \
     } while (0)
 
 // the body of one step, queued on ctx->stream
@@ -190,6 +201,7 @@ int step_body(sph_ctx *ctx) {
     MARK(1, ctx->stream);
     if ((rc = launch_sort(ctx))) return rc;
     MARK(2, ctx->stream);
+    CK(record_ext(ctx->ev_io[0], ctx->stream));
     if ((rc = launch_tree(ctx))) return rc;
     MARK(3, ctx->stream);
     // gravity depends only on the tree: run it beside the SPH passes
@@ -208,6 +220,7 @@ int step_body(sph_ctx *ctx) {
     MARK(5, ctx->stream);
     if ((rc = launch_lists_density(ctx))) return rc;
     MARK(6, ctx->stream);
+    CK(record_ext(ctx->ev_io[1], ctx->stream));
     MARK(7, ctx->stream);
     if ((rc = launch_forces(ctx, true, fused, false))) return rc;
     MARK(8, ctx->stream);
@@ -215,6 +228,7 @@ int step_body(sph_ctx *ctx) {
     const bool courant = ctx->cfg.dt_fixed <= 0.0 && ctx->cfg.dt_mode == SPH_DT_COURANT;
     if ((rc = launch_kick(ctx, 0.5, courant))) return rc;
     MARK(9, ctx->stream);
+    CK(record_ext(ctx->ev_io[2], ctx->stream));
     if (!fused)
         if ((rc = launch_forces(ctx, false, true, false))) return rc;
     MARK(10, ctx->stream);
@@ -229,6 +243,7 @@ int step_body(sph_ctx *ctx) {
         if ((rc = launch_dt_individual(ctx))) return rc;
     rc = launch_dt_commit(ctx);
     MARK(11, ctx->stream);
+    if (!rc) CK(record_ext(ctx->ev_io[3], ctx->stream));
     return rc;
 }
 
@@ -309,6 +324,9 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
         return fail(SPH_ERR_CUDA);
     cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+    for (int k = 0; k < 4; k++)
+        if (cudaEventCreateWithFlags(&ctx->ev_io[k], cudaEventDisableTiming) != cudaSuccess)
+            return fail(SPH_ERR_CUDA);
 #define DAF(ptr, count)                            \
     do {                                           \
         int r_ = dalloc(ctx, &(ptr), (count));     \
@@ -397,6 +415,11 @@ void sph_ctx_destroy(sph_ctx *ctx) {
         for (int k = 0; k < 16; k++) cudaEventDestroy(ctx->tev[k]);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->stream_io) cudaStreamSynchronize(ctx->stream_io);
+    for (int k = 0; k < 4; k++)
+        if (ctx->ev_io[k]) cudaEventDestroy(ctx->ev_io[k]);
+    if (ctx->io_stage) cudaFree(ctx->io_stage);
+    if (ctx->stream_io) cudaStreamDestroy(ctx->stream_io);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->stream_g) cudaStreamDestroy(ctx->stream_g);
     delete ctx;
@@ -1078,55 +1101,160 @@ int sph_prologue(sph_ctx *ctx) {
     return ctx_check_launch(ctx, "prologue");
 }
 
+}  // extern "C"
+
+namespace {
+
+// one step on ctx->stream: the body in eager mode, else the CUDA graph of
+// the current buffer parity (captured on first use)
+int step_launch(sph_ctx *ctx) {
+    int rc;
+    if (ctx->cfg.flags & SPH_FLAG_NO_GRAPH) {
+        if ((rc = step_body(ctx))) return rc;
+    } else {
+        const int par = ctx->cur;
+        if (!ctx->graph[par]) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            rc = step_body(ctx);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                ctx->cur = par;
+                return rc;
+            }
+            if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
+            e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
+            {
+                size_t nn = 0;
+                cudaGraphGetNodes(g, nullptr, &nn);
+                std::vector<cudaGraphNode_t> nodes(nn);
+                if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+                int kc = 0;
+                for (size_t q = 0; q < nn; q++) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
+                        t == cudaGraphNodeTypeKernel)
+                        kc++;
+                }
+                ctx->graph_kernels = kc;
+            }
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaGraphInstantiate", __LINE__);
+            ctx->cur = par;  // capture did not run anything: restore the parity
+        }
+        CK(cudaGraphLaunch(ctx->graph[par], ctx->stream));
+        ctx->cur = par ^ 1;
+    }
+    ctx->step_count++;
+    return SPH_OK;
+}
+
+// the step's event after which a field holds its value at the end of the
+// step: positions and masses after the sort (the drift came before it), h
+// after the neighbour pass, velocities after the closing kick, the rest at
+// the end
+int io_event(int field) {
+    if (field <= SPH_F_Z || field == SPH_F_M) return 0;
+    if (field == SPH_F_H) return 1;
+    if (field <= SPH_F_VZ) return 2;
+    return 3;
+}
+
+}  // namespace
+
+extern "C" {
+
 int sph_step(sph_ctx *ctx, int32_t nsteps) {
     int rc = enter(ctx);
     if (rc) return rc;
     if (nsteps < 0) return SPH_ERR_ARG;
     if (!ctx->prologue_done) return SPH_ERR_STATE;
     if (ctx->n == 0) return SPH_OK;
-    const bool eager = ctx->cfg.flags & SPH_FLAG_NO_GRAPH;
-    for (int k = 0; k < nsteps; k++) {
-        if (eager) {
-            if ((rc = step_body(ctx))) return rc;
-        } else {
-            const int par = ctx->cur;
-            if (!ctx->graph[par]) {
-                cudaGraph_t g = nullptr;
-                CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-                rc = step_body(ctx);
-                cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-                if (rc) {
-                    if (g) cudaGraphDestroy(g);
-                    ctx->cur = par;
-                    return rc;
-                }
-                if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
-                e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
-                {
-                    size_t nn = 0;
-                    cudaGraphGetNodes(g, nullptr, &nn);
-                    std::vector<cudaGraphNode_t> nodes(nn);
-                    if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
-                    int kc = 0;
-                    for (size_t q = 0; q < nn; q++) {
-                        cudaGraphNodeType t;
-                        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess &&
-                            t == cudaGraphNodeTypeKernel)
-                            kc++;
-                    }
-                    ctx->graph_kernels = kc;
-                }
-                cudaGraphDestroy(g);
-                if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaGraphInstantiate", __LINE__);
-                ctx->cur = par;  // capture did not run anything: restore the parity
-            }
-            CK(cudaGraphLaunch(ctx->graph[par], ctx->stream));
-            ctx->cur = par ^ 1;
-        }
-        ctx->step_count++;
-    }
+    for (int k = 0; k < nsteps; k++)
+        if ((rc = step_launch(ctx))) return rc;
     ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;
     return ctx_check_launch(ctx, "step");
+}
+
+int sph_step_io(sph_ctx *ctx, int32_t nin, const int32_t *fin, const double *const *in,
+                int32_t nout, const int32_t *fout, double *const *out) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (nin < 0 || nout < 0 || (nin > 0 && (!fin || !in)) || (nout > 0 && (!fout || !out)))
+        return SPH_ERR_ARG;
+    for (int k = 0; k < nin; k++)
+        if (!field_ptr(ctx, fin[k]) || !in[k]) return SPH_ERR_ARG;
+    for (int k = 0; k < nout; k++)
+        if (!field_ptr(ctx, fout[k]) || !out[k]) return SPH_ERR_ARG;
+    if (!ctx->prologue_done) return SPH_ERR_STATE;
+    const int n = ctx->n;
+    if (n == 0) return SPH_OK;
+    // one staging slot of n_max doubles per field of the larger list, and the
+    // copy stream, made on first use
+    const int slots = std::max(std::max(nin, nout), 1);
+    if (slots > ctx->io_slots) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (ctx->stream_io) CK(cudaStreamSynchronize(ctx->stream_io));
+        if (ctx->io_stage) cudaFree(ctx->io_stage);
+        ctx->io_stage = nullptr;
+        ctx->io_slots = 0;
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, sizeof(double) * (size_t)slots * ctx->cfg.n_max);
+        if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaMalloc", __LINE__);
+        ctx->io_stage = (double *)p;
+        ctx->io_slots = slots;
+    }
+    if (!ctx->stream_io) {
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        CK(cudaStreamCreateWithPriority(&ctx->stream_io, cudaStreamNonBlocking, hi));
+    }
+    cudaStream_t s = ctx->stream;
+    // in: every copy first (back to back on the copy engine), then the
+    // scatters into storage order; the step's first kernels need them all
+    for (int k = 0; k < nin; k++)
+        CK(cudaMemcpyAsync(ctx->io_stage + (size_t)k * n, in[k], sizeof(double) * n,
+                           cudaMemcpyHostToDevice, s));
+    bool pack = false;
+    for (int k = 0; k < nin; k++) {
+        const int field = fin[k];
+        k_gather_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur],
+                                                       ctx->io_stage + (size_t)k * n,
+                                                       field_ptr(ctx, field));
+        if (field <= SPH_F_H) {
+            pack = true;
+            if (field <= SPH_F_Z || field == SPH_F_M) ctx->tree_ok = false;
+            ctx->cand_ok = false;
+        }
+        if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
+    }
+    if (pack && (rc = launch_pack_p1(ctx))) return rc;
+    if ((rc = step_launch(ctx))) return rc;
+    ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;
+    // out: on the copy stream, each field gathered into caller order and
+    // copied out as soon as the step has written its last value; the rest
+    // of the step runs meanwhile.  ctx->cur is the step's output buffer.
+    int waited = -1;
+    for (int ev = 0; ev < 4; ev++) {
+        for (int k = 0; k < nout; k++) {
+            if (io_event(fout[k]) != ev) continue;
+            if (waited < ev) {
+                CK(cudaStreamWaitEvent(ctx->stream_io, ctx->ev_io[ev], 0));
+                waited = ev;
+            }
+            double *stage = ctx->io_stage + (size_t)k * n;
+            k_scatter_by_id<<<div_up(n, 256), 256, 0, ctx->stream_io>>>(n, ctx->id[ctx->cur],
+                                                                        field_ptr(ctx, fout[k]),
+                                                                        stage);
+            CK(cudaMemcpyAsync(out[k], stage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               ctx->stream_io));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream_io));
+    CK(cudaStreamSynchronize(ctx->stream_g));
+    CK(cudaStreamSynchronize(s));
+    return ctx_check_launch(ctx, "step_io");
 }
 
 int sph_get_phase_times(sph_ctx *ctx, float *ms) {

@@ -48,6 +48,13 @@ struct sph_ctx {
     cudaStream_t stream = nullptr, stream_g = nullptr;
     bool own_stream = false;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // points of the step after which fields are final (recorded in every
+    // step): positions and masses (after the sort), h (after the neighbour
+    // pass), velocities (after the closing kick), everything (the end)
+    cudaEvent_t ev_io[4] = {};
+    cudaStream_t stream_io = nullptr;   // copies of sph_step_io (created on first use)
+    double *io_stage = nullptr;         // io_slots x n_max doubles (allocated on first use)
+    int io_slots = 0;
     std::string err;
     int n = 0, ncloud = 0;
     std::vector<int> cloud_start_h;  // ncloud+1
