@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-cooling", action="store_true", help="skip the 2M cooling-cloud key")
     ap.add_argument("--no-large", action="store_true", help="skip the 16M Evrard key")
     ap.add_argument("--large-steps", type=int, default=50)
+    ap.add_argument("--rebuild-every", type=int, default=4,
+                    help="sort and split the tree every k-th step, refit it between (both arms)")
     return ap.parse_args()
 
 
@@ -346,8 +348,8 @@ def main():
     def make(precision, flags=0, vel=None, walk=None):
         if a.static_grid:
             flags |= L.FLAG_STATIC_GRID
-        cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf,
-                     ngb_lanes=a.lanes, flags=flags, **(walk or walk_kw(a, precision)))
+        cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf, ngb_lanes=a.lanes,
+                     flags=flags, rebuild_every=a.rebuild_every, **(walk or walk_kw(a, precision)))
         c = Context(cfg)
         c.set_stream(stream.cuda_stream)
         c.load(d["pos"], d["vel"] if vel is None else vel, d["m"], d["h"], d["u"])
@@ -378,17 +380,18 @@ def main():
     sampler.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.graph_kernels_launched(reset=True)
     with torch.cuda.stream(stream):
         e0.record()
         ctx.step(a.steps)
         e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
+    launches_timed = ctx.graph_kernels_launched()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = world * n * a.steps / (ms * 1e-3)
     phases = ctx.phase_times()
-    kernels_per_step = ctx.graph_kernel_count()
     status = ctx.status()
 
     # ---- roofline of the dominant kernel (the gravity walk) ----
@@ -468,6 +471,18 @@ def main():
                                            np.sqrt(np.mean(ctx64.get("dudt")[sub] ** 2))),
                "subset": len(sub), "definition": "RMS over the subset of |a-a_ref|/|a_ref|",
                "state": "seeded sphere, v = -0.3 r + N(0, 0.05) (seed 11); the prologue's a and du/dt"}
+        if a.rebuild_every > 1:
+            # the walk on a refitted tree: the mixed context after the steps
+            # that keep the last sort's topology, against the FP64 direct sum
+            # on its own positions
+            ctx_m.step(a.rebuild_every - 1)
+            ctx_m.gravity()
+            inv_m = np.empty(n, np.int64)
+            inv_m[ctx_m.ids()] = np.arange(n)
+            tg_m = inv_m[sub].astype(np.int32)
+            ad_m, _ = ctx_m.gravity_direct(tg_m)
+            err["grav_mixed_vs_direct_fp64_refit_tree"] = rms_rel(ctx_m.get_acc("grav", True)[tg_m], ad_m)
+            err["refit_steps_before_that_check"] = a.rebuild_every - 1
         ctx_m.close()
         ctx64.close()
         ctx64 = make("fp64", L.FLAG_TIMING)
@@ -612,11 +627,12 @@ def main():
                    "n_ngb": 64, "eps": 1e-2, "av": "monaghan-gingold alpha=1 beta=2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "working set > L2 (neighbour rows ~0.3 GB + tree ~0.5 GB per step)",
-                   "graph": "CUDA graph per step"},
+                   "graph": "CUDA graph per step",
+                   "rebuild_every": a.rebuild_every},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": kernels_per_step * a.steps,
+        "gpu_launches": launches_timed,
         "clocks": clocks,
         "fp64_plain": fp64,
         "mixed_same_walk": same_walk,
@@ -655,7 +671,8 @@ def ensemble_run(a, stream, timed, rank=0, world=1):
     mine = local_ensemble(e, owner, rank)
     n = len(mine["m"])
     ctx = Context(Config(n_max=n, n_cloud_max=len(mine["counts"]), precision="mixed",
-                         leaf_size=a.leaf, ngb_lanes=a.lanes, **walk_kw(a, "mixed")))
+                         leaf_size=a.leaf, ngb_lanes=a.lanes, rebuild_every=a.rebuild_every,
+                         **walk_kw(a, "mixed")))
     ctx.set_stream(stream.cuda_stream)
     ctx.load(mine["pos"], mine["vel"], mine["m"], mine["h"], mine["u"], cloud=mine["cloud"])
     ctx.prologue()
@@ -697,8 +714,8 @@ def large_evrard(a, stream, timed):
     res = {}
     for arm, prec, mlp in (("mixed_mlp", "mixed", True), ("fp64_exact", "fp64", False)):
         flags = L.FLAG_COOLING | L.FLAG_TIMING | L.FLAG_POTENTIAL | (L.FLAG_COOLING_MLP if mlp else 0)
-        ctx = Context(Config(n_max=n, precision=prec, leaf_size=a.leaf,
-                             ngb_lanes=a.lanes, flags=flags, **walk_kw(a, prec)))
+        ctx = Context(Config(n_max=n, precision=prec, leaf_size=a.leaf, ngb_lanes=a.lanes,
+                             flags=flags, rebuild_every=a.rebuild_every, **walk_kw(a, prec)))
         ctx.set_stream(stream.cuda_stream)
         cooling.setup(ctx, units)
         if mlp:
@@ -746,8 +763,8 @@ def cooling_run(a, stream, timed, n=2_000_000):
     res = {}
     for mode in ("exact", "mlp"):
         flags = L.FLAG_COOLING | (L.FLAG_COOLING_MLP if mode == "mlp" else 0) | L.FLAG_TIMING
-        ctx = Context(Config(n_max=n, precision="mixed", leaf_size=a.leaf,
-                             flags=flags, **walk_kw(a, "mixed")))
+        ctx = Context(Config(n_max=n, precision="mixed", leaf_size=a.leaf, flags=flags,
+                             rebuild_every=a.rebuild_every, **walk_kw(a, "mixed")))
         ctx.set_stream(stream.cuda_stream)
         cooling.setup(ctx, d["units"])
         if mode == "mlp":

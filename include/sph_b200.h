@@ -156,6 +156,18 @@ typedef struct sph_config {
                              r / |r|^2 about the origin (galaxy_isothermal_
                              potential, hfvCLibs_v7_hfv_v2.h:1215-1235); it is
                              not part of the potential energy of sph_energies */
+    int32_t rebuild_every;/* sph_step sorts the particles and builds the tree
+                             topology on every rebuild_every-th step; the
+                             steps between keep the storage order and the
+                             topology and refit the tree (every node's box,
+                             moments, h_max and opening radius recomputed
+                             from the drifted particles, so every walk and
+                             search stays exact for the tree it walks).
+                             1 (default): every step, the reference's order.
+                             A load, an injection, a restart file read or
+                             written, or an explicit sph_sort makes the next
+                             step a full rebuild                               */
+    int32_t reserved;     /* 0                                                 */
 } sph_config;
 
 typedef struct sph_ctx sph_ctx;
@@ -439,8 +451,12 @@ int sph_get_phase_times(sph_ctx *ctx, float *ms);
 /* run nsteps of sph_step between two CUDA events on the context's stream and
  * return their device time in ms (the autotuner's clock) */
 int sph_time_steps(sph_ctx *ctx, int32_t nsteps, float *ms);
-/* kernel nodes in the captured step graph (0 before the first graph step) */
+/* kernel nodes in the step graph captured last (0 before the first graph
+ * step) */
 int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
+/* kernel nodes of every step graph launched since the last reset (rebuild
+ * and refit steps have graphs of their own); reset != 0: start again at 0 */
+int sph_graph_kernels_launched(sph_ctx *ctx, int64_t *count, int32_t reset);
 /* FP32 FMA throughput of this GPU measured by a dependent-chain kernel,
  * TFLOP/s (2 flops per FMA), the denominator for FP32-bound kernels */
 int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
@@ -500,7 +516,9 @@ int sph_outflow_inject(sph_ctx *ctx, const sph_outflow_params *p, double *leftov
  * neighbour h), the last step's accelerations and every cloud's dt.  A context
  * that reads it (capacity permitting) continues exactly as the writing context
  * would have: the next sph_step repeats it bit for bit in the same precision.
- * Cooling tables and surrogate parameters are not part of it. */
+ * (With rebuild_every > 1 both the writing and the reading context make that
+ * next step a full rebuild.)  Cooling tables and surrogate parameters are not
+ * part of it. */
 int sph_write_restart(sph_ctx *ctx, const char *path);
 int sph_read_restart(sph_ctx *ctx, const char *path);
 

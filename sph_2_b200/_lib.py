@@ -54,7 +54,7 @@ class SphConfig(C.Structure):
         ("eps", C.c_double), ("theta", C.c_double), ("courant", C.c_double),
         ("dt_max", C.c_double), ("dt_fixed", C.c_double), ("theta_local", C.c_double),
         ("theta_small", C.c_double), ("small_cell", C.c_int32), ("dt_mode", C.c_int32),
-        ("ext_sigma", C.c_double),
+        ("ext_sigma", C.c_double), ("rebuild_every", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -156,6 +156,7 @@ SIGNATURES = [
     ("sph_get_phase_times", C.c_int, [_P, _P]),
     ("sph_time_steps", C.c_int, [_P, _I, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
+    ("sph_graph_kernels_launched", C.c_int, [_P, _P, _I]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),
     ("sph_morton_sort_noalloc", C.c_int, [_P, _P, _P, _I, _P, _P, _P]),
     ("sph_ic_count", C.c_int, [C.c_char_p, _P]),

@@ -51,6 +51,7 @@ class Config:
     small_cell: int = 0
     dt_mode: str = "courant"
     ext_sigma: float = 0.0
+    rebuild_every: int = 1
 
     def to_c(self) -> L.SphConfig:
         c = L.SphConfig()
@@ -464,6 +465,13 @@ class Context:
     def graph_kernel_count(self) -> int:
         c = C.c_int32()
         self._chk(self._L.sph_graph_kernel_count(self._h, C.byref(c)), "graph_kernel_count")
+        return int(c.value)
+
+    def graph_kernels_launched(self, reset=False) -> int:
+        """Kernel nodes of the step graphs launched since the last reset."""
+        c = C.c_int64(0)
+        self._chk(self._L.sph_graph_kernels_launched(self._h, C.byref(c), int(bool(reset))),
+                  "graph_kernels_launched")
         return int(c.value)
 
     def fp32_peak_tflops(self) -> float:

@@ -41,10 +41,11 @@ int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem) {
 
 void drop_graphs(sph_ctx *ctx) {
     for (int k = 0; k < 2; k++)
-        if (ctx->graph[k]) {
-            cudaGraphExecDestroy(ctx->graph[k]);
-            ctx->graph[k] = nullptr;
-        }
+        for (int r = 0; r < 2; r++)
+            if (ctx->graph[k][r]) {
+                cudaGraphExecDestroy(ctx->graph[k][r]);
+                ctx->graph[k][r] = nullptr;
+            }
     ctx->graph_valid = false;
 }
 
@@ -122,6 +123,7 @@ int check_cfg(const sph_config *c) {
     if (!(c->courant > 0.0)) return SPH_ERR_ARG;
     if (c->dt_mode != SPH_DT_COURANT && c->dt_mode != SPH_DT_INDIVIDUAL) return SPH_ERR_ARG;
     if (!(c->ext_sigma >= 0.0)) return SPH_ERR_ARG;
+    if (c->rebuild_every < 0 || c->rebuild_every > 1000) return SPH_ERR_ARG;
     return SPH_OK;
 }
 
@@ -189,8 +191,10 @@ cudaError_t record_ext(cudaEvent_t e, cudaStream_t s) {
         if (timing) CK(record_ext(ctx->tev[k], (strm)));      \
     } while (0)
 
-// the body of one step, queued on ctx->stream
-int step_body(sph_ctx *ctx) {
+// the body of one step, queued on ctx->stream; refit: keep the storage order
+// and the tree topology of the last full rebuild and refit the tree to the
+// drifted particles (no sort, no Karras split, no group tables)
+int step_body(sph_ctx *ctx, bool refit) {
     int rc;
     const bool fused = ctx->cfg.flags & SPH_FLAG_DUDT_FUSED;
     const bool pot = ctx->cfg.flags & SPH_FLAG_POTENTIAL;
@@ -199,10 +203,10 @@ int step_body(sph_ctx *ctx) {
     MARK(0, ctx->stream);
     if ((rc = launch_kick_drift(ctx))) return rc;
     MARK(1, ctx->stream);
-    if ((rc = launch_sort(ctx))) return rc;
+    if ((rc = refit ? launch_sort_refit(ctx) : launch_sort(ctx))) return rc;
     MARK(2, ctx->stream);
     CK(record_ext(ctx->ev_io[0], ctx->stream));
-    if ((rc = launch_tree(ctx))) return rc;
+    if ((rc = refit ? launch_tree_refit(ctx) : launch_tree(ctx))) return rc;
     MARK(3, ctx->stream);
     // gravity depends only on the tree: run it beside the SPH passes
     CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
@@ -292,6 +296,7 @@ int sph_default_config(sph_config *c) {
     c->courant = 0.25;
     c->dt_max = 0.0;
     c->dt_fixed = 0.0;
+    c->rebuild_every = 1;
     return SPH_OK;
 }
 
@@ -465,6 +470,7 @@ int sph_set_params(sph_ctx *ctx, const sph_config *c) {
     t.theta_small = c->theta_small; t.small_cell = c->small_cell;
     t.dt_mode = c->dt_mode;
     t.ext_sigma = c->ext_sigma;
+    t.rebuild_every = c->rebuild_every;
     int rc = check_cfg(&t);
     if (rc) return rc;
     if (t.theta != ctx->cfg.theta || t.leaf_size != ctx->cfg.leaf_size ||
@@ -541,6 +547,7 @@ int sph_load(sph_ctx *ctx, int32_t n, const int32_t *cloud, const double *x, con
     ctx->prologue_done = false;
     ctx->step_count = 0;
     ctx->last_injected_id = -1;
+    ctx->topo_ok = false;
     return ctx_check_launch(ctx, "load");
 }
 
@@ -1023,6 +1030,7 @@ int sph_outflow_inject(sph_ctx *ctx, const sph_outflow_params *p, double *leftov
         if ((rc = launch_pack_p1(ctx))) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = ctx->cand_ok = false;
+        ctx->topo_ok = false;  // new particles: the next step sorts and splits again
         ctx->p2_dirty = true;
         mass -= 2.0 * p->m_particle * npairs;
     }
@@ -1106,25 +1114,30 @@ int sph_prologue(sph_ctx *ctx) {
 namespace {
 
 // one step on ctx->stream: the body in eager mode, else the CUDA graph of
-// the current buffer parity (captured on first use)
+// the current buffer parity and step kind (captured on first use).  Every
+// rebuild_every-th step (and the first after the topology was invalidated)
+// sorts and rebuilds the tree; the steps between refit it.
 int step_launch(sph_ctx *ctx) {
     int rc;
+    const int every = ctx->cfg.rebuild_every;
+    const bool refit = every > 1 && ctx->topo_ok && ctx->refits + 1 < every;
     if (ctx->cfg.flags & SPH_FLAG_NO_GRAPH) {
-        if ((rc = step_body(ctx))) return rc;
+        if ((rc = step_body(ctx, refit))) return rc;
     } else {
         const int par = ctx->cur;
-        if (!ctx->graph[par]) {
+        cudaGraphExec_t &gx = ctx->graph[par][refit ? 1 : 0];
+        if (!gx) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-            rc = step_body(ctx);
+            rc = step_body(ctx, refit);
             cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            ctx->cur = par;  // capture did not run anything: restore the parity
             if (rc) {
                 if (g) cudaGraphDestroy(g);
-                ctx->cur = par;
                 return rc;
             }
             if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
-            e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
+            e = cudaGraphInstantiate(&gx, g, 0);
             {
                 size_t nn = 0;
                 cudaGraphGetNodes(g, nullptr, &nn);
@@ -1138,13 +1151,20 @@ int step_launch(sph_ctx *ctx) {
                         kc++;
                 }
                 ctx->graph_kernels = kc;
+                ctx->graph_nk[par][refit ? 1 : 0] = kc;
             }
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return ctx_fail(ctx, e, "cudaGraphInstantiate", __LINE__);
-            ctx->cur = par;  // capture did not run anything: restore the parity
         }
-        CK(cudaGraphLaunch(ctx->graph[par], ctx->stream));
-        ctx->cur = par ^ 1;
+        CK(cudaGraphLaunch(gx, ctx->stream));
+        ctx->graph_kernels_launched += ctx->graph_nk[par][refit ? 1 : 0];
+        if (!refit) ctx->cur = par ^ 1;
+    }
+    if (refit) {
+        ctx->refits++;
+    } else {
+        ctx->refits = 0;
+        ctx->topo_ok = true;
     }
     ctx->step_count++;
     return SPH_OK;
@@ -1335,6 +1355,13 @@ int sph_time_steps(sph_ctx *ctx, int32_t nsteps, float *ms) {
 int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count) {
     if (!ctx || !count) return SPH_ERR_ARG;
     *count = ctx->graph_kernels;
+    return SPH_OK;
+}
+
+int sph_graph_kernels_launched(sph_ctx *ctx, int64_t *count, int32_t reset) {
+    if (!ctx || !count) return SPH_ERR_ARG;
+    *count = ctx->graph_kernels_launched;
+    if (reset) ctx->graph_kernels_launched = 0;
     return SPH_OK;
 }
 

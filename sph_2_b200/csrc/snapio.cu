@@ -210,6 +210,9 @@ int sph_write_restart(sph_ctx *ctx, const char *path) {
         if (n > 0) CK(cudaMemcpy(buf.data(), a, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
         ok = F.write(buf.data(), sizeof(double) * 3 * n);
     }
+    // a context resumed from this file starts with a full rebuild; so does
+    // this one, so that both continue alike
+    ctx->topo_ok = false;
     return ok ? SPH_OK : SPH_ERR_IO;
 }
 
@@ -268,6 +271,7 @@ int sph_read_restart(sph_ctx *ctx, const char *path) {
     ctx->p2_dirty = true;
     ctx->prologue_done = h.prologue_done != 0;
     ctx->step_count = h.step_count;
+    ctx->topo_ok = false;  // the topology is not in the file: the next step rebuilds
     ctx->last_injected_id = h.last_injected_id;
     return ctx_check_launch(ctx, "read_restart");
 }

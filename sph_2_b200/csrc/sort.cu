@@ -299,8 +299,27 @@ static int morton_bits_for(int ncloud) {
     return (63 - cb) / 3;
 }
 
+// The first phase of a refit step: the per-cloud boxes (non-finite check and
+// the origin of the FP32 walk coordinates) and the packed records of the
+// drifted particles, in the storage order of the last sort.
+int launch_sort_refit(sph_ctx *ctx) {
+    ctx->cand_ok = false;
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    double *const *st = ctx->st[ctx->cur];
+    k_box_reset<<<div_up(6 * ctx->ncloud, 256), 256, 0, s>>>(ctx->box, ctx->ncloud);
+    k_box<<<div_up(n, 256), 256, 0, s>>>(st[ST_X], st[ST_Y], st[ST_Z], ctx->cloud[ctx->cur], n,
+                                         ctx->box, ctx->status);
+    k_origin<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->box, ctx->ncloud, ctx->corg);
+    int rc = launch_pack_p1(ctx);
+    if (rc) return rc;
+    return ctx_check_launch(ctx, "sort refit");
+}
+
 int launch_sort(sph_ctx *ctx) {
     ctx->cand_ok = false;
+    ctx->topo_ok = false;  // the next tree build splits the new order
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;

@@ -165,7 +165,14 @@ struct sph_ctx {
     int graph_kernels = 0;
 
     // step graphs (one per buffer parity)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // step graphs per buffer parity, full rebuild [0] or refit [1]
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // the tree topology (child / parent / first / last, groups, super-groups)
+    // matches the storage order and particle set, so a step may refit it
+    bool topo_ok = false;
+    int refits = 0;  // refit steps since the last full rebuild
+    int graph_nk[2][2] = {{0, 0}, {0, 0}};  // kernel nodes of each step graph
+    int64_t graph_kernels_launched = 0;     // kernel nodes of the graphs launched
     bool graph_valid = false;
     bool prologue_done = false;
     bool in_step = false;  // the walk being queued is sph_step's (beside the SPH passes)
@@ -328,6 +335,7 @@ enum { WQ_WALK = 0, WQ_SG_WALK = 1, WQ_SEARCH = 2, WQ_N = 3 };
 
 // ---- host-side launch helpers implemented per translation unit ----
 int launch_sort(sph_ctx *ctx);
+int launch_sort_refit(sph_ctx *ctx);
 int launch_scan(sph_ctx *ctx, const int *in, int *out, int n, int *total);
 int launch_groups(sph_ctx *ctx);
 int launch_leaf_records(sph_ctx *ctx);  // the leaves' 16-double records (export only)
@@ -341,6 +349,7 @@ int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 int queue_launch(sph_ctx *ctx, cudaStream_t s, int slot, const void *kernel, int block,
                  int static_grid, int *grid, unsigned **queue);
 int launch_tree(sph_ctx *ctx);
+int launch_tree_refit(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);
 int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac, int max_iter);

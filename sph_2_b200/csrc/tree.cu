@@ -386,34 +386,26 @@ __global__ void k_refit_up(int n, const int *__restrict__ ngroup_p, const int *_
 
 }  // namespace
 
-int launch_tree(sph_ctx *ctx) {
-    ctx->cand_ok = false;
+namespace {
+
+// leaf records, then the moments, boxes and walk records of the nodes inside
+// the groups and of those above them (groups: the tables of the current
+// topology, rebuilt first when `groups`)
+int tree_records(sph_ctx *ctx, bool groups) {
     const int n = ctx->n;
-    if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
-    const unsigned long long *key = ctx->key[0];
-    const bool mixed = ctx->cfg.precision == SPH_PREC_MIXED;
-    if (n > 1)
-        k_karras<<<div_up(n - 1, 256), 256, 0, s>>>(key, ctx->cloud[c], n, ctx->child, ctx->parent,
-                                                    ctx->first, ctx->last, ctx->croot, ctx->wL);
-    k_single_roots<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->cloud_start, ctx->ncloud, n,
-                                                            ctx->croot);
-    // the root has no parent
-    CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
-    // leaf records (they complete the leaves' first / last the groups read),
-    // the groups, the nodes inside the groups, then the climb above them
     float4 *boxA = (float4 *)ctx->node_box;
     float4 *boxB = boxA + (2 * (size_t)ctx->cfg.n_max);
     const int ggrid = max(1, div_up(div_up(n, 16) + ctx->ncloud, GUP_WARPS));
     const Opening op{ctx->cfg.theta, ctx->cfg.theta_small, ctx->cfg.small_cell};
     int rc;
-    if (mixed) {
+    if (ctx->cfg.precision == SPH_PREC_MIXED) {
         k_leaves<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (float4 *)ctx->wA,
             ctx->wL, ctx->cloud[c], ctx->corg);
-        if ((rc = launch_groups(ctx))) return rc;
+        if (groups && (rc = launch_groups(ctx))) return rc;
         k_group_up<float><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
@@ -429,7 +421,7 @@ int launch_tree(sph_ctx *ctx) {
             n, ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_H], ctx->hmax,
             ctx->ropen2, boxA, boxB, ctx->flag, ctx->first, ctx->last, ctx->child, (double4 *)ctx->wA,
             ctx->wL, ctx->cloud[c], ctx->corg);
-        if ((rc = launch_groups(ctx))) return rc;
+        if (groups && (rc = launch_groups(ctx))) return rc;
         k_group_up<double><<<ggrid, GUP_WARPS * 32, 0, s>>>(
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
@@ -441,8 +433,47 @@ int launch_tree(sph_ctx *ctx) {
             ctx->ropen2, boxA, boxB, ctx->flag, op, ctx->wL, (double4 *)ctx->wA,
             (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->cloud[c], ctx->corg);
     }
+    return SPH_OK;
+}
+
+}  // namespace
+
+int launch_tree(sph_ctx *ctx) {
+    ctx->cand_ok = false;
+    const int n = ctx->n;
+    if (n <= 0) return SPH_OK;
+    cudaStream_t s = ctx->stream;
+    const int c = ctx->cur;
+    const unsigned long long *key = ctx->key[0];
+    if (n > 1)
+        k_karras<<<div_up(n - 1, 256), 256, 0, s>>>(key, ctx->cloud[c], n, ctx->child, ctx->parent,
+                                                    ctx->first, ctx->last, ctx->croot, ctx->wL);
+    k_single_roots<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->cloud_start, ctx->ncloud, n,
+                                                            ctx->croot);
+    // the root has no parent
+    CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
+    // leaf records (they complete the leaves' first / last the groups read),
+    // the groups, the nodes inside the groups, then the climb above them
+    int rc = tree_records(ctx, true);
+    if (rc) return rc;
     ctx->tree_ok = true;
+    ctx->topo_ok = true;
+    ctx->refits = 0;
     return ctx_check_launch(ctx, "tree");
+}
+
+// The tree of a refit step: the topology, groups and super-groups of the last
+// full build (the storage order has not changed since), every record of every
+// node recomputed from the drifted particles.  The boxes may be looser than a
+// fresh split would give, never wrong.
+int launch_tree_refit(sph_ctx *ctx) {
+    ctx->cand_ok = false;
+    if (ctx->n <= 0) return SPH_OK;
+    if (!ctx->topo_ok) return SPH_ERR_STATE;
+    int rc = tree_records(ctx, false);
+    if (rc) return rc;
+    ctx->tree_ok = true;
+    return ctx_check_launch(ctx, "tree refit");
 }
 
 int launch_leaf_records(sph_ctx *ctx) {
