@@ -417,8 +417,8 @@ def main():
     roofline = {"kernel": "k_sg_walk + k_walk<float> (gravity walk)", "bound": "fp32",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp32_peak, "traffic": None,
-                "peak_source": "FP32 FMA-chain kernel measured in this run (MEASURED_PEAKS.json "
-                               "has no FP32 figure)",
+                "peak_source": ("FP32 FMA-chain kernels, scalar and packed f32x2, the larger, "
+                                "measured in this run (MEASURED_PEAKS.json has no FP32 figure)"),
                 "algorithmic": ("60 flop per quadrupole cell + 20 per particle interaction "
                                 "+ 190 per far cell (once per group or super-group) + 115 per "
                                 "particle for each of the group and super-group expansions"),

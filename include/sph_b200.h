@@ -457,8 +457,9 @@ int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
 /* kernel nodes of every step graph launched since the last reset (rebuild
  * and refit steps have graphs of their own); reset != 0: start again at 0 */
 int sph_graph_kernels_launched(sph_ctx *ctx, int64_t *count, int32_t reset);
-/* FP32 FMA throughput of this GPU measured by a dependent-chain kernel,
- * TFLOP/s (2 flops per FMA), the denominator for FP32-bound kernels */
+/* FP32 FMA throughput of this GPU measured by dependent-chain kernels of
+ * scalar and of packed (f32x2) FMAs, the larger of the two, TFLOP/s (2 flops
+ * per FMA): the denominator for FP32-bound kernels */
 int sph_measure_fp32_peak(sph_ctx *ctx, double *tflops);
 
 /* ---- allocation-free Morton order ---- */
