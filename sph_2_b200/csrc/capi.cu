@@ -395,7 +395,8 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->ngb, K * N); DAF(ctx->ngb_cnt, N);
     DAF(ctx->cand_idx, K * N);
     DAF(ctx->cand_cnt, N);
-    DAF(ctx->lflag, N + 2);
+    DAF(ctx->lflag, N + 3);
+    DAF(ctx->mlist, N);
     DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N); DAF(ctx->hover, N);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C); DAF(ctx->dtmax_bits, C);
     DAF(ctx->dt_part, N); DAF(ctx->dhdt, N); DAF(ctx->dbin, N);

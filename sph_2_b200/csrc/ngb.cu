@@ -129,6 +129,9 @@ struct SearchArgs {
     // exact search restricted to the particles with only[i] != 0, or to all
     // of them when *only_all != 0 (null: every particle)
     const int *only, *only_all;
+    // with only: the marked particles also listed (mlist, *mcount entries);
+    // k_lists then runs only when *only_all, k_lists_list otherwise
+    const int *mlist, *mcount;
     long long *status;
 };
 
@@ -461,6 +464,7 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
+    if (A.mlist && !*A.only_all) return;  // the listed particles: k_lists_list
     for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
          g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
@@ -472,6 +476,29 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32)
         }
         const double4 pi = A.p0[i];
         group_search<1>(smem[w], A, g, act, i, pi, pi.w);
+    }
+}
+
+// exact lists for the listed particles (A.mlist, *A.mcount entries; nothing
+// when *A.only_all, which k_lists covers): one warp per particle, its own box
+// (the search of one lane), the cloud root of the group holding it
+__global__ void __launch_bounds__(SEARCH_WARPS * 32)
+    k_lists_list(const int *__restrict__ ngroup_p, SearchArgs A) {
+    __shared__ SearchSmem smem[SEARCH_WARPS];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (*A.only_all) return;
+    const int m = *A.mcount, ngroup = *ngroup_p;
+    for (int e = blockIdx.x * SEARCH_WARPS + w; e < m; e += gridDim.x * SEARCH_WARPS) {
+        const int i = A.mlist[e];
+        // the group holding i: the last one starting at or before it
+        int lo = 0, hi = ngroup - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (A.gstart[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const double4 pi = A.p0[i];
+        group_search<1>(smem[w], A, lo, lane == 0, i, pi, pi.w);
     }
 }
 
@@ -919,6 +946,8 @@ SearchArgs search_args(sph_ctx *ctx, int *rows, int *cnt) {
     A.hnb = ctx->st[ctx->cur][ST_HNB];
     A.only = nullptr;
     A.only_all = nullptr;
+    A.mlist = nullptr;
+    A.mcount = nullptr;
     A.p1 = ctx->p1;
     A.status = ctx->status;
     return A;
@@ -1086,6 +1115,8 @@ int launch_lists_marked(sph_ctx *ctx) {
     SearchArgs A = search_args(ctx, ctx->ngb, ctx->ngb_cnt);
     A.only = ctx->lflag;
     A.only_all = ctx->lflag + n;
+    A.mlist = ctx->mlist;
+    A.mcount = ctx->lflag + n + 2;
     int rc = launch_refit_hmax(ctx, ctx->lflag + n + 1);
     if (rc) return rc;
     int g;
@@ -1094,6 +1125,7 @@ int launch_lists_marked(sph_ctx *ctx) {
                            grid, &g, &q)))
         return rc;
     k_lists<<<g, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup, A, q);
+    k_lists_list<<<ctx->num_sms * 2, SEARCH_WARPS * 32, 0, ctx->stream>>>(ctx->d_ngroup, A);
     return ctx_check_launch(ctx, "lists_marked");
 }
 

@@ -126,21 +126,16 @@ __global__ void __launch_bounds__(256)
 // div/curl sums need only the particle's own density (sum m_j/rho_i ...), so
 // they are accumulated unnormalised beside the density sum and divided by
 // rho_i at the end
+// density, EOS, div v, |curl v| and the packed p2 record of particle i from
+// its list, on the LANES lanes of its segment (every lane of the warp calls:
+// the segment sums are warp collectives; valid false: no particle)
 template <class R, int LANES>
-__global__ void __launch_bounds__(256)
-    k_density_divcurl(int n, const double4 *__restrict__ p0,
-                      const typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ p2,
-                      const int *__restrict__ rows, const int *__restrict__ cnt, int K,
-                      const double *__restrict__ u, double gamma, int balsara,
-                      double *__restrict__ rho_out, double *__restrict__ P_out,
-                      double *__restrict__ c_out, double *__restrict__ divV,
-                      double *__restrict__ curlV, const int *__restrict__ only = nullptr,
-                      const int *__restrict__ only_all = nullptr) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (int)(t / LANES), sl = (int)(t % LANES);
-    // only (may be null): recompute just the particles with only[i] != 0
-    // (all of them when *only_all != 0)
-    const bool valid = i < n && (!only || *only_all || only[i]);
+__device__ __forceinline__ void density_divcurl_one(
+    bool valid, int i, int sl, const double4 *__restrict__ p0,
+    const typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ p2,
+    const int *__restrict__ rows, const int *__restrict__ cnt, int K, const double *__restrict__ u,
+    double gamma, int balsara, double *__restrict__ rho_out, double *__restrict__ P_out,
+    double *__restrict__ c_out, double *__restrict__ divV, double *__restrict__ curlV) {
     KSum<R> S, s, cx, cy, cz;
     double hi = 1.0;
     if (valid) {
@@ -195,6 +190,50 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_density_divcurl(int n, const double4 *__restrict__ p0,
+                      const typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ p2,
+                      const int *__restrict__ rows, const int *__restrict__ cnt, int K,
+                      const double *__restrict__ u, double gamma, int balsara,
+                      double *__restrict__ rho_out, double *__restrict__ P_out,
+                      double *__restrict__ c_out, double *__restrict__ divV,
+                      double *__restrict__ curlV) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t / LANES), sl = (int)(t % LANES);
+    density_divcurl_one<R, LANES>(i < n, i, sl, p0, p1, p2, rows, cnt, K, u, gamma, balsara,
+                                  rho_out, P_out, c_out, divV, curlV);
+}
+
+// The same for the particles the fused list pass sent to the tree search:
+// the *mcount entries of mlist, or every particle when *all is set; a grid
+// of a few blocks per SM strides over them, so a step that marks a hundred
+// particles does not launch a thread per particle
+template <class R, int LANES>
+__global__ void __launch_bounds__(256)
+    k_density_divcurl_list(int n, const int *__restrict__ mlist, const int *__restrict__ mcount,
+                           const int *__restrict__ all, const double4 *__restrict__ p0,
+                           const typename R4<R>::T *__restrict__ p1,
+                           typename R4<R>::T *__restrict__ p2, const int *__restrict__ rows,
+                           const int *__restrict__ cnt, int K, const double *__restrict__ u,
+                           double gamma, int balsara, double *__restrict__ rho_out,
+                           double *__restrict__ P_out, double *__restrict__ c_out,
+                           double *__restrict__ divV, double *__restrict__ curlV) {
+    const bool every = *all != 0;
+    const int m = every ? n : *mcount;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // the trip count is the same for every thread (the segment sums need
+    // the whole warp)
+    for (long long base = 0; base < (long long)m * LANES; base += stride) {
+        const long long t = base + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const int e = (int)(t / LANES), sl = (int)(t % LANES);
+        const bool ok = e < m;
+        const int i = ok ? (every ? e : mlist[e]) : 0;
+        density_divcurl_one<R, LANES>(ok, i, sl, p0, p1, p2, rows, cnt, K, u, gamma, balsara,
+                                      rho_out, P_out, c_out, divV, curlV);
+    }
+}
+
 // The exact lists and the density pass in one: each particle's LANES lanes
 // walk its candidate row from the h iteration (rows i K .. i K + ccnt - 1),
 // keep the pairs with |r| <= h_i + h_j (the FP64 predicate of the tree
@@ -213,7 +252,8 @@ __global__ void __launch_bounds__(256, std::is_same<R, float>::value ? SPH_LISTS
                            const int *__restrict__ ccnt, const double *__restrict__ hc, int K,
                            int *__restrict__ rows, int *__restrict__ cnt, double *__restrict__ hnb,
                            int *__restrict__ full, int *__restrict__ full_all,
-                           int *__restrict__ full_any, long long *status,
+                           int *__restrict__ full_any, int *__restrict__ mlist,
+                           int *__restrict__ mcount, long long *status,
                            const double *__restrict__ u, double gamma, int balsara,
                            double *__restrict__ rho_out, double *__restrict__ P_out,
                            double *__restrict__ c_out, double *__restrict__ divV,
@@ -283,7 +323,8 @@ __global__ void __launch_bounds__(256, std::is_same<R, float>::value ? SPH_LISTS
             const double ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
             const double rj = 2.0 * hc[j];
             if (ex * ex + ey * ey + ez * ez > rj * rj * (1.0 - 1e-9)) {
-                full[j] = 1;
+                // j joins the list of particles to search once
+                if (atomicExch(&full[j], 1) == 0) mlist[atomicAdd(mcount, 1)] = j;
                 *full_any = 1;
             }
         }
@@ -453,13 +494,14 @@ int run_density_divcurl(sph_ctx *ctx) {
     return SPH_OK;
 }
 template <class R, int L>
-int run_density_divcurl_only(sph_ctx *ctx, const int *only, const int *only_all) {
+int run_density_divcurl_marked(sph_ctx *ctx) {
     const int n = ctx->n, c = ctx->cur;
     const int bs = ctx->cfg.block_size;
-    k_density_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
-        n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb,
-        ctx->ngb_cnt, ctx->cfg.max_ngb, ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara,
-        ctx->rho, ctx->P, ctx->c, ctx->divV, ctx->curlV, only, only_all);
+    k_density_divcurl_list<R, L><<<ctx->num_sms * 4, bs, 0, ctx->stream>>>(
+        n, ctx->mlist, ctx->lflag + n + 2, ctx->lflag + n, ctx->p0,
+        (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2, ctx->ngb, ctx->ngb_cnt,
+        ctx->cfg.max_ngb, ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara, ctx->rho, ctx->P,
+        ctx->c, ctx->divV, ctx->curlV);
     return SPH_OK;
 }
 template <class R, int L>
@@ -469,7 +511,8 @@ int run_cand_density_divcurl(sph_ctx *ctx) {
     k_cand_density_divcurl<R, L><<<div_up((long long)n * L, bs), bs, 0, ctx->stream>>>(
         n, ctx->p0, (const typename R4<R>::T *)ctx->p1, (typename R4<R>::T *)ctx->p2,
         ctx->cand_idx, ctx->cand_cnt, ctx->hcand, ctx->cfg.max_ngb, ctx->ngb, ctx->ngb_cnt,
-        ctx->st[c][ST_HNB], ctx->lflag, ctx->lflag + n, ctx->lflag + n + 1, ctx->status,
+        ctx->st[c][ST_HNB], ctx->lflag, ctx->lflag + n, ctx->lflag + n + 1, ctx->mlist,
+        ctx->lflag + n + 2, ctx->status,
         ctx->st[c][ST_U], ctx->cfg.gamma, ctx->cfg.balsara, ctx->rho, ctx->P, ctx->c, ctx->divV,
         ctx->curlV);
     return SPH_OK;
@@ -525,17 +568,16 @@ int launch_lists_density(sph_ctx *ctx) {
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     if (!ctx->cand_ok) return SPH_ERR_STATE;
-    CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 2), ctx->stream));
+    CK(cudaMemsetAsync(ctx->lflag, 0, sizeof(int) * (n + 3), ctx->stream));
     int rc;
     if (ctx->cfg.precision == SPH_PREC_MIXED) { SPH_DISPATCH_LANES(run_cand_density_divcurl, float, ctx); }
     else { SPH_DISPATCH_LANES(run_cand_density_divcurl, double, ctx); }
     if (rc) return rc;
     if ((rc = launch_lists_marked(ctx))) return rc;
-    const int *only = ctx->lflag, *only_all = ctx->lflag + n;
     if (ctx->cfg.precision == SPH_PREC_MIXED) {
-        SPH_DISPATCH_LANES(run_density_divcurl_only, float, ctx, only, only_all);
+        SPH_DISPATCH_LANES(run_density_divcurl_marked, float, ctx);
     } else {
-        SPH_DISPATCH_LANES(run_density_divcurl_only, double, ctx, only, only_all);
+        SPH_DISPATCH_LANES(run_density_divcurl_marked, double, ctx);
     }
     if (rc) return rc;
     ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;

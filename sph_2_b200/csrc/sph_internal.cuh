@@ -121,7 +121,9 @@ struct sph_ctx {
     int *ngb = nullptr, *ngb_cnt = nullptr;
     int *cand_idx = nullptr;  // candidate slots j of the h iteration, max_ngb per particle
     int *cand_cnt = nullptr;
-    int *lflag = nullptr;     // n+2: per particle "needs the tree search", "all do", "any does"
+    int *lflag = nullptr;     // n+3: per particle "needs the tree search", "all do", "any does",
+                              // how many are listed in mlist
+    int *mlist = nullptr;     // the particles the fused list pass marked, each once
     bool cand_ok = false;     // candidate rows match the current order, positions and h
     int *retry = nullptr;        // per particle: 1 = candidate radius too small
     int *hiter = nullptr;        // per particle: iterations of the count iteration so far
