@@ -997,6 +997,14 @@ int launch_smoothing_h(sph_ctx *ctx) {
         unsigned *q;
         int rc = queue_launch(ctx, s, WQ_SEARCH, kern, SEARCH_WARPS * 32, grid, &g, &q);
         if (rc) return rc;
+        if (r > 0) {
+            // the later rounds search again only for the few particles whose
+            // h left the candidate radius: a fixed stride over the groups,
+            // which most warps skip after one ballot, costs less than one
+            // work-queue atomic per group
+            g = min(grid, ctx->num_sms * 8);
+            q = nullptr;
+        }
         if (mixed)
             k_cand_newton<float><<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, q);
         else
