@@ -206,7 +206,7 @@ int step_body(sph_ctx *ctx, bool refit) {
     if ((rc = refit ? launch_sort_refit(ctx) : launch_sort(ctx))) return rc;
     MARK(2, ctx->stream);
     CK(record_ext(ctx->ev_io[0], ctx->stream));
-    if ((rc = refit ? launch_tree_refit(ctx) : launch_tree(ctx))) return rc;
+    if ((rc = refit ? launch_tree_refit(ctx, false) : launch_tree(ctx, false))) return rc;
     MARK(3, ctx->stream);
     // gravity depends only on the tree: run it beside the SPH passes
     CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
@@ -764,6 +764,9 @@ int sph_get_tree(sph_ctx *ctx, double *node, int32_t *child, int32_t *first, int
     cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     cudaStream_t s = ctx->stream;
     if (node) {
+        // the step stores the build records of the group nodes and above
+        // only: recompute the rest for the current topology first
+        if (!ctx->records_all && (rc = launch_tree_records(ctx))) return rc;
         if ((rc = launch_leaf_records(ctx))) return rc;
         CK(cudaMemcpyAsync(node, ctx->node, 16 * sizeof(double) * nn, k, s));
     }

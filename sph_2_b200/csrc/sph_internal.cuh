@@ -173,6 +173,7 @@ struct sph_ctx {
     // matches the storage order and particle set, so a step may refit it
     bool topo_ok = false;
     int refits = 0;  // refit steps since the last full rebuild
+    bool records_all = false;  // every node's 16-double build record is current
     int graph_nk[2][2] = {{0, 0}, {0, 0}};  // kernel nodes of each step graph
     int64_t graph_kernels_launched = 0;     // kernel nodes of the graphs launched
     bool graph_valid = false;
@@ -350,8 +351,11 @@ int persistent_grid(sph_ctx *ctx, const void *kernel, int block, size_t smem);
 // SPH_FLAG_STATIC_GRID is set
 int queue_launch(sph_ctx *ctx, cudaStream_t s, int slot, const void *kernel, int block,
                  int static_grid, int *grid, unsigned **queue);
-int launch_tree(sph_ctx *ctx);
-int launch_tree_refit(sph_ctx *ctx);
+// all_records false: the 16-double build records of the nodes inside the
+// groups are not stored (only sph_get_tree reads them; it rebuilds them)
+int launch_tree(sph_ctx *ctx, bool all_records = true);
+int launch_tree_refit(sph_ctx *ctx, bool all_records = true);
+int launch_tree_records(sph_ctx *ctx);
 int launch_refit_hmax(sph_ctx *ctx, const int *need = nullptr);
 int launch_smoothing_h(sph_ctx *ctx);
 int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac, int max_iter);

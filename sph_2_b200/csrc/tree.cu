@@ -196,15 +196,19 @@ struct Opening {
 };
 
 // the records of node nd from its combined moments o and h_max hm
+// (record false: the 16-double build record is not stored; the walks and
+// searches read only the other records)
 template <class R>
 __device__ __forceinline__ void store_node(int nd, const double *o, double hm, double theta,
                                            double *node, double *hmax, double *ropen2,
                                            float4 *sA, float4 *sB, typename R4<R>::T *wA,
                                            typename R4<R>::T *wB, typename R4<R>::T *wC,
-                                           const double *org) {
+                                           const double *org, bool record = true) {
     const double r2 = open_r2(o, theta);
-    double *dst = node + (size_t)16 * nd;
-    for (int q = 0; q < 16; q++) dst[q] = o[q];
+    if (record) {
+        double *dst = node + (size_t)16 * nd;
+        for (int q = 0; q < 16; q++) dst[q] = o[q];
+    }
     hmax[nd] = hm;
     ropen2[nd] = r2;
     sA[nd] = box_lo(o[10], o[11], o[12], hm);
@@ -232,7 +236,8 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
                const double *__restrict__ h, double *node, double *hmax, double *ropen2,
                float4 *sA, float4 *sB, Opening op, typename R4<R>::T *wA,
                typename R4<R>::T *wB, typename R4<R>::T *wC,
-               const int *__restrict__ cloud, const double *__restrict__ corg) {
+               const int *__restrict__ cloud, const double *__restrict__ corg,
+               int all_records) {
     __shared__ double px[GUP_WARPS][32], py[GUP_WARPS][32], pz[GUP_WARPS][32],
         pm[GUP_WARPS][32], ph[GUP_WARPS][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -279,8 +284,10 @@ __global__ void __launch_bounds__(GUP_WARPS * 32)
             }
             o[0] = cx; o[1] = cy; o[2] = cz; o[3] = M;
             o[4] = qxx; o[5] = qyy; o[6] = qzz; o[7] = qxy; o[8] = qxz; o[9] = qyz;
+            // the climb reads the 16-double record of the group's own node
+            // only; the others are for sph_get_tree
             store_node<R>(nd, o, hm, op.at(l - f + 1), node, hmax, ropen2, sA, sB, wA, wB, wC,
-                          corg + 3 * cloud[s0]);
+                          corg + 3 * cloud[s0], all_records || nd == gnode[g]);
         }
         __syncwarp();
     }
@@ -391,7 +398,7 @@ namespace {
 // leaf records, then the moments, boxes and walk records of the nodes inside
 // the groups and of those above them (groups: the tables of the current
 // topology, rebuilt first when `groups`)
-int tree_records(sph_ctx *ctx, bool groups) {
+int tree_records(sph_ctx *ctx, bool groups, bool all_records) {
     const int n = ctx->n;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
@@ -410,7 +417,8 @@ int tree_records(sph_ctx *ctx, bool groups) {
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
-            (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->cloud[c], ctx->corg);
+            (float4 *)ctx->wA, (float4 *)ctx->wB, (float4 *)ctx->wC, ctx->cloud[c], ctx->corg,
+            all_records ? 1 : 0);
         k_bottom_up<float><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
@@ -426,7 +434,8 @@ int tree_records(sph_ctx *ctx, bool groups) {
             n, ctx->d_ngroup, ctx->gstart, ctx->gcount, ctx->gnode, ctx->first, ctx->last,
             ctx->st[c][ST_X], ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M],
             ctx->st[c][ST_H], ctx->node, ctx->hmax, ctx->ropen2, boxA, boxB, op,
-            (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->cloud[c], ctx->corg);
+            (double4 *)ctx->wA, (double4 *)ctx->wB, (double4 *)ctx->wC, ctx->cloud[c], ctx->corg,
+            all_records ? 1 : 0);
         k_bottom_up<double><<<div_up(n, 256), 256, 0, s>>>(
             n, ctx->d_ngroup, ctx->gnode, ctx->parent, ctx->child, ctx->st[c][ST_X],
             ctx->st[c][ST_Y], ctx->st[c][ST_Z], ctx->st[c][ST_M], ctx->node, ctx->hmax,
@@ -438,7 +447,7 @@ int tree_records(sph_ctx *ctx, bool groups) {
 
 }  // namespace
 
-int launch_tree(sph_ctx *ctx) {
+int launch_tree(sph_ctx *ctx, bool all_records) {
     ctx->cand_ok = false;
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
@@ -454,25 +463,37 @@ int launch_tree(sph_ctx *ctx) {
     CK(cudaMemsetAsync(ctx->parent, 0xff, sizeof(int), s));
     // leaf records (they complete the leaves' first / last the groups read),
     // the groups, the nodes inside the groups, then the climb above them
-    int rc = tree_records(ctx, true);
+    int rc = tree_records(ctx, true, all_records);
     if (rc) return rc;
     ctx->tree_ok = true;
     ctx->topo_ok = true;
     ctx->refits = 0;
+    ctx->records_all = all_records;
     return ctx_check_launch(ctx, "tree");
+}
+
+// every record of every node for the current topology (sph_get_tree after a
+// step, which stores the build records of the group nodes and above only)
+int launch_tree_records(sph_ctx *ctx) {
+    if (ctx->n <= 0) return SPH_OK;
+    int rc = tree_records(ctx, false, true);
+    if (rc) return rc;
+    ctx->records_all = true;
+    return ctx_check_launch(ctx, "tree records");
 }
 
 // The tree of a refit step: the topology, groups and super-groups of the last
 // full build (the storage order has not changed since), every record of every
 // node recomputed from the drifted particles.  The boxes may be looser than a
 // fresh split would give, never wrong.
-int launch_tree_refit(sph_ctx *ctx) {
+int launch_tree_refit(sph_ctx *ctx, bool all_records) {
     ctx->cand_ok = false;
     if (ctx->n <= 0) return SPH_OK;
     if (!ctx->topo_ok) return SPH_ERR_STATE;
-    int rc = tree_records(ctx, false);
+    int rc = tree_records(ctx, false, all_records);
     if (rc) return rc;
     ctx->tree_ok = true;
+    ctx->records_all = all_records;
     return ctx_check_launch(ctx, "tree refit");
 }
 

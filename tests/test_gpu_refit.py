@@ -12,9 +12,10 @@ context resumed from a restart file repeats the one that wrote it.
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from sph_2_b200 import Config, Context, ic
 from sph_2_b200 import _lib as L
-from test_gpu_step_parity import check_step_state, infall
+from test_gpu_step_parity import check_step_state, infall, storage
 
 pytestmark = pytest.mark.gpu
 
@@ -103,3 +104,20 @@ def test_refit_restart_resumes_bit_for_bit(tmp_path, precision):
     for f in ("x", "y", "z", "vx", "vy", "vz", "u", "h", "rho", "ax_grav", "ax_sph"):
         assert np.array_equal(a.get(f), b.get(f)), f
     assert np.array_equal(a.ids(), b.ids())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tree_export_after_refit_steps_is_bitexact(precision):
+    """A step stores the FP64 build records of the group nodes and above
+    only; sph_get_tree recomputes the others, so the exported tree after two
+    refit steps holds the oracle's moments of the current particles on the
+    current topology, bit for bit."""
+    ctx = evrard_ctx(precision, 4, n=5000)
+    ctx.step(2)
+    ctx.sync()
+    t = ctx.tree()
+    x, y, z, m, h = storage(ctx)
+    node, hmax = O.tree_moments(t["child"], t["first"], t["last"], x, y, z, m, h)
+    assert np.array_equal(t["node"].view(np.uint64), node.view(np.uint64))
+    assert np.array_equal(t["hmax"], hmax)
+    ctx.close()
