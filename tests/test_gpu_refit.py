@@ -121,3 +121,26 @@ def test_tree_export_after_refit_steps_is_bitexact(precision):
     assert np.array_equal(t["node"].view(np.uint64), node.view(np.uint64))
     assert np.array_equal(t["hmax"], hmax)
     ctx.close()
+
+
+def test_refit_ensemble_lists_exact():
+    """A 3-cloud ensemble with rebuild_every = 3: after two refit steps the
+    lists of every cloud equal the oracle's (the clouds overlap in space and
+    must stay apart) and the per-cloud storage ranges are unchanged."""
+    e = ic.ensemble(n_clouds=3, nmin=2000, nmax=6000, seed=5)
+    n = len(e["m"])
+    ctx = Context(Config(n_max=n, n_cloud_max=3, precision="mixed", theta=0.5, dt_fixed=1e-3,
+                         rebuild_every=3))
+    vel = e["vel"] + 0.05 * np.random.default_rng(5).normal(size=(n, 3))
+    ctx.load(e["pos"], vel, e["m"], e["h"], e["u"], cloud=e["cloud"])
+    ctx.prologue()
+    ids0 = ctx.ids()
+    ctx.step(2)
+    ctx.sync()
+    assert np.array_equal(ctx.ids(), ids0)
+    x, y, z, m, h = storage(ctx)
+    cl = np.repeat(np.arange(3), np.bincount(e["cloud"], minlength=3)).astype(np.int32)
+    off, lst = ctx.neighbour_lists()
+    oo, ol = O.neighbours(x, y, z, h, cloud=cl)
+    assert np.array_equal(off, oo) and np.array_equal(lst, ol)
+    ctx.close()
