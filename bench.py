@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--theta-small", type=float, default=0.45,
                     help="mixed walk: opening angle of the cells of at most --small-cell particles")
     ap.add_argument("--small-cell", type=int, default=128)
+    ap.add_argument("--no-row-reuse", action="store_true",
+                    help="search every particle in each h iteration (no kept candidate rows)")
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 plain arm")
@@ -348,6 +350,8 @@ def main():
     def make(precision, flags=0, vel=None, walk=None):
         if a.static_grid:
             flags |= L.FLAG_STATIC_GRID
+        if a.no_row_reuse:
+            flags |= L.FLAG_NO_ROW_REUSE
         cfg = Config(n_max=n, precision=precision, leaf_size=a.leaf, ngb_lanes=a.lanes,
                      flags=flags, rebuild_every=a.rebuild_every, **(walk or walk_kw(a, precision)))
         c = Context(cfg)
@@ -628,7 +632,8 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "working set > L2 (neighbour rows ~0.3 GB + tree ~0.5 GB per step)",
                    "graph": "CUDA graph per step",
-                   "rebuild_every": a.rebuild_every},
+                   "rebuild_every": a.rebuild_every,
+                   "kept_candidate_rows": not a.no_row_reuse},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -111,6 +111,9 @@ extern "C" {
 #define SPH_FLAG_STATIC_GRID 128 /* launch the group kernels (walk, searches, h
                                   iteration) with a grid over the groups instead of
                                   a persistent grid draining a work queue        */
+#define SPH_FLAG_NO_ROW_REUSE 512 /* search every particle in each h iteration
+                                  instead of keeping a candidate row that the
+                                  particles' moves since its search leave complete */
 
 typedef struct sph_config {
     int32_t n_max;        /* particle capacity                                    */
@@ -457,6 +460,12 @@ int sph_graph_kernel_count(sph_ctx *ctx, int32_t *count);
 /* kernel nodes of every step graph launched since the last reset (rebuild
  * and refit steps have graphs of their own); reset != 0: start again at 0 */
 int sph_graph_kernels_launched(sph_ctx *ctx, int64_t *count, int32_t reset);
+/* particles whose candidate row the last h iteration (sph_step or
+ * sph_smoothing_h) kept instead of searching again: the distances that they
+ * and the particles near them moved since the row's search leave it complete
+ * (0 with SPH_FLAG_NO_ROW_REUSE, after a sort, or after the count and k-th
+ * iterations) */
+int sph_rows_kept(sph_ctx *ctx, int64_t *kept);
 /* FP32 FMA throughput of this GPU measured by dependent-chain kernels of
  * scalar and of packed (f32x2) FMAs, the larger of the two, TFLOP/s (2 flops
  * per FMA): the denominator for FP32-bound kernels */

@@ -37,6 +37,7 @@ FLAG_TIMING = 32
 FLAG_COOLING_TABLE = 64
 FLAG_STATIC_GRID = 128
 FLAG_MLP_WARP_MMA = 256
+FLAG_NO_ROW_REUSE = 512
 PHASES = ["kick_drift", "sort", "tree", "smoothing_h", "neighbours", "density", "divcurl",
           "forces", "wait_kick", "dudt", "update_dt", "gravity"]
 MLP_NPARAM = 3 * 64 + 64 + 64 * 64 + 64 + 64 + 1
@@ -157,6 +158,7 @@ SIGNATURES = [
     ("sph_time_steps", C.c_int, [_P, _I, _P]),
     ("sph_graph_kernel_count", C.c_int, [_P, _P]),
     ("sph_graph_kernels_launched", C.c_int, [_P, _P, _I]),
+    ("sph_rows_kept", C.c_int, [_P, _P]),
     ("sph_measure_fp32_peak", C.c_int, [_P, _P]),
     ("sph_morton_sort_noalloc", C.c_int, [_P, _P, _P, _I, _P, _P, _P]),
     ("sph_ic_count", C.c_int, [C.c_char_p, _P]),

@@ -474,6 +474,13 @@ class Context:
                   "graph_kernels_launched")
         return int(c.value)
 
+    def rows_kept(self):
+        """Particles whose candidate row the last h iteration kept instead of
+        searching again."""
+        c = C.c_int64(0)
+        self._chk(self._L.sph_rows_kept(self._h, C.byref(c)), "rows_kept")
+        return int(c.value)
+
     def fp32_peak_tflops(self) -> float:
         v = C.c_double()
         self._chk(self._L.sph_measure_fp32_peak(self._h, C.byref(v)), "fp32 peak")

@@ -398,6 +398,10 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
     DAF(ctx->lflag, N + 3);
     DAF(ctx->mlist, N);
     DAF(ctx->retry, N); DAF(ctx->hcand, N); DAF(ctx->hiter, N); DAF(ctx->hover, N);
+    DAF(ctx->hsr, N); DAF(ctx->dmv, N); DAF(ctx->gdm, N);
+    DAF(ctx->dmv_max, C + 1);
+    ctx->rows_ok = (int *)(ctx->dmv_max + C);
+    DAF(ctx->kept_cnt, 3);
     DAF(ctx->dt, C); DAF(ctx->dt_next, C); DAF(ctx->dt_bits, C); DAF(ctx->dtmax_bits, C);
     DAF(ctx->dt_part, N); DAF(ctx->dhdt, N); DAF(ctx->dbin, N);
     DAF(ctx->status, SPH_NSTATUS);
@@ -422,7 +426,10 @@ int sph_ctx_create(const sph_config *cfg, sph_ctx **out) {
         cudaMemsetAsync(ctx->dt, 0, C * sizeof(double), ctx->stream) ||
         cudaMemsetAsync(ctx->divV, 0, N * sizeof(double), ctx->stream) ||
         cudaMemsetAsync(ctx->curlV, 0, N * sizeof(double), ctx->stream) ||
-        cudaMemsetAsync(ctx->corg, 0, 3 * C * sizeof(double), ctx->stream))
+        cudaMemsetAsync(ctx->corg, 0, 3 * C * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->dmv_max, 0, (C + 1) * sizeof(unsigned long long), ctx->stream) ||
+        cudaMemsetAsync(ctx->dmv, 0, N * sizeof(double), ctx->stream) ||
+        cudaMemsetAsync(ctx->kept_cnt, 0, 3 * sizeof(int), ctx->stream))
         return fail(SPH_ERR_CUDA);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(SPH_ERR_CUDA);
 #undef DAF
@@ -612,7 +619,7 @@ int sph_set_field(sph_ctx *ctx, int32_t field, const double *in, int32_t host,
         k_gather_by_id<<<div_up(n, 256), 256, 0, s>>>(n, ctx->id[ctx->cur], ctx->red, dst);
     }
     if (field <= SPH_F_H) {
-        rc = launch_pack_p1(ctx);
+        rc = launch_pack_p1(ctx, true);
         if (rc) return rc;
         if (field <= SPH_F_Z || field == SPH_F_M) ctx->tree_ok = false;
         ctx->cand_ok = false;
@@ -654,7 +661,7 @@ int sph_set_fields(sph_ctx *ctx, int32_t nfield, const int32_t *fields, const do
         }
         if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
     }
-    if (pack && (rc = launch_pack_p1(ctx))) return rc;
+    if (pack && (rc = launch_pack_p1(ctx, true))) return rc;
     CK(cudaStreamSynchronize(s));
     return ctx_check_launch(ctx, "set_fields");
 }
@@ -1182,6 +1189,7 @@ int step_launch(sph_ctx *ctx) {
         }
         CK(cudaGraphLaunch(gx, ctx->stream));
         ctx->graph_kernels_launched += ctx->graph_nk[par][refit ? 1 : 0];
+        ctx->rows_host = true;  // every step ends with the rows of its h iteration
         if (!refit) ctx->cur = par ^ 1;
     }
     if (refit) {
@@ -1273,7 +1281,7 @@ int sph_step_io(sph_ctx *ctx, int32_t nin, const int32_t *fin, const double *con
         }
         if (field == SPH_F_H || (field >= SPH_F_RHO && field <= SPH_F_CURLV)) ctx->p2_dirty = true;
     }
-    if (pack && (rc = launch_pack_p1(ctx))) return rc;
+    if (pack && (rc = launch_pack_p1(ctx, true))) return rc;
     if ((rc = step_launch(ctx))) return rc;
     ctx->tree_ok = ctx->lists_ok = ctx->rho_ok = ctx->divcurl_ok = true;
     // out: on the copy stream, each field gathered into caller order and
@@ -1386,6 +1394,19 @@ int sph_graph_kernels_launched(sph_ctx *ctx, int64_t *count, int32_t reset) {
     if (!ctx || !count) return SPH_ERR_ARG;
     *count = ctx->graph_kernels_launched;
     if (reset) ctx->graph_kernels_launched = 0;
+    return SPH_OK;
+}
+
+int sph_rows_kept(sph_ctx *ctx, int64_t *kept) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!kept) return SPH_ERR_ARG;
+    *kept = 0;
+    if (!ctx->kept_counted) return SPH_OK;
+    int v = 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(&v, ctx->kept_cnt, sizeof(int), cudaMemcpyDeviceToHost));
+    *kept = v;
     return SPH_OK;
 }
 

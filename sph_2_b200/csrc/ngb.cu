@@ -21,7 +21,12 @@
 // with FP64 updates and convergence test, gathering its row again only for
 // the rare second and later evaluations.  Particles whose h outgrows the
 // candidate radius are flagged and searched again in the next round; a row
-// that overflows shrinks the radius instead.
+// that overflows shrinks the radius instead.  Between sorts a group keeps its
+// rows without a search while the distances its particles and the particles
+// near them moved since the rows' search leave the rows complete for a
+// radius above 2 h (refit steps move particles by 1e-4 to 1e-2 h each).
+#include <climits>
+
 #include "sph_internal.cuh"
 
 namespace {
@@ -571,21 +576,173 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 6)
 // to reach h_i + 1.05 h_nb (the largest neighbour h of the last list build) so
 // that the next list is complete from the particle's own candidates, at most
 // to 2 (1.5 h)
+__device__ __forceinline__ double cand_half_radius(double h, double hnb, double grow) {
+    return fmax(h * grow, fmin(0.5 * (h + 1.05 * hnb), 1.5 * h));
+}
+
+// the smallest room a kept row must leave above h: a Newton root beyond it
+// sends the particle to the search; and the reach it must keep towards the
+// largest neighbour h of the last list build (times REACH), below which the
+// list pass would send that neighbour to a tree search: at most REACH_CAP h,
+// just below the 1.5 h that caps a search's own reach
+#ifndef SPH_REUSE_ROOM
+#define SPH_REUSE_ROOM 1.01
+#endif
+#ifndef SPH_REUSE_REACH
+#define SPH_REUSE_REACH 1.01
+#endif
+#ifndef SPH_REUSE_REACH_CAP
+#define SPH_REUSE_REACH_CAP 1.48
+#endif
+
+// the radius / 2 a kept row must still cover
+__device__ __forceinline__ double reuse_need(double h, double hnb) {
+    return fmax(h * SPH_REUSE_ROOM,
+                fmin(0.5 * (h + SPH_REUSE_REACH * hnb), SPH_REUSE_REACH_CAP * h));
+}
+
+// Row reuse.  A search at radius 2 hsr_i listed every j within 2 hsr_i of
+// particle i's position then.  Since that search i moved at most dmv_i and
+// every j at most dmv_j, so the row still lists every j now within
+// 2 hsr_i - dmv_i - M of i, M the largest dmv_j of the particles now that
+// close: half of that is the particle's candidate radius hc without a
+// search.  M = the cloud's largest dmv decides here (retry 2); where that is
+// too coarse but the particle's own move leaves room (retry 3), the first
+// search round bounds M by the particles of the tree nodes near its group.
+// An h iteration that searches every particle (the rows dropped, reuse off,
+// or the last attempt kept fewer than an eighth of the rows) restarts the
+// distances moved, so the next one can keep rows again.
+struct ReuseArgs {
+    int on;                     // rows may be kept
+    const int *rows_ok;         // device flag: the rows belong to the storage order
+    const double *hsr;
+    double *dmv;
+    unsigned long long *dmv_max;
+    const int *cloud;
+    int *kept;                  // rows kept: [0] this h iteration, [1] the last attempt
+                                // (INT_MAX after a full search), [2] this one attempts
+};
+
+// the kept-row counts moved on by one h iteration (one thread)
+__global__ void k_kept_shift(int *kept) {
+    kept[1] = kept[2] ? kept[0] : INT_MAX;
+    kept[0] = 0;
+    kept[2] = 0;
+}
+
 __global__ void k_h_init(int n, const double *__restrict__ h, const double *__restrict__ hnb,
                          double *__restrict__ hc, int *__restrict__ retry, double grow,
-                         double *__restrict__ hover) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+                         double *__restrict__ hover, ReuseArgs U) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double hi = h[i];
-    hc[i] = fmax(hi * grow, fmin(0.5 * (hi + 1.05 * hnb[i]), 1.5 * hi));
-    retry[i] = 1;
+    const double hi = h[i], hn = hnb[i];
+    double c = cand_half_radius(hi, hn, grow);
+    int r = 1;
+    const bool attempt = U.on && *U.rows_ok && U.kept[1] >= n / 8;
+    if (U.kept && i == 0) U.kept[2] = attempt ? 1 : 0;
+    if (attempt) {
+        const double hs = U.hsr[i], own = U.dmv[i];
+        const double cl = __longlong_as_double((long long)U.dmv_max[U.cloud[i]]);
+        const double keep = (hs - 0.5 * (own + cl)) * (1.0 - 1e-12);
+        const double need = reuse_need(hi, hn);
+        if (hs > 0.0 && keep >= need) {
+            c = keep;
+            r = 2;
+        } else if (hs > 0.0 && (hs - 0.5 * own) * (1.0 - 1e-12) >= need) {
+            r = 3;
+        }
+    } else if (U.dmv) {
+        U.dmv[i] = 0.0;
+        if (i == 0 || U.cloud[i] != U.cloud[i - 1]) U.dmv_max[U.cloud[i]] = 0ull;
+    }
+    hc[i] = c;
+    retry[i] = r;
     if (hover) hover[i] = INFINITY;
+}
+
+// per particle: the largest distance moved in its group, rounded up to FP32
+// (every tree node of at most 32 particles lies inside one group); one warp
+// per group
+__global__ void k_group_moved(const int *__restrict__ ngroup_p, const int *__restrict__ gstart,
+                              const int *__restrict__ gcount, const double *__restrict__ dmv,
+                              float *__restrict__ gdm) {
+    const int lane = threadIdx.x & 31;
+    const int ngroup = *ngroup_p;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < ngroup; g += nw) {
+        const int s0 = gstart[g], gc = gcount[g];
+        double d = lane < gc ? dmv[s0 + lane] : 0.0;
+        for (int o = 16; o; o >>= 1) d = fmax(d, __shfl_xor_sync(FULL, d, o));
+        if (lane < gc) gdm[s0 + lane] = __double2float_ru(d);
+    }
+}
+
+// The largest distance moved (gdm) over the particles of the tree nodes of
+// the cloud whose boxes come within frmax of the box [fg0, fg1] (boxes as the
+// search tests them, rounded outward): every particle now that close to the
+// box is in one of them.  INFINITY as soon as it passes lim, or if the
+// stack would overflow.
+__device__ float moved_near(SearchSmem &S, const SearchArgs &A, int root, float fgx0, float fgy0,
+                           float fgz0, float fgx1, float fgy1, float fgz1, float frmax, float lim,
+                           const float *__restrict__ gdm) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const float reach2 = __fmul_ru(__fmul_ru(frmax, frmax), 1.000001f);
+    int sp = 1;
+    if (lane == 0) S.stk[0] = root;
+    __syncwarp();
+    float m = 0.f;
+    bool bad = false;
+    while (sp > 0) {
+        const int take = min(sp, 32);
+        sp -= take;
+        int f = 0, cn = 0, cl = 0, cr = 0;
+        bool open = false;
+        if (lane < take) {
+            const int nd = S.stk[sp + lane];
+            const float4 a = A.sA[nd], b = A.sB[nd];
+            const int4 L = A.wL[nd];
+            f = L.x;
+            cn = L.y;
+            cl = L.z;
+            cr = L.w;
+            const float ex = fmaxf(fmaxf(__fsub_rd(a.x, fgx1), __fsub_rd(fgx0, b.x)), 0.f);
+            const float ey = fmaxf(fmaxf(__fsub_rd(a.y, fgy1), __fsub_rd(fgy0, b.y)), 0.f);
+            const float ez = fmaxf(fmaxf(__fsub_rd(a.z, fgz1), __fsub_rd(fgz0, b.z)), 0.f);
+            const float d2 = __fmaf_rd(ez, ez, __fmaf_rd(ey, ey, __fmul_rd(ex, ex)));
+            open = d2 <= reach2;
+        }
+        __syncwarp();
+        const bool small = cn <= 32;
+        if (open && small) m = fmaxf(m, gdm[f]);
+        const unsigned pm = __ballot_sync(FULL, open && !small);
+        const int npush = 2 * __popc(pm);
+        if (sp + npush > SSTK || __any_sync(FULL, m > lim)) {
+            bad = true;
+            break;
+        }
+        if (open && !small) {
+            const int pos = sp + 2 * __popc(pm & lt);
+            S.stk[pos] = cr;
+            S.stk[pos + 1] = cl;
+        }
+        sp += npush;
+        __syncwarp();
+    }
+    __syncwarp();
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    return bad ? INFINITY : m;
 }
 
 struct NewtonArgs {
     const void *p1;  // Real4 (v, m)
     double *h_out, *hc;
     double *hover;   // per particle: the smallest candidate radius / 2 whose row overflowed
+    double *hsr;     // per particle: radius / 2 of the search that wrote the row (0: incomplete)
+    const double *hnb;
+    const double *dmv;  // distances moved (with hsr: the bound of a kept row)
+    const float *gdm;   // per particle: its group's largest dmv, rounded up
+    int *kept;       // count of the particles that kept their row (null: not counted)
     int *retry;
     double n_ngb, tol, grow, regrow;
     int max_iter, last_round;
@@ -593,18 +750,19 @@ struct NewtonArgs {
 
 // Newton iteration of the particle of every active lane, FP32 or FP64 kernel
 // sums with FP64 update and convergence test.  The first evaluation (at
-// h = pi.w) comes from the search (hs0); later ones, rare once h has settled
-// from step to step, gather the candidates again through the particle's slot
-// row in the same order, so every
-// evaluation sums the same terms in the same order.  No warp collectives:
-// lanes run independent iteration counts.
+// h = pi.w), S0 and D0, comes from the search (searched) or from the kept
+// row; later ones, rare once h has settled from step to step, gather the
+// candidates again through the particle's slot row in the same order, so
+// they sum the same terms in the same order.  No warp collectives: lanes run
+// independent iteration counts.
 template <class R>
 __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArgs &B, int i,
-                                            const double4 &pi, const int *row,
-                                            const HSums<R> &hs0) {
+                                            const double4 &pi, const int *row, double S0,
+                                            double D0, bool searched) {
     typedef typename R4<R>::T V4;
     const V4 *p1 = (const V4 *)B.p1;
     const int craw = A.cnt[i];
+    if (searched) B.hsr[i] = craw > A.K ? 0.0 : B.hc[i];
     if (craw > A.K) {
         // more candidates inside 2 hc than the row holds: the sums would miss
         // some, so remember that radius, shrink hc towards a three-quarter
@@ -639,8 +797,8 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
         }
         double Ssum, Dsum;
         if (it == 1) {
-            Ssum = hs0.S.value();
-            Dsum = hs0.D.value();
+            Ssum = S0;
+            Dsum = D0;
         } else {
             HSums<R> hs;
             hs.inv_h = R(1.0 / h);
@@ -693,9 +851,11 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
         }
     }
     if (need && !B.last_round) {
-        // a wider search, kept below a radius whose row already overflowed
+        // a wider search, kept below a radius whose row already overflowed;
+        // a kept row that h outgrew is searched at the usual radius
         const double ov = B.hover[i];
-        B.hc[i] = h < ov ? fmin(h * B.regrow, h + 0.5 * (ov - h)) : h * B.regrow;
+        const double g = searched ? h * B.regrow : cand_half_radius(h, B.hnb[i], B.grow);
+        B.hc[i] = h < ov ? fmin(g, h + 0.5 * (ov - h)) : g;
         B.retry[i] = 1;
     } else {
         B.retry[i] = 0;
@@ -707,27 +867,83 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
 }
 
 // candidate search + Newton iteration for the flagged particles of each group
-// (latency-bound: 8 blocks per SM, 64 registers, measured faster than 95)
+// (retry 1), and in the first round the Newton iteration from the kept rows
+// (retry 2 and 3) in the same warps, so both share the persistent grid that
+// runs beside the gravity walk (latency-bound: 8 blocks per SM, 64
+// registers, measured faster than 95)
 template <class R>
 __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
     k_cand_newton(const int *__restrict__ ngroup_p, SearchArgs A, NewtonArgs B, unsigned *queue) {
+    typedef typename R4<R>::T V4;
     __shared__ SearchSmem smem[SEARCH_WARPS];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ngroup = *ngroup_p;
     for (int g = q_first(queue, blockIdx.x * SEARCH_WARPS + w); g < ngroup;
          g = q_next(queue, g, gridDim.x * SEARCH_WARPS)) {
         const int s0 = A.gstart[g], gc = A.gcount[g];
-        bool act = lane < gc;
-        const int i = s0 + (act ? lane : 0);
-        act = act && B.retry[i];
-        const unsigned todo = __ballot_sync(FULL, act);
-        if (!todo) continue;
+        const bool in = lane < gc;
+        const int i = s0 + (in ? lane : 0);
+        const int rt = in ? B.retry[i] : 0;
         const double4 pi = A.p0[i];
+        // a group keeps its rows only as a whole: a lane gathering its row
+        // alone would hold up the warp's search for the others
+        bool part = __any_sync(FULL, rt == 1);
+        if (!part && __any_sync(FULL, rt == 3)) {
+            // the moves of the particles near the group decide: M, bounded
+            // over the tree nodes within the largest kept radius of the
+            // group's box, must leave each lane's row the radius it needs
+            const bool l3 = rt == 3;
+            const double hs = l3 ? B.hsr[i] : 0.0, own = l3 ? B.dmv[i] : 0.0;
+            const double lim =
+                l3 ? 2.0 * (hs - reuse_need(pi.w, B.hnb[i]) / (1.0 - 1e-12)) - own : INFINITY;
+            const float flim = __double2float_rd(wmin(lim));
+            const float fgx0 = __double2float_rd(wmin(l3 ? pi.x : INFINITY)),
+                        fgy0 = __double2float_rd(wmin(l3 ? pi.y : INFINITY)),
+                        fgz0 = __double2float_rd(wmin(l3 ? pi.z : INFINITY));
+            const float fgx1 = __double2float_ru(wmax(l3 ? pi.x : -INFINITY)),
+                        fgy1 = __double2float_ru(wmax(l3 ? pi.y : -INFINITY)),
+                        fgz1 = __double2float_ru(wmax(l3 ? pi.z : -INFINITY));
+            const float frmax = __double2float_ru(wmax(2.0 * hs));
+            const float M = flim >= 0.f ? moved_near(smem[w], A, A.croot[A.gcloud[g]], fgx0, fgy0,
+                                                     fgz0, fgx1, fgy1, fgz1, frmax, flim, B.gdm)
+                                        : INFINITY;
+            if (M <= flim) {
+                if (l3) B.hc[i] = (hs - 0.5 * (own + (double)M)) * (1.0 - 1e-12);
+            } else {
+                part = true;
+            }
+        }
+        const bool act = rt == 1 || (rt >= 2 && part), keep = rt >= 2 && !part;
+        const unsigned todo = __ballot_sync(FULL, act);
+        const unsigned km = __ballot_sync(FULL, keep);
+        if (!todo && !km) continue;
+        if (km && lane == 0 && B.kept) atomicAdd(B.kept, __popc(km));
+        const int *row = A.cidx + (size_t)i * A.K;
+        double hci = act ? B.hc[i] : 0.0;
+        if (rt >= 2 && part) {
+            // searched after all, at the usual radius
+            hci = cand_half_radius(pi.w, B.hnb[i], B.grow);
+            B.hc[i] = hci;
+        }
         HSums<R> hs;
         hs.inv_h = R(1.0 / pi.w);
-        group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * B.hc[i], &hs);
-        // each lane reads back only the row entries it wrote itself
-        if (act) newton_lane<R>(A, B, i, pi, A.cidx + (size_t)i * A.K, hs);
+        if (todo) group_search<0, R>(smem[w], A, g, act, i, pi, 2.0 * hci, &hs);
+        if (act) {
+            // each lane reads back only the row entries it wrote itself
+            newton_lane<R>(A, B, i, pi, row, hs.S.value(), hs.D.value(), true);
+        } else if (keep) {
+            // a kept row (first round only): the first evaluation gathers
+            // the row at the current positions (terms beyond 2 h are zero)
+            HSums<R> hk;
+            hk.inv_h = R(1.0 / pi.w);
+            const int c = A.cnt[i];
+#pragma unroll 4
+            for (int k = 0; k < c; k++) {
+                const int j = row[k];
+                hk.add(pair_r<R>(pi, A.p0[j]), (R)(double)((const V4 *)B.p1)[j].w);
+            }
+            newton_lane<R>(A, B, i, pi, row, hk.S.value(), hk.D.value(), false);
+        }
         __syncwarp();
     }
 }
@@ -973,8 +1189,24 @@ int launch_smoothing_h(sph_ctx *ctx) {
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
+    // rows kept from the last h iteration when they can be: decided per
+    // particle and group on the device; the host only knows whether to try
+    const bool reuse = ctx->rows_host && !(ctx->cfg.flags & SPH_FLAG_NO_ROW_REUSE);
+    ReuseArgs U;
+    U.on = reuse ? 1 : 0;
+    U.rows_ok = ctx->rows_ok;
+    U.hsr = ctx->hsr;
+    U.dmv = ctx->dmv;
+    U.dmv_max = ctx->dmv_max;
+    U.cloud = ctx->cloud[c];
+    U.kept = ctx->kept_cnt;
+    k_kept_shift<<<1, 1, 0, s>>>(ctx->kept_cnt);
+    ctx->kept_counted = true;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW, ctx->hover);
+                                            ctx->retry, H_GROW, ctx->hover, U);
+    if (reuse)
+        k_group_moved<<<ctx->num_sms * 4, 256, 0, s>>>(ctx->d_ngroup, ctx->gstart, ctx->gcount,
+                                                       ctx->dmv, ctx->gdm);
     const int rounds = ctx->prologue_done ? 4 : 8;
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
@@ -983,6 +1215,11 @@ int launch_smoothing_h(sph_ctx *ctx) {
     B.h_out = ctx->st[c][ST_H];
     B.hc = ctx->hcand;
     B.hover = ctx->hover;
+    B.hsr = ctx->hsr;
+    B.hnb = ctx->st[c][ST_HNB];
+    B.dmv = ctx->dmv;
+    B.gdm = ctx->gdm;
+    B.kept = ctx->kept_cnt;
     B.retry = ctx->retry;
     B.n_ngb = ctx->cfg.n_ngb;
     B.tol = ctx->cfg.h_tol;
@@ -1001,7 +1238,9 @@ int launch_smoothing_h(sph_ctx *ctx) {
             // the later rounds search again only for the few particles whose
             // h left the candidate radius: a fixed stride over the groups,
             // which most warps skip after one ballot, costs less than one
-            // work-queue atomic per group
+            // work-queue atomic per group (the first round keeps the queue:
+            // after kept rows its share of searched groups ranges from none
+            // to all)
             g = min(grid, ctx->num_sms * 8);
             q = nullptr;
         }
@@ -1010,6 +1249,9 @@ int launch_smoothing_h(sph_ctx *ctx) {
         else
             k_cand_newton<double><<<g, SEARCH_WARPS * 32, 0, s>>>(ctx->d_ngroup, A, B, q);
     }
+    // every row now lists the candidates of its hsr (or is marked incomplete)
+    CK(cudaMemsetAsync(ctx->rows_ok, 1, sizeof(int), s));
+    ctx->rows_host = true;
     ctx->lists_ok = false;
     ctx->cand_ok = true;
     return ctx_check_launch(ctx, "smoothing_h");
@@ -1020,8 +1262,12 @@ int launch_smoothing_h_count(sph_ctx *ctx, int n_target, int n_tol, double frac,
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
+    // these iterations write the rows without their search radii
+    int rc0 = launch_rows_invalidate(ctx);
+    if (rc0) return rc0;
+    ctx->kept_counted = false;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW_COUNT, nullptr);
+                                            ctx->retry, H_GROW_COUNT, nullptr, ReuseArgs{});
     k_zero_int<<<div_up(n, 256), 256, 0, s>>>(n, ctx->hiter);
     // each round widens the radius by H_GROW_COUNT; 0.3 % steps need about 26
     // iterations for that, so 16 rounds cover a 3.4x change of h
@@ -1060,8 +1306,12 @@ int launch_smoothing_kth(sph_ctx *ctx, int k) {
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;
     const int c = ctx->cur;
+    // these iterations write the rows without their search radii
+    int rc0 = launch_rows_invalidate(ctx);
+    if (rc0) return rc0;
+    ctx->kept_counted = false;
     k_h_init<<<div_up(n, 256), 256, 0, s>>>(n, ctx->st[c][ST_H], ctx->st[c][ST_HNB], ctx->hcand,
-                                            ctx->retry, H_GROW_COUNT, nullptr);
+                                            ctx->retry, H_GROW_COUNT, nullptr, ReuseArgs{});
     const int grid = max(1, div_up(div_up(n, 16) + ctx->ncloud, SEARCH_WARPS));
     SearchArgs A = search_args(ctx, nullptr, ctx->cand_cnt);
     CountArgs B{};

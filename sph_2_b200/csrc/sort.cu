@@ -312,7 +312,8 @@ int launch_sort_refit(sph_ctx *ctx) {
     k_box<<<div_up(n, 256), 256, 0, s>>>(st[ST_X], st[ST_Y], st[ST_Z], ctx->cloud[ctx->cur], n,
                                          ctx->box, ctx->status);
     k_origin<<<div_up(ctx->ncloud, 128), 128, 0, s>>>(ctx->box, ctx->ncloud, ctx->corg);
-    int rc = launch_pack_p1(ctx);
+    // same order: the drift is added to the distances moved
+    int rc = launch_pack_p1(ctx, true);
     if (rc) return rc;
     return ctx_check_launch(ctx, "sort refit");
 }
@@ -320,6 +321,9 @@ int launch_sort_refit(sph_ctx *ctx) {
 int launch_sort(sph_ctx *ctx) {
     ctx->cand_ok = false;
     ctx->topo_ok = false;  // the next tree build splits the new order
+    // the candidate rows hold storage indices of the old order
+    int rc0 = launch_rows_invalidate(ctx);
+    if (rc0) return rc0;
     const int n = ctx->n;
     if (n <= 0) return SPH_OK;
     cudaStream_t s = ctx->stream;

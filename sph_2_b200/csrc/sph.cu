@@ -459,8 +459,38 @@ __global__ void k_pack_p1(int n, const double *__restrict__ vx, const double *__
                           const double *__restrict__ z, const double *__restrict__ h,
                           typename R4<R>::T *__restrict__ p1, typename R4<R>::T *__restrict__ pw,
                           double4 *__restrict__ p0, const int *__restrict__ cloud,
-                          const double *__restrict__ corg) {
+                          const double *__restrict__ corg, double *__restrict__ dmv,
+                          unsigned long long *__restrict__ dmv_max) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (dmv) {
+        // the move of the record since the last pack, added to the particle's
+        // distance moved and to its cloud's largest (warp maximum first; the
+        // valid lanes of a warp are a prefix, so lane 0 is one of them)
+        const bool ok = i < n;
+        unsigned long long bits = 0ull;
+        int cl = -1;
+        if (ok) {
+            const double4 o = p0[i];
+            const double dx = x[i] - o.x, dy = y[i] - o.y, dz = z[i] - o.z;
+            // rounded up: a bound, not an estimate
+            const double d = sqrt(dx * dx + dy * dy + dz * dz) * (1.0 + 1e-12);
+            const double D = dmv[i] + d;
+            dmv[i] = D;
+            bits = (unsigned long long)__double_as_longlong(D);
+            cl = cloud[i];
+        }
+        const int c0 = __shfl_sync(0xffffffffu, cl, 0);
+        if (__all_sync(0xffffffffu, !ok || cl == c0)) {
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const unsigned long long t = __shfl_xor_sync(0xffffffffu, bits, o);
+                bits = t > bits ? t : bits;
+            }
+            if ((threadIdx.x & 31) == 0 && c0 >= 0) atomicMax(&dmv_max[c0], bits);
+        } else if (ok) {
+            atomicMax(&dmv_max[cl], bits);
+        }
+    }
     if (i >= n) return;
     typename R4<R>::T a, b;
     a.x = (R)vx[i]; a.y = (R)vy[i]; a.z = (R)vz[i]; a.w = (R)m[i];
@@ -622,18 +652,36 @@ int launch_repack_p2(sph_ctx *ctx) {
     return ctx_check_launch(ctx, "repack_p2");
 }
 
-int launch_pack_p1(sph_ctx *ctx) {
+// The candidate rows of the last h iteration no longer match the storage
+// order or particle set: the next h iteration searches every particle.
+int launch_rows_invalidate(sph_ctx *ctx) {
+    ctx->rows_host = false;
+    CK(cudaMemsetAsync(ctx->rows_ok, 0, sizeof(int), ctx->stream));
+    return SPH_OK;
+}
+
+// track: the storage order is that of the last pack, so the records' moves
+// are added to the distances moved (the candidate rows stay usable);
+// otherwise the rows are dropped
+int launch_pack_p1(sph_ctx *ctx, bool track) {
     const int n = ctx->n, c = ctx->cur;
+    if (!track) {
+        int rc = launch_rows_invalidate(ctx);
+        if (rc) return rc;
+    }
     if (n <= 0) return SPH_OK;
     double *const *st = ctx->st[c];
+    double *dmv = track ? ctx->dmv : nullptr;
     if (ctx->cfg.precision == SPH_PREC_MIXED)
         k_pack_p1<float><<<div_up(n, 256), 256, 0, ctx->stream>>>(
             n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
-            (float4 *)ctx->p1, (float4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg);
+            (float4 *)ctx->p1, (float4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg, dmv,
+            ctx->dmv_max);
     else
         k_pack_p1<double><<<div_up(n, 256), 256, 0, ctx->stream>>>(
             n, st[ST_VX], st[ST_VY], st[ST_VZ], st[ST_M], st[ST_X], st[ST_Y], st[ST_Z], st[ST_H],
-            (double4 *)ctx->p1, (double4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg);
+            (double4 *)ctx->p1, (double4 *)ctx->pw, ctx->p0, ctx->cloud[c], ctx->corg, dmv,
+            ctx->dmv_max);
     return ctx_check_launch(ctx, "pack_p1");
 }
 

@@ -125,10 +125,22 @@ struct sph_ctx {
                               // how many are listed in mlist
     int *mlist = nullptr;     // the particles the fused list pass marked, each once
     bool cand_ok = false;     // candidate rows match the current order, positions and h
-    int *retry = nullptr;        // per particle: 1 = candidate radius too small
+    int *retry = nullptr;        // per particle: 1 search, 2 or 3 keep the row, 0 done
     int *hiter = nullptr;        // per particle: iterations of the count iteration so far
     double *hcand = nullptr;     // candidate radius / 2 used per particle
     double *hover = nullptr;     // smallest candidate radius / 2 whose row overflowed this call
+    // candidate rows kept between the h iterations of refit steps: a row
+    // searched at radius 2 hsr still holds every particle within
+    // 2 hsr - dmv_i - (the largest dmv_j nearby) of the particle's position
+    double *hsr = nullptr;  // per particle: radius / 2 of the search that wrote its row (0: none)
+    double *dmv = nullptr;  // per particle: distance moved through the packed records since the
+                            // last h iteration that searched every particle
+    unsigned long long *dmv_max = nullptr;  // per cloud: the largest dmv (FP64 bits)
+    float *gdm = nullptr;   // per particle: the largest dmv of its group (rounded up)
+    int *rows_ok = nullptr;  // device flag: the rows, hsr and dmv belong to the storage order
+    bool rows_host = false;  // host view of rows_ok, for the choice of launches only
+    int *kept_cnt = nullptr;     // [0] particles whose row the last h iteration kept (3 ints)
+    bool kept_counted = false;   // that count belongs to the last h iteration
     bool lists_ok = false, rho_ok = false, divcurl_ok = false;
 
     // time step, status, counters
@@ -384,7 +396,8 @@ int launch_dt_individual(sph_ctx *ctx);
 int launch_dt_bins(sph_ctx *ctx);
 int launch_dt_commit(sph_ctx *ctx);
 int launch_energies(sph_ctx *ctx, double *out10_host);
-int launch_pack_p1(sph_ctx *ctx);
+int launch_pack_p1(sph_ctx *ctx, bool track = false);
+int launch_rows_invalidate(sph_ctx *ctx);
 int launch_export_neighbours(sph_ctx *ctx, int64_t *off_dev, int *lst_dev, int64_t cap);
 int launch_cooling_exact(sph_ctx *ctx);
 int launch_cooling_table(sph_ctx *ctx);

@@ -144,3 +144,86 @@ def test_refit_ensemble_lists_exact():
     oo, ol = O.neighbours(x, y, z, h, cloud=cl)
     assert np.array_equal(off, oo) and np.array_equal(lst, ol)
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_kept_rows_match_a_fresh_search(precision):
+    """rebuild_every = 4 with the candidate rows kept between the h
+    iterations and with every particle searched each step: the refit steps
+    keep most rows, the rebuild step keeps none, the lists stay the
+    oracle's, and h agrees with the searching run to the rounding of the
+    first Newton evaluation (same terms, another summation order)."""
+    n, dt = 10_000, 1e-3
+    a = evrard_ctx(precision, 4, n=n, dt=dt)
+    b = evrard_ctx(precision, 4, n=n, dt=dt, flags=L.FLAG_NO_ROW_REUSE)
+    assert a.rows_kept() == 0  # the prologue sorted: every particle searched
+    kept = []
+    for k in range(4):
+        a.step(1)
+        b.step(1)
+        a.sync()
+        b.sync()
+        kept.append(a.rows_kept())
+        assert b.rows_kept() == 0
+        st = a.status()
+        assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0 and st["stack_overflow"] == 0, st
+        check_step_state(a, dt, precision)
+        ha, hb = a.get("h", True), b.get("h", True)
+        assert np.max(np.abs(ha / hb - 1.0)) < 1e-5, k
+    # the prologue's rows were searched before its first lists (their reach
+    # towards the largest neighbour h is unknown): the first refit step may
+    # search again; the later ones keep most rows
+    assert max(kept[:3]) > n // 2 and kept[3] == 0, kept
+    a.close()
+    b.close()
+
+
+def test_kept_rows_follow_moves_through_set_fields():
+    """Positions set from the host between steps count as moves: a small
+    shift of every particle keeps the rows, a large jump of a few particles
+    makes the groups near them search again (and no other cloud's), and the
+    lists stay exact either way, per cloud in an ensemble."""
+    e = ic.ensemble(n_clouds=3, nmin=3000, nmax=6000, seed=7)
+    n = len(e["m"])
+    ctx = Context(Config(n_max=n, n_cloud_max=3, precision="mixed", theta=0.5, dt_fixed=1e-4,
+                         rebuild_every=50))
+    ctx.load(e["pos"], e["vel"], e["m"], e["h"], e["u"], cloud=e["cloud"])
+    ctx.prologue()
+    # the prologue's rows lack the reach of its first lists; after one step
+    # that keeps few rows the next searches every particle
+    ctx.step(2)
+    ctx.sync()
+    counts = np.bincount(e["cloud"], minlength=3)
+    cl = np.repeat(np.arange(3), counts).astype(np.int32)
+
+    def lists_exact():
+        x, y, z, m, h = storage(ctx)
+        off, lst = ctx.neighbour_lists()
+        oo, ol = O.neighbours(x, y, z, h, cloud=cl)
+        assert np.array_equal(off, oo) and np.array_equal(lst, ol)
+
+    lists_exact()
+    pos = ctx.get_pos(True)
+    h = ctx.get("h", True)
+    # a shift far below every h: rows kept almost everywhere
+    ctx.set_fields({"x": pos[:, 0] + 1e-3 * float(h.min())}, storage_order=True)
+    ctx.step(1)
+    ctx.sync()
+    assert ctx.rows_kept() > n // 2
+    lists_exact()
+    # ten particles of cloud 0 jump by 3 h: the groups near them cannot keep
+    # their rows, the other clouds keep theirs
+    pos = ctx.get_pos(True)
+    h = ctx.get("h", True)
+    x = pos[:, 0].copy()
+    x[:10] += 3.0 * h[:10]
+    ctx.set_fields({"x": x}, storage_order=True)
+    ctx.step(1)
+    ctx.sync()
+    kept = ctx.rows_kept()
+    assert kept < n, (kept, counts)
+    assert kept > (n - counts[0]) // 2, (kept, counts)
+    lists_exact()
+    st = ctx.status()
+    assert st["h_noconv"] == 0 and st["ngb_overflow"] == 0 and st["stack_overflow"] == 0, st
+    ctx.close()
