@@ -866,6 +866,40 @@ __device__ __forceinline__ void newton_lane(const SearchArgs &A, const NewtonArg
     A.p0[i].w = h;  // p0 is written only by the lane owning particle i
 }
 
+// the first Newton evaluation of the kept rows of a group: four lanes per
+// row over interleaved entries (terms beyond 2 h are zero), eight rows at a
+// time, each row's sums handed to the lane of its particle
+template <class R>
+__device__ __forceinline__ void kept_sums(const SearchArgs &A, const NewtonArgs &B, int s0, int gc,
+                                       double &S0, double &D0) {
+    typedef typename R4<R>::T V4;
+    const int lane = threadIdx.x & 31, q = lane >> 2, sl = lane & 3;
+    S0 = 0.0;
+    D0 = 0.0;
+    for (int p = 0; p < gc; p += 8) {
+        HSums<R> hk;
+        hk.inv_h = R(1);
+        if (p + q < gc) {
+            const int ii = s0 + p + q;
+            const double4 pp = A.p0[ii];
+            hk.inv_h = R(1.0 / pp.w);
+            const int c = A.cnt[ii];
+            const int *rw = A.cidx + (size_t)ii * A.K;
+            for (int k = sl; k < c; k += 4) {
+                const int j = rw[k];
+                hk.add(pair_r<R>(pp, A.p0[j]), (R)(double)((const V4 *)B.p1)[j].w);
+            }
+        }
+        const double sS = seg_sum<4>(hk.S.value()), sD = seg_sum<4>(hk.D.value());
+        const int src = ((lane - p) & 7) * 4;
+        const double tS = __shfl_sync(FULL, sS, src), tD = __shfl_sync(FULL, sD, src);
+        if (lane >= p && lane < p + 8) {
+            S0 = tS;
+            D0 = tD;
+        }
+    }
+}
+
 // candidate search + Newton iteration for the flagged particles of each group
 // (retry 1), and in the first round the Newton iteration from the kept rows
 // (retry 2 and 3) in the same warps, so both share the persistent grid that
@@ -931,18 +965,12 @@ __global__ void __launch_bounds__(SEARCH_WARPS * 32, 8)
         if (act) {
             // each lane reads back only the row entries it wrote itself
             newton_lane<R>(A, B, i, pi, row, hs.S.value(), hs.D.value(), true);
-        } else if (keep) {
-            // a kept row (first round only): the first evaluation gathers
-            // the row at the current positions (terms beyond 2 h are zero)
-            HSums<R> hk;
-            hk.inv_h = R(1.0 / pi.w);
-            const int c = A.cnt[i];
-#pragma unroll 4
-            for (int k = 0; k < c; k++) {
-                const int j = row[k];
-                hk.add(pair_r<R>(pi, A.p0[j]), (R)(double)((const V4 *)B.p1)[j].w);
-            }
-            newton_lane<R>(A, B, i, pi, row, hk.S.value(), hk.D.value(), false);
+        }
+        if (km) {
+            // the group kept its rows (first round only; no lane searches)
+            double S0, D0;
+            kept_sums<R>(A, B, s0, gc, S0, D0);
+            if (keep) newton_lane<R>(A, B, i, pi, row, S0, D0, false);
         }
         __syncwarp();
     }
